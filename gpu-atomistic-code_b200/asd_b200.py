@@ -1,0 +1,352 @@
+"""ctypes binding of the C ABI in include/asd.h (libasd_b200.so, built next to this file).
+
+The binding is a thin layer: every method maps to one asd_* call and raises
+AsdError with the library's message on a non-zero status.  There is no CPU
+fallback: importing works without a GPU, but creating a handle needs the CUDA
+library and a device, and fails loudly otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libasd_b200.so")
+
+ASD_OK, ASD_EINVAL, ASD_ECUDA, ASD_ENOMEM, ASD_ETIMEOUT, ASD_ESTATE, ASD_ECUFFT, ASD_ENOTSUP, ASD_ENOTFINITE = range(9)
+HEUN, RK4, RK5 = 0, 1, 2
+FP64_PLAIN, FP32, FP64_FUSED = 0, 1, 2
+EXCH_FFT, EXCH_DIA, EXCH_CSR, EXCH_NONE = 0, 1, 2, 3
+LR_NONE, LR_DIPOLE, LR_FFT = 0, 1, 2
+FLAG_RK_DOUBLE_RDT = 1 << 2
+FLAG_RK_STAGE_SPIN_MIXED = 1 << 3
+FLAG_GPU_CSR_DIP_STALE = 1 << 4
+FLAG_GPU_DZZ_FROM_DYY = 1 << 6
+FLAG_GPU_HDEMAG_FP32 = 1 << 7
+FLAG_COMPENSATED = 1 << 16
+FLAG_AUTOTUNE = 1 << 17
+ALL_REPLICAS = 0xFFFFFFFF
+
+MUB, KB, GYRO = 9.27e-24, 1.38e-23, 1.76e11  # reference constants (src/llg.cpp:25)
+
+EXPORTED = [
+    "asd_create", "asd_destroy", "asd_last_error", "asd_version", "asd_set_spins", "asd_get_spins",
+    "asd_get_det_field", "asd_get_field", "asd_step", "asd_get_step", "asd_set_step", "asd_sync",
+    "asd_set_temperature", "asd_set_applied", "asd_set_site_field", "asd_set_site_field_scale",
+    "asd_magnetisation", "asd_num_sublattices", "asd_time_steps", "asd_time_kernels", "asd_kernel_stats",
+    "asd_thermal_normals", "asd_build_csr", "asd_csr_to_dia", "asd_build_dipole_nr", "asd_fold_exchange_nr",
+]
+
+
+class Material(C.Structure):
+    _fields_ = [("mu", C.c_double), ("lambda_", C.c_double), ("gamma", C.c_double), ("k1u", C.c_double),
+                ("k1u_dir", C.c_double * 3), ("sublattice", C.c_uint32)]
+
+
+class Params(C.Structure):
+    _fields_ = [("integrator", C.c_uint32), ("precision", C.c_uint32), ("dt", C.c_double),
+                ("applied", C.c_double * 3), ("k2perp", C.c_double), ("k2perpdir", C.c_double * 3),
+                ("k2par", C.c_double), ("k2pardir", C.c_double * 3), ("k4perp", C.c_double),
+                ("k4perpdirs", C.c_double * 9), ("k4par", C.c_double), ("k4pardirs", C.c_double * 9),
+                ("seed", C.c_uint64), ("update", C.c_uint32), ("flags", C.c_uint32),
+                ("gyro", C.c_double), ("muB", C.c_double), ("kB", C.c_double)]
+
+
+class System(C.Structure):
+    _fields_ = [("nspins", C.c_uint32), ("nmat", C.c_uint32), ("mat", C.POINTER(Material)),
+                ("atom", C.POINTER(C.c_uint32)), ("exch", C.c_uint32), ("exch_full", C.c_uint32),
+                ("xadj", C.POINTER(C.c_uint32)), ("adjncy", C.POINTER(C.c_uint32)), ("nnz", C.c_uint32),
+                ("csr_val", C.POINTER(C.c_double)), ("ndiag", C.c_uint32), ("dia_offset", C.POINTER(C.c_int32)),
+                ("dia_val", C.POINTER(C.c_double)), ("lr", C.c_uint32), ("mesh", C.c_uint32 * 3),
+                ("mesh_xyz", C.POINTER(C.c_uint32)), ("nr", C.POINTER(C.c_double)), ("temperature", C.c_double),
+                ("stream", C.c_uint32), ("site_field", C.POINTER(C.c_double))]
+
+
+class AsdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"asd error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libasd_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} not built: run `make -C {HERE}` (or __graft_entry__.build())")
+    lib = C.CDLL(path)
+    P = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    u32p = C.POINTER(C.c_uint32)
+    i32p = C.POINTER(C.c_int32)
+    sig = {
+        "asd_create": ([C.POINTER(Params), C.POINTER(System), C.c_uint32, C.POINTER(P)], C.c_int),
+        "asd_destroy": ([P], C.c_int),
+        "asd_last_error": ([P], C.c_char_p),
+        "asd_version": ([], C.c_char_p),
+        "asd_set_spins": ([P, dp, C.c_size_t], C.c_int),
+        "asd_get_spins": ([P, dp, C.c_size_t], C.c_int),
+        "asd_get_det_field": ([P, dp, C.c_size_t], C.c_int),
+        "asd_get_field": ([P, dp, C.c_size_t], C.c_int),
+        "asd_step": ([P, C.c_uint64], C.c_int),
+        "asd_get_step": ([P, C.POINTER(C.c_uint64)], C.c_int),
+        "asd_set_step": ([P, C.c_uint64], C.c_int),
+        "asd_sync": ([P], C.c_int),
+        "asd_set_temperature": ([P, C.c_uint32, C.c_double], C.c_int),
+        "asd_set_applied": ([P, dp], C.c_int),
+        "asd_set_site_field": ([P, dp, C.c_size_t], C.c_int),
+        "asd_set_site_field_scale": ([P, C.c_double], C.c_int),
+        "asd_magnetisation": ([P, dp, C.c_size_t], C.c_int),
+        "asd_num_sublattices": ([P, u32p], C.c_int),
+        "asd_time_steps": ([P, C.c_uint64, dp, C.POINTER(C.c_uint64)], C.c_int),
+        "asd_time_kernels": ([P, C.c_uint64], C.c_int),
+        "asd_kernel_stats": ([P, C.c_char_p, C.c_size_t, dp, C.POINTER(C.c_uint64), dp], C.c_int),
+        "asd_thermal_normals": ([C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, dp], C.c_int),
+        "asd_build_csr": ([u32p, C.POINTER(C.c_int), C.c_uint32, dp, C.c_uint32, u32p, u32p, i32p, dp, C.c_double,
+                           u32p, u32p, dp, u32p], C.c_int),
+        "asd_csr_to_dia": ([C.c_uint32, u32p, u32p, dp, i32p, dp, u32p], C.c_int),
+        "asd_build_dipole_nr": ([u32p, u32p, dp, C.c_double, C.c_double, dp], C.c_int),
+        "asd_fold_exchange_nr": ([u32p, C.c_uint32, i32p, dp, C.c_double, dp, u32p], C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def _p(a: Optional[np.ndarray], ct):
+    if a is None:
+        return C.cast(None, C.POINTER(ct))
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def _check(rc: int, h=None):
+    if rc != ASD_OK:
+        msg = ""
+        if h is not None:
+            m = load_library().asd_last_error(h)
+            msg = m.decode() if m else ""
+        raise AsdError(rc, msg or "call failed")
+
+
+@dataclass
+class MaterialSpec:
+    mu: float = 1.5                 # [muB]
+    lam: float = 0.1                # damping
+    gamma: float = 1.0              # relative gyromagnetic ratio
+    k1u: float = 0.0                # [J/atom]
+    k1u_dir: Sequence[float] = (0.0, 0.0, 1.0)
+    sublattice: int = 0
+
+
+@dataclass
+class SpinSystem:
+    """One lattice with its interactions, in the reference's data contract."""
+    nspins: int
+    materials: list
+    atom: Optional[np.ndarray] = None          # unit-cell atom per spin (None -> i % nmat)
+    exch: int = EXCH_NONE
+    full: bool = False
+    xadj: Optional[np.ndarray] = None
+    adjncy: Optional[np.ndarray] = None
+    csr_val: Optional[np.ndarray] = None       # nnz x 9 [T]
+    dia_offset: Optional[np.ndarray] = None
+    dia_val: Optional[np.ndarray] = None       # 9 x ndiag x n [T]
+    lr: int = LR_NONE
+    mesh: Sequence[int] = (0, 0, 0)
+    mesh_xyz: Optional[np.ndarray] = None      # n x 3
+    nr: Optional[np.ndarray] = None            # 9 x P real-space interaction matrix
+    temperature: float = 0.0
+    stream: int = 0
+    site_field: Optional[np.ndarray] = None    # n x 3
+    sublattice_of_spin: Optional[np.ndarray] = None
+    meta: dict = field(default_factory=dict)
+
+    def nmat(self):
+        return len(self.materials)
+
+
+@dataclass
+class RunParams:
+    integrator: int = HEUN
+    precision: int = FP32
+    dt: float = 1e-16
+    applied: Sequence[float] = (0.0, 0.0, 0.0)
+    k2perp: float = 0.0
+    k2perpdir: Sequence[float] = (0.0, 0.0, 0.0)
+    k2par: float = 0.0
+    k2pardir: Sequence[float] = (0.0, 0.0, 0.0)
+    k4perp: float = 0.0
+    k4perpdirs: Sequence[float] = (0.0,) * 9
+    k4par: float = 0.0
+    k4pardirs: Sequence[float] = (0.0,) * 9
+    seed: int = 1
+    update: int = 1
+    flags: int = 0
+
+    def to_c(self) -> Params:
+        p = Params()
+        p.integrator, p.precision, p.dt = self.integrator, self.precision, self.dt
+        p.applied[:] = list(self.applied)
+        p.k2perp, p.k2par, p.k4perp, p.k4par = self.k2perp, self.k2par, self.k4perp, self.k4par
+        p.k2perpdir[:] = list(self.k2perpdir)
+        p.k2pardir[:] = list(self.k2pardir)
+        p.k4perpdirs[:] = list(self.k4perpdirs)
+        p.k4pardirs[:] = list(self.k4pardirs)
+        p.seed, p.update, p.flags = self.seed, self.update, self.flags
+        p.gyro, p.muB, p.kB = GYRO, MUB, KB
+        return p
+
+
+class Handle:
+    """An asd_handle: one or more replicas advanced together on the current CUDA device."""
+
+    def __init__(self, params: RunParams, systems):
+        lib = load_library()
+        if isinstance(systems, SpinSystem):
+            systems = [systems]
+        self._keep = []
+        csys = (System * len(systems))()
+        for r, s in enumerate(systems):
+            mats = (Material * len(s.materials))()
+            for t, m in enumerate(s.materials):
+                mats[t].mu, mats[t].lambda_, mats[t].gamma, mats[t].k1u = m.mu, m.lam, m.gamma, m.k1u
+                mats[t].k1u_dir[:] = list(m.k1u_dir)
+                mats[t].sublattice = m.sublattice
+            self._keep.append(mats)
+            cs = csys[r]
+            cs.nspins, cs.nmat, cs.mat = s.nspins, len(s.materials), mats
+            arr = lambda a, dt: None if a is None else np.ascontiguousarray(a, dtype=dt)
+            atom = arr(s.atom, np.uint32)
+            xadj, adj, cv = arr(s.xadj, np.uint32), arr(s.adjncy, np.uint32), arr(s.csr_val, np.float64)
+            doff, dval = arr(s.dia_offset, np.int32), arr(s.dia_val, np.float64)
+            mxyz, nr, site = arr(s.mesh_xyz, np.uint32), arr(s.nr, np.float64), arr(s.site_field, np.float64)
+            self._keep += [atom, xadj, adj, cv, doff, dval, mxyz, nr, site]
+            cs.atom = _p(atom, C.c_uint32)
+            cs.exch, cs.exch_full = s.exch, 1 if s.full else 0
+            cs.xadj, cs.adjncy = _p(xadj, C.c_uint32), _p(adj, C.c_uint32)
+            cs.nnz = 0 if adj is None else len(adj)
+            cs.csr_val = _p(cv, C.c_double)
+            cs.ndiag = 0 if doff is None else len(doff)
+            cs.dia_offset, cs.dia_val = _p(doff, C.c_int32), _p(dval, C.c_double)
+            cs.lr = s.lr
+            cs.mesh[:] = list(s.mesh)
+            cs.mesh_xyz, cs.nr = _p(mxyz, C.c_uint32), _p(nr, C.c_double)
+            cs.temperature, cs.stream = s.temperature, s.stream
+            cs.site_field = _p(site, C.c_double)
+        self.params = params
+        self.n = sum(s.nspins for s in systems)
+        self.nrep = len(systems)
+        self._cp = params.to_c()
+        h = C.c_void_p()
+        rc = lib.asd_create(C.byref(self._cp), csys, len(systems), C.byref(h))
+        if rc != ASD_OK:
+            raise AsdError(rc, "asd_create failed")
+        self.h = h
+        self._keep = None
+        ns = C.c_uint32()
+        _check(lib.asd_num_sublattices(self.h, C.byref(ns)), self.h)
+        self.nsub = ns.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().asd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_spins(self, s: np.ndarray):
+        s = np.ascontiguousarray(s, dtype=np.float64).reshape(-1)
+        _check(load_library().asd_set_spins(self.h, _p(s, C.c_double), len(s) // 3), self.h)
+
+    def _read(self, fn):
+        out = np.empty(3 * self.n, dtype=np.float64)
+        _check(fn(self.h, _p(out, C.c_double), self.n), self.h)
+        return out.reshape(self.n, 3)
+
+    def get_spins(self):
+        return self._read(load_library().asd_get_spins)
+
+    def get_det_field(self):
+        return self._read(load_library().asd_get_det_field)
+
+    def get_field(self):
+        return self._read(load_library().asd_get_field)
+
+    def step(self, n: int):
+        _check(load_library().asd_step(self.h, n), self.h)
+
+    @property
+    def t(self) -> int:
+        v = C.c_uint64()
+        _check(load_library().asd_get_step(self.h, C.byref(v)), self.h)
+        return v.value
+
+    def set_step(self, t: int):
+        _check(load_library().asd_set_step(self.h, t), self.h)
+
+    def sync(self):
+        _check(load_library().asd_sync(self.h), self.h)
+
+    def set_temperature(self, T: float, replica: int = ALL_REPLICAS):
+        _check(load_library().asd_set_temperature(self.h, replica, T), self.h)
+
+    def set_applied(self, b):
+        a = np.ascontiguousarray(b, dtype=np.float64)
+        _check(load_library().asd_set_applied(self.h, _p(a, C.c_double)), self.h)
+
+    def set_site_field(self, prof: Optional[np.ndarray]):
+        a = None if prof is None else np.ascontiguousarray(prof, dtype=np.float64).reshape(-1)
+        _check(load_library().asd_set_site_field(self.h, _p(a, C.c_double), self.n if a is not None else 0), self.h)
+
+    def set_site_field_scale(self, rv: float):
+        _check(load_library().asd_set_site_field_scale(self.h, rv), self.h)
+
+    def magnetisation(self):
+        out = np.empty(self.nrep * self.nsub * 3, dtype=np.float64)
+        _check(load_library().asd_magnetisation(self.h, _p(out, C.c_double), len(out)), self.h)
+        return out.reshape(self.nrep, self.nsub, 3)
+
+    def time_steps(self, n: int):
+        ms = C.c_double()
+        l = C.c_uint64()
+        _check(load_library().asd_time_steps(self.h, n, C.byref(ms), C.byref(l)), self.h)
+        return ms.value, l.value
+
+    def time_kernels(self, n: int):
+        lib = load_library()
+        _check(lib.asd_time_kernels(self.h, n), self.h)
+        name = C.create_string_buffer(128)
+        avg, cnt, b = C.c_double(), C.c_uint64(), C.c_double()
+        _check(lib.asd_kernel_stats(self.h, name, 128, C.byref(avg), C.byref(cnt), C.byref(b)), self.h)
+        return {"name": name.value.decode(), "avg_ms": avg.value, "count": cnt.value, "bytes": b.value}
+
+
+def thermal_normals(seed: int, stream: int, step: int, nspins: int) -> np.ndarray:
+    out = np.empty(3 * nspins, dtype=np.float64)
+    _check(load_library().asd_thermal_normals(seed, stream, step, nspins, _p(out, C.c_double)))
+    return out.reshape(nspins, 3)
+
+
+def version() -> str:
+    return load_library().asd_version().decode()

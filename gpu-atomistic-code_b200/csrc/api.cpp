@@ -1,0 +1,818 @@
+// C ABI implementation (include/asd.h): handle life cycle, uploads into the
+// device layouts, step scheduling (direct launches for the FP64 plain form,
+// CUDA-graph chunks for the fused forms), read-backs and timing.
+#include "internal.h"
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace asd;
+
+namespace {
+
+const double REF_GYRO = 1.76e11, REF_MUB = 9.27e-24, REF_KB = 1.38e-23;  // src/llg.cpp:25
+
+struct Fail {
+    int code;
+    std::string msg;
+};
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            throw Fail{e_ == cudaErrorMemoryAllocation ? ASD_ENOMEM : ASD_ECUDA,                   \
+                       std::string(#call) + ": " + cudaGetErrorString(e_)};                        \
+    } while (0)
+#define CKFFT(call)                                                                                \
+    do {                                                                                           \
+        cufftResult r_ = (call);                                                                   \
+        if (r_ != CUFFT_SUCCESS) throw Fail{ASD_ECUFFT, std::string(#call) + " failed (" + std::to_string((int)r_) + ")"}; \
+    } while (0)
+#define REQUIRE(cond, msg) \
+    do { if (!(cond)) throw Fail{ASD_EINVAL, msg}; } while (0)
+
+template <typename T>
+T* dalloc(size_t n) {
+    T* p = nullptr;
+    CK(cudaMalloc(&p, sizeof(T) * (n ? n : 1)));
+    CK(cudaMemset(p, 0, sizeof(T) * (n ? n : 1)));
+    return p;
+}
+
+template <typename T>
+T* dupload(const T* src, size_t n) {
+    T* p = dalloc<T>(n);
+    if (n) CK(cudaMemcpy(p, src, sizeof(T) * n, cudaMemcpyHostToDevice));
+    return p;
+}
+
+int fail(asd_handle* h, const Fail& f) {
+    if (h) h->err = f.msg;
+    return f.code;
+}
+
+void free_all(asd_handle* h) {
+    auto F = [](void* p) { if (p) cudaFree(p); };
+    F(h->d_rep_off); F(h->d_rep_stream); F(h->d_atom); F(h->d_rep_sqrtT); F(h->d_dyn); F(h->d_step);
+    for (int c = 0; c < 3; c++) {
+        F(h->sf[c]); F(h->sl[c]); F(h->esf[c]); F(h->fnf[c]); F(h->detf[c]); F(h->stagf[c]);
+        F(h->sd[c]); F(h->esd[c]); F(h->fnd[c]); F(h->detd[c]); F(h->stagd[c]);
+        for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
+    }
+    F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
+    F(h->dia.off); F(h->dia.valf); F(h->dia.vald);
+    F(h->p_s); F(h->p_es); F(h->p_fn); F(h->p_ch); F(h->p_hdemag); F(h->p_rand); F(h->p_det); F(h->p_hstg); F(h->p_hinit);
+    for (int q = 0; q < 6; q++) F(h->p_k[q]);
+    F(h->p_sigma); F(h->p_llgpf); F(h->p_lambda); F(h->p_k1u); F(h->p_k1udir);
+    F(h->pex.xadj); F(h->pex.adjncy); F(h->pex.off);
+    for (int q = 0; q < 9; q++) F(h->pex.v[q]);
+    LongRange& L = h->lr;
+    F(L.mesh_idx); F(L.w); F(L.r); F(L.k); F(L.nkr); F(L.nkc); F(L.zr); F(L.zk); F(L.zh); F(L.znk);
+    if (L.r2c) cufftDestroy(L.r2c);
+    if (L.c2r) cufftDestroy(L.c2r);
+    if (L.z2z) cufftDestroy(L.z2z);
+    F(h->d_magpart); F(h->d_mag); F(h->d_inv_count); F(h->d_sub_of_atom);
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->kev[0]) cudaEventDestroy(h->kev[0]);
+    if (h->kev[1]) cudaEventDestroy(h->kev[1]);
+    if (h->stream) cudaStreamDestroy(h->stream);
+}
+
+// CSR (all replicas concatenated) -> SELL-32 device layout.
+void build_sell(asd_handle* h, const std::vector<uint32_t>& xadj, const std::vector<uint32_t>& adj,
+                const std::vector<double>& val9) {
+    const uint32_t n = h->n;
+    const bool full = h->full != 0;
+    const bool zz_yy = (h->p.flags & ASD_FLAG_GPU_DZZ_FROM_DYY) != 0;
+    const uint32_t ns = (n + 31) / 32;
+    std::vector<uint32_t> sp(ns + 1, 0);
+    for (uint32_t s = 0; s < ns; s++) {
+        uint32_t w = 0;
+        for (uint32_t r = 32 * s; r < std::min(n, 32 * s + 32); r++) w = std::max(w, xadj[r + 1] - xadj[r]);
+        sp[s + 1] = sp[s] + 32 * w;
+    }
+    const uint32_t E = sp[ns];
+    h->sell.nslices = ns;
+    h->sell.entries = E;
+    h->sell.slice_ptr = dupload(sp.data(), sp.size());
+    auto value = [&](uint32_t k, int q) {
+        if (q == 8 && zz_yy) q = 4;
+        return val9[9 * (size_t)k + q];
+    };
+    if (h->p.precision == ASD_FP32) {
+        std::vector<float4> a(E), b(full ? E : 0);
+        std::vector<float2> c(full ? E : 0);
+        for (uint32_t s = 0; s < ns; s++) {
+            const uint32_t w = (sp[s + 1] - sp[s]) / 32;
+            for (uint32_t k = 0; k < w; k++)
+                for (uint32_t lane = 0; lane < 32; lane++) {
+                    const uint32_t r = 32 * s + lane, e = sp[s] + 32 * k + lane;
+                    int col = r < n ? (int)r : 0;
+                    float v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                    if (r < n && k < xadj[r + 1] - xadj[r]) {
+                        const uint32_t kk = xadj[r] + k;
+                        col = (int)adj[kk];
+                        for (int q = 0; q < 9; q++) v[q] = (float)value(kk, q);
+                    }
+                    int ci;
+                    memcpy(&ci, &col, 4);
+                    float cf;
+                    memcpy(&cf, &ci, 4);
+                    if (!full) a[e] = make_float4(cf, v[0], v[4], v[8]);
+                    else {
+                        a[e] = make_float4(cf, v[0], v[1], v[2]);
+                        b[e] = make_float4(v[3], v[4], v[5], v[6]);
+                        c[e] = make_float2(v[7], v[8]);
+                    }
+                }
+        }
+        h->sell.a = dupload(a.data(), a.size());
+        if (full) { h->sell.b = dupload(b.data(), b.size()); h->sell.c = dupload(c.data(), c.size()); }
+    } else {
+        const int nc = full ? 9 : 3;
+        const int qmap3[3] = {0, 4, 8};
+        std::vector<int32_t> col(E);
+        std::vector<double> v((size_t)nc * E, 0.0);
+        for (uint32_t s = 0; s < ns; s++) {
+            const uint32_t w = (sp[s + 1] - sp[s]) / 32;
+            for (uint32_t k = 0; k < w; k++)
+                for (uint32_t lane = 0; lane < 32; lane++) {
+                    const uint32_t r = 32 * s + lane, e = sp[s] + 32 * k + lane;
+                    col[e] = r < n ? (int)r : 0;
+                    if (r < n && k < xadj[r + 1] - xadj[r]) {
+                        const uint32_t kk = xadj[r] + k;
+                        col[e] = (int)adj[kk];
+                        for (int q = 0; q < nc; q++) v[(size_t)q * E + e] = value(kk, full ? q : qmap3[q]);
+                    }
+                }
+        }
+        h->sell.col = dupload(col.data(), col.size());
+        h->sell.val = dupload(v.data(), v.size());
+    }
+}
+
+void setup_lr(asd_handle* h, const asd_system& s, bool plain) {
+    LongRange& L = h->lr;
+    L.mode = (int)s.lr;
+    for (int a = 0; a < 3; a++) L.mesh[a] = s.mesh[a];
+    REQUIRE(L.mesh[0] && L.mesh[1] && L.mesh[2], "long-range field needs a mesh");
+    REQUIRE(L.mesh[2] % 2 == 0, "last mesh dimension must be even");
+    L.P = (size_t)L.mesh[0] * L.mesh[1] * L.mesh[2];
+    L.Pk = (size_t)L.mesh[0] * L.mesh[1] * (L.mesh[2] / 2 + 1);
+    REQUIRE(s.mesh_xyz && s.nr, "long-range field needs mesh_xyz and nr");
+    std::vector<uint32_t> idx(h->n);
+    std::vector<float> w(h->n);
+    for (uint32_t i = 0; i < h->n; i++) {
+        const uint32_t x = s.mesh_xyz[3 * i], y = s.mesh_xyz[3 * i + 1], z = s.mesh_xyz[3 * i + 2];
+        REQUIRE(x < L.mesh[0] && y < L.mesh[1] && z < L.mesh[2], "mesh_xyz outside the mesh");
+        idx[i] = (uint32_t)(((size_t)x * L.mesh[1] + y) * L.mesh[2] + z);
+        const uint32_t at = s.atom ? s.atom[i] : i % s.nmat;
+        w[i] = s.lr == ASD_LR_DIPOLE ? (float)s.mat[at].mu : 1.0f;
+    }
+    L.mesh_idx = dupload(idx.data(), idx.size());
+    L.w = dupload(w.data(), w.size());
+    // symmetry of N_r decides 6 or 9 stored components
+    bool sym = true;
+    for (size_t c = 0; c < L.P && sym; c++) {
+        if (s.nr[1 * L.P + c] != s.nr[3 * L.P + c] || s.nr[2 * L.P + c] != s.nr[6 * L.P + c] ||
+            s.nr[5 * L.P + c] != s.nr[7 * L.P + c])
+            sym = false;
+    }
+    L.ncomp = sym ? 6 : 9;
+    double* d_nr = dupload(s.nr, 9 * L.P);
+    int dims[3] = {(int)L.mesh[0], (int)L.mesh[1], (int)L.mesh[2]};
+    cudaError_t e;
+    if (plain) {
+        L.zr = dalloc<double2>(3 * L.P);
+        L.zk = dalloc<double2>(3 * L.P);
+        L.zh = dalloc<double2>(3 * L.P);
+        L.znk = dalloc<double2>(9 * L.P);
+        CKFFT(cufftPlanMany(&L.z2z, 3, dims, nullptr, 1, (int)L.P, nullptr, 1, (int)L.P, CUFFT_Z2Z, 3));
+        CKFFT(cufftSetStream(L.z2z, h->stream));
+        e = build_nk_plain(h, d_nr);
+    } else {
+        L.r = dalloc<float>(6 * L.P);   // [0,3P): M_r, [3P,6P): H_r
+        L.k = dalloc<float2>(3 * L.Pk);
+        CKFFT(cufftPlanMany(&L.r2c, 3, dims, nullptr, 1, (int)L.P, nullptr, 1, (int)L.Pk, CUFFT_R2C, 3));
+        CKFFT(cufftPlanMany(&L.c2r, 3, dims, nullptr, 1, (int)L.Pk, nullptr, 1, (int)L.P, CUFFT_C2R, 3));
+        CKFFT(cufftSetStream(L.r2c, h->stream));
+        CKFFT(cufftSetStream(L.c2r, h->stream));
+        e = build_nk_f32(h, d_nr);
+    }
+    cudaFree(d_nr);
+    CK(e);
+}
+
+void set_dyn(asd_handle* h, int idx, double v) { CK(launch_set_scalar(h, h->d_dyn + idx, v)); }
+
+void scatter_if_needed(asd_handle* h) {
+    if (h->lr.mode == ASD_LR_NONE || h->p.precision == ASD_FP64_PLAIN || h->lr_scattered) return;
+    CK(launch_lr_scatter_f32(h, h->sf));
+    h->lr_scattered = true;
+}
+
+void destroy_graph(asd_handle* h) {
+    if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_steps = 0; }
+}
+
+// Capture `steps` fused steps + the counter advance into one graph.
+void build_graph(asd_handle* h, uint32_t steps) {
+    destroy_graph(h);
+    cudaGraph_t g;
+    const uint64_t before = h->launches;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (uint32_t r = 0; r < steps && e == cudaSuccess; r++) e = launch_fused_step(h, r, true);
+    if (e == cudaSuccess) e = launch_step_advance(h, steps);
+    cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+    h->graph_launches = h->launches - before;
+    h->launches = before;
+    CK(e);
+    CK(e2);
+    CK(cudaGraphInstantiate(&h->graph, g, 0));
+    cudaGraphDestroy(g);
+    h->graph_steps = steps;
+}
+
+void run_steps(asd_handle* h, uint64_t nsteps) {
+    if (nsteps == 0) return;
+    if (h->p.precision == ASD_FP64_PLAIN) {
+        for (uint64_t q = 0; q < nsteps; q++) CK(launch_plain_step(h, h->step + q));
+        h->step += nsteps;
+        return;
+    }
+    scatter_if_needed(h);
+    set_dyn(h, DYN_DET_STEP, (double)(h->step + nsteps - 1));
+    const uint32_t upd = h->p.update ? h->p.update : 1;
+    const uint32_t G = h->graph_steps;
+    uint64_t left = nsteps;
+    auto direct = [&](uint64_t k) {
+        for (uint64_t r = 0; r < k; r++) CK(launch_fused_step(h, (uint32_t)r, false));
+        CK(launch_step_advance(h, (uint32_t)k));
+        h->step += k;
+    };
+    // align to the dipole refresh period so that one captured chunk fits every chunk
+    if (h->lr.mode == ASD_LR_DIPOLE && h->step % upd) {
+        const uint64_t k = std::min<uint64_t>(left, upd - h->step % upd);
+        direct(k);
+        left -= k;
+    }
+    while (G && left >= G) {
+        CK(cudaGraphLaunch(h->graph, h->stream));
+        h->launches += h->graph_launches;
+        h->step += G;
+        left -= G;
+    }
+    if (left) direct(left);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* asd_version(void) { return "asd-b200 0.1 (sm_100a)"; }
+
+const char* asd_last_error(const asd_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_handle** out) {
+    if (!out) return ASD_EINVAL;
+    *out = nullptr;
+    if (!pp || !sys || nsys == 0) return ASD_EINVAL;
+    asd_handle* h = new asd_handle();
+    h->p = *pp;
+    try {
+        asd_params& p = h->p;
+        if (p.gyro == 0) p.gyro = REF_GYRO;
+        if (p.muB == 0) p.muB = REF_MUB;
+        if (p.kB == 0) p.kB = REF_KB;
+        if (p.update == 0) p.update = 1;
+        REQUIRE(p.integrator <= ASD_RK5, "unknown integrator");
+        REQUIRE(p.precision <= ASD_FP64_FUSED, "unknown precision");
+        REQUIRE(p.dt > 0 && std::isfinite(p.dt), "dt must be positive");
+        CK(cudaGetDevice(&h->device));
+        CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+        // ---- replicas, materials
+        const asd_system& s0 = sys[0];
+        h->nrep = nsys;
+        h->exch = s0.exch;
+        h->full = s0.exch_full ? 1 : 0;
+        h->nmat = s0.nmat;
+        REQUIRE(h->nmat >= 1 && h->nmat <= ASD_MAX_MAT, "nmat must be 1..16");
+        REQUIRE(h->exch <= ASD_EXCH_NONE, "unknown exchange storage");
+        h->h_rep_off.assign(1, 0);
+        uint64_t ntot = 0;
+        for (uint32_t r = 0; r < nsys; r++) {
+            const asd_system& s = sys[r];
+            REQUIRE(s.nspins > 0, "empty lattice");
+            REQUIRE(s.exch == h->exch && (s.exch_full ? 1u : 0u) == h->full, "replicas must share the exchange storage");
+            REQUIRE(s.nmat == h->nmat && s.mat, "replicas must share the material table");
+            for (uint32_t t = 0; t < s.nmat; t++)
+                REQUIRE(memcmp(&s.mat[t], &s0.mat[t], sizeof(asd_material)) == 0, "replicas must share the material table");
+            REQUIRE(s.lr == ASD_LR_NONE || nsys == 1, "long-range field supports one replica per handle");
+            REQUIRE(s.temperature >= 0 && std::isfinite(s.temperature), "temperature must be >= 0");
+            ntot += s.nspins;
+            REQUIRE(ntot < (1ull << 31), "too many spins");
+            h->h_rep_off.push_back((uint32_t)ntot);
+            h->h_rep_T.push_back(s.temperature);
+        }
+        h->n = (uint32_t)ntot;
+        const uint32_t n = h->n;
+        if (s0.lr == ASD_LR_FFT) REQUIRE(h->exch == ASD_EXCH_FFT || h->exch == ASD_EXCH_NONE, "FFT field excludes CSR/DIA exchange");
+        if (h->exch == ASD_EXCH_FFT) REQUIRE(s0.lr == ASD_LR_FFT, "exchange method fft needs lr = ASD_LR_FFT");
+        REQUIRE(!(p.precision == ASD_FP64_FUSED && s0.lr != ASD_LR_NONE), "FP64 fused form has no long-range field; use FP64 plain");
+        // material constants (src/llg.cpp:591-592, src/geom.cpp:244)
+        StepConst& sc = h->sc;
+        sc.n = n; sc.nmat = h->nmat; sc.nrep = nsys; sc.flags = p.flags;
+        const double basemm = s0.mat[0].mu * p.muB;
+        std::vector<uint32_t> subs;
+        for (uint32_t t = 0; t < h->nmat; t++) {
+            const asd_material& m = s0.mat[t];
+            REQUIRE(m.mu > 0 && m.lambda >= 0 && m.gamma > 0, "material needs mu>0, lambda>=0, gamma>0");
+            REQUIRE(m.sublattice < ASD_MAX_SUB, "sublattice index out of range");
+            MatConst& mc = sc.mat[t];
+            mc.llgpf = -1. / (1.0 + m.lambda * m.lambda);
+            mc.lambda = m.lambda;
+            mc.sigma = sqrt(2.0 * p.kB * m.lambda / (m.mu * p.muB * p.dt * m.gamma * p.gyro));
+            mc.k1u = 2.0 * m.k1u / (p.muB * m.mu);
+            for (int a = 0; a < 3; a++) mc.k1udir[a] = m.k1u_dir[a];
+            mc.sub = m.sublattice;
+            h->h_sub_of_mat.push_back(m.sublattice);
+            h->nsub = std::max(h->nsub, m.sublattice + 1);
+        }
+        sc.rdt = p.dt * p.gyro;
+        sc.k2perp_f = 2.0 * p.k2perp / basemm;
+        sc.k2par_f = 2.0 * p.k2par / basemm;
+        sc.k4perp_f = 2.0 * p.k4perp / basemm;
+        sc.k4par_f = 2.0 * p.k4par / basemm;
+        for (int a = 0; a < 3; a++) { sc.k2perpdir[a] = p.k2perpdir[a]; sc.k2pardir[a] = p.k2pardir[a]; }
+        for (int a = 0; a < 9; a++) { sc.k4perpdirs[a] = p.k4perpdirs[a]; sc.k4pardirs[a] = p.k4pardirs[a]; }
+        sc.seed = p.seed;
+        // per-spin atom table (only when not i % nmat)
+        bool need_atom = false;
+        std::vector<uint32_t> atom(n);
+        for (uint32_t r = 0; r < nsys; r++) {
+            const asd_system& s = sys[r];
+            for (uint32_t i = 0; i < s.nspins; i++) {
+                const uint32_t a = s.atom ? s.atom[i] : i % h->nmat;
+                REQUIRE(a < h->nmat, "atom index out of range");
+                atom[h->h_rep_off[r] + i] = a;
+                if (a != (h->h_rep_off[r] + i) % h->nmat) need_atom = true;
+            }
+        }
+        if (need_atom) { h->h_atom = atom; h->d_atom = dupload(atom.data(), n); }
+        sc.atom = h->d_atom;
+        h->d_rep_off = dupload(h->h_rep_off.data(), h->h_rep_off.size());
+        std::vector<double> sq(nsys);
+        std::vector<uint32_t> strm(nsys);
+        for (uint32_t r = 0; r < nsys; r++) { sq[r] = sqrt(h->h_rep_T[r]); strm[r] = sys[r].stream; }
+        h->d_rep_sqrtT = dupload(sq.data(), nsys);
+        h->d_rep_stream = dupload(strm.data(), nsys);
+        sc.rep_off = h->d_rep_off; sc.rep_sqrtT = h->d_rep_sqrtT; sc.rep_stream = h->d_rep_stream;
+        std::vector<double> dyn(DYN_COUNT, 0.0);
+        for (int a = 0; a < 3; a++) dyn[DYN_APPLIED + a] = p.applied[a];
+        dyn[DYN_STAG_SCALE] = 1.0;
+        dyn[DYN_DET_STEP] = -1.0;
+        h->d_dyn = dupload(dyn.data(), dyn.size());
+        h->d_step = dalloc<uint64_t>(1);
+        sc.dyn = h->d_dyn; sc.step_base = h->d_step;
+        // ---- exchange, concatenated over replicas
+        std::vector<uint32_t> xadj(1, 0), adj;
+        std::vector<double> val9;
+        std::vector<int32_t> doff;
+        std::vector<double> dval;  // 9 x ndiag x n
+        if (h->exch == ASD_EXCH_CSR) {
+            for (uint32_t r = 0; r < nsys; r++) {
+                const asd_system& s = sys[r];
+                REQUIRE(s.xadj && (s.nnz == 0 || (s.adjncy && s.csr_val)), "CSR arrays missing");
+                REQUIRE(s.xadj[0] == 0 && s.xadj[s.nspins] == s.nnz, "xadj must start at 0 and end at nnz");
+                const uint32_t off = h->h_rep_off[r], base = (uint32_t)adj.size();
+                for (uint32_t i = 0; i < s.nspins; i++) {
+                    REQUIRE(s.xadj[i + 1] >= s.xadj[i], "xadj must be non-decreasing");
+                    xadj.push_back(base + s.xadj[i + 1]);
+                }
+                for (uint32_t k = 0; k < s.nnz; k++) {
+                    REQUIRE(s.adjncy[k] < s.nspins, "adjncy index out of range");
+                    adj.push_back(off + s.adjncy[k]);
+                    for (int q = 0; q < 9; q++) {
+                        REQUIRE(std::isfinite(s.csr_val[9 * (size_t)k + q]), "non-finite exchange value");
+                        val9.push_back(s.csr_val[9 * (size_t)k + q]);
+                    }
+                }
+            }
+            h->nnz_per_row = (double)adj.size() / n;
+        } else if (h->exch == ASD_EXCH_DIA) {
+            REQUIRE(nsys == 1, "DIA exchange supports one replica per handle");
+            REQUIRE(s0.ndiag == 0 || (s0.dia_offset && s0.dia_val), "DIA arrays missing");
+            doff.assign(s0.dia_offset, s0.dia_offset + s0.ndiag);
+            dval.assign(s0.dia_val, s0.dia_val + 9 * (size_t)s0.ndiag * n);
+            size_t nz = 0;
+            for (uint32_t d = 0; d < s0.ndiag; d++)
+                for (uint32_t i = 0; i < n; i++) {
+                    const int64_t col = (int64_t)i + doff[d];
+                    if (col < 0 || col >= (int64_t)n) continue;
+                    bool any = false;
+                    for (int q = 0; q < 9; q++) any |= dval[(size_t)q * s0.ndiag * n + (size_t)d * n + i] != 0.0;
+                    nz += any;
+                }
+            h->nnz_per_row = (double)nz / n;
+        }
+        const bool plain = p.precision == ASD_FP64_PLAIN;
+        const bool zz_yy = (p.flags & ASD_FLAG_GPU_DZZ_FROM_DYY) != 0;
+        if (plain) {
+            // reference-structured arrays: per-spin parameters, separate component arrays
+            std::vector<double> sig(n), lpf(n), lam(n), k1(n), k1d(3 * (size_t)n);
+            for (uint32_t i = 0; i < n; i++) {
+                const MatConst& mc = sc.mat[atom[i]];
+                sig[i] = mc.sigma; lpf[i] = mc.llgpf; lam[i] = mc.lambda; k1[i] = mc.k1u;
+                for (int a = 0; a < 3; a++) k1d[3 * (size_t)i + a] = mc.k1udir[a];
+            }
+            h->p_sigma = dupload(sig.data(), n); h->p_llgpf = dupload(lpf.data(), n); h->p_lambda = dupload(lam.data(), n);
+            h->p_k1u = dupload(k1.data(), n); h->p_k1udir = dupload(k1d.data(), 3 * (size_t)n);
+            const size_t n3 = 3 * (size_t)n;
+            h->p_s = dalloc<double>(n3); h->p_es = dalloc<double>(n3); h->p_fn = dalloc<double>(n3);
+            h->p_ch = dalloc<double>(n3); h->p_hdemag = dalloc<double>(n3); h->p_rand = dalloc<double>(n3);
+            h->p_det = dalloc<double>(n3); h->p_hstg = dalloc<double>(n3); h->p_hinit = dalloc<double>(n3);
+            if (p.integrator != ASD_HEUN)
+                for (int q = 0; q < (p.integrator == ASD_RK4 ? 4 : 6); q++) h->p_k[q] = dalloc<double>(n3);
+            if (h->exch == ASD_EXCH_CSR) {
+                h->pex.xadj = dupload(xadj.data(), xadj.size());
+                h->pex.adjncy = dupload(adj.data(), adj.size());
+                std::vector<double> comp(adj.size());
+                for (int q = 0; q < 9; q++) {
+                    for (size_t k = 0; k < adj.size(); k++) comp[k] = val9[9 * k + q];
+                    h->pex.v[q] = dupload(comp.data(), comp.size());
+                }
+            } else if (h->exch == ASD_EXCH_DIA) {
+                h->pex.ndiag = s0.ndiag;
+                h->pex.off = dupload(doff.data(), doff.size());
+                const size_t m = (size_t)s0.ndiag * n;
+                for (int q = 0; q < 9; q++) h->pex.v[q] = dupload(dval.data() + q * m, m);
+            }
+            (void)zz_yy;  // applied inside the plain kernels
+        } else {
+            const size_t bytes = p.precision == ASD_FP32 ? 4 : 8;
+            for (int c = 0; c < 3; c++) {
+                if (bytes == 4) {
+                    h->sf[c] = dalloc<float>(n); h->esf[c] = dalloc<float>(n); h->fnf[c] = dalloc<float>(n);
+                    h->detf[c] = dalloc<float>(n);
+                    if (p.flags & ASD_FLAG_COMPENSATED) h->sl[c] = dalloc<float>(n);
+                    if (p.integrator != ASD_HEUN)
+                        for (int q = 0; q < (p.integrator == ASD_RK4 ? 3 : 5); q++) h->kf[q][c] = dalloc<float>(n);
+                } else {
+                    h->sd[c] = dalloc<double>(n); h->esd[c] = dalloc<double>(n); h->fnd[c] = dalloc<double>(n);
+                    h->detd[c] = dalloc<double>(n);
+                    if (p.integrator != ASD_HEUN)
+                        for (int q = 0; q < (p.integrator == ASD_RK4 ? 3 : 5); q++) h->kd[q][c] = dalloc<double>(n);
+                }
+            }
+            if (h->exch == ASD_EXCH_CSR) build_sell(h, xadj, adj, val9);
+            else if (h->exch == ASD_EXCH_DIA) {
+                h->dia.ndiag = s0.ndiag;
+                h->dia.off = dupload(doff.data(), doff.size());
+                const size_t m = (size_t)s0.ndiag * n;
+                const int nc = h->full ? 9 : 3;
+                const int qmap3[3] = {0, 4, zz_yy ? 4 : 8};
+                if (bytes == 4) {
+                    std::vector<float> v(nc * m);
+                    for (int q = 0; q < nc; q++) {
+                        int src = h->full ? (q == 8 && zz_yy ? 4 : q) : qmap3[q];
+                        for (size_t k = 0; k < m; k++) v[q * m + k] = (float)dval[(size_t)src * m + k];
+                    }
+                    h->dia.valf = dupload(v.data(), v.size());
+                } else {
+                    std::vector<double> v(nc * m);
+                    for (int q = 0; q < nc; q++) {
+                        int src = h->full ? (q == 8 && zz_yy ? 4 : q) : qmap3[q];
+                        for (size_t k = 0; k < m; k++) v[q * m + k] = dval[(size_t)src * m + k];
+                    }
+                    h->dia.vald = dupload(v.data(), v.size());
+                }
+            }
+        }
+        // ---- site fields
+        bool any_site = false;
+        for (uint32_t r = 0; r < nsys; r++) any_site |= sys[r].site_field != nullptr;
+        if (any_site) {
+            std::vector<double> prof(3 * (size_t)n, 0.0);
+            for (uint32_t r = 0; r < nsys; r++)
+                if (sys[r].site_field)
+                    std::copy(sys[r].site_field, sys[r].site_field + 3 * (size_t)sys[r].nspins, prof.begin() + 3 * (size_t)h->h_rep_off[r]);
+            if (plain) {
+                CK(cudaMemcpy(h->p_hinit, prof.data(), prof.size() * 8, cudaMemcpyHostToDevice));
+                CK(cudaMemcpy(h->p_hstg, prof.data(), prof.size() * 8, cudaMemcpyHostToDevice));
+            } else {
+                for (int c = 0; c < 3; c++) {
+                    std::vector<double> comp(n);
+                    for (uint32_t i = 0; i < n; i++) comp[i] = prof[3 * (size_t)i + c];
+                    if (p.precision == ASD_FP32) {
+                        std::vector<float> f(comp.begin(), comp.end());
+                        h->stagf[c] = dupload(f.data(), n);
+                    } else {
+                        h->stagd[c] = dupload(comp.data(), n);
+                    }
+                }
+            }
+        }
+        // ---- long-range field
+        if (s0.lr != ASD_LR_NONE) setup_lr(h, s0, plain);
+        // ---- magnetisation buffers
+        {
+            uint32_t maxrep = 0;
+            for (uint32_t r = 0; r < nsys; r++) maxrep = std::max(maxrep, h->h_rep_off[r + 1] - h->h_rep_off[r]);
+            const uint32_t nchunk = (maxrep + 8191) / 8192;
+            h->magpart_len = (size_t)nsys * nchunk * h->nsub * 3;
+            h->d_magpart = dalloc<double>(h->magpart_len);
+            h->d_mag = dalloc<double>((size_t)nsys * h->nsub * 3);
+            std::vector<double> inv((size_t)nsys * h->nsub, 0.0);
+            for (uint32_t r = 0; r < nsys; r++) {
+                std::vector<uint32_t> cnt(h->nsub, 0);
+                for (uint32_t i = h->h_rep_off[r]; i < h->h_rep_off[r + 1]; i++) cnt[h->h_sub_of_mat[atom[i]]]++;
+                for (uint32_t s = 0; s < h->nsub; s++) inv[r * h->nsub + s] = cnt[s] ? 1. / (double)cnt[s] : 0.0;
+            }
+            h->d_inv_count = dupload(inv.data(), inv.size());
+            h->d_sub_of_atom = dupload(h->h_sub_of_mat.data(), h->h_sub_of_mat.size());
+        }
+        // ---- default spins +z, then a graph for the fused forms
+        {
+            std::vector<double> s3(3 * (size_t)n, 0.0);
+            for (uint32_t i = 0; i < n; i++) s3[3 * (size_t)i + 2] = 1.0;
+            int rc = asd_set_spins(h, s3.data(), n);
+            if (rc != ASD_OK) throw Fail{rc, h->err};
+        }
+        CK(cudaEventCreate(&h->kev[0]));
+        CK(cudaEventCreate(&h->kev[1]));
+        if (!plain) {
+            const uint32_t upd = p.update;
+            uint32_t G = 32;
+            if (s0.lr == ASD_LR_DIPOLE) G = upd * std::max<uint32_t>(1, 32 / upd);
+            if (G > 4096) G = upd;
+            build_graph(h, G);
+        }
+        CK(cudaStreamSynchronize(h->stream));
+    } catch (const Fail& f) {
+        std::string msg = f.msg;
+        int code = f.code;
+        free_all(h);
+        delete h;
+        (void)msg;
+        return code;
+    }
+    *out = h;
+    return ASD_OK;
+}
+
+int asd_destroy(asd_handle* h) {
+    if (!h) return ASD_EINVAL;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    free_all(h);
+    delete h;
+    return ASD_OK;
+}
+
+int asd_set_spins(asd_handle* h, const double* s, size_t n_spins) {
+    if (!h) return ASD_EINVAL;
+    try {
+        REQUIRE(s && n_spins == h->n, "spin array must hold 3*nspins doubles");
+        for (size_t q = 0; q < 3 * n_spins; q++)
+            if (!std::isfinite(s[q])) throw Fail{ASD_ENOTFINITE, "non-finite spin component at index " + std::to_string(q)};
+        for (size_t i = 0; i < n_spins; i++) {
+            const double m = s[3 * i] * s[3 * i] + s[3 * i + 1] * s[3 * i + 1] + s[3 * i + 2] * s[3 * i + 2];
+            REQUIRE(m > 1e-24, "zero-length spin at index " + std::to_string(i));
+        }
+        CK(cudaSetDevice(h->device));
+        if (h->p.precision == ASD_FP64_PLAIN) {
+            std::vector<double> v(s, s + 3 * n_spins);
+            for (size_t i = 0; i < n_spins; i++) {
+                const double m = sqrt(v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+                v[3 * i] /= m; v[3 * i + 1] /= m; v[3 * i + 2] /= m;
+            }
+            CK(cudaMemcpyAsync(h->p_s, v.data(), v.size() * 8, cudaMemcpyHostToDevice, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        } else {
+            double* d = dupload(s, 3 * n_spins);
+            cudaError_t e = launch_convert_spins_in(h, d);
+            cudaError_t e2 = cudaStreamSynchronize(h->stream);
+            cudaFree(d);
+            CK(e);
+            CK(e2);
+            h->lr_scattered = false;
+        }
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+static int read_back(asd_handle* h, int what, double* out, size_t n_spins) {
+    try {
+        REQUIRE(out && n_spins == h->n, "output must hold 3*nspins doubles");
+        CK(cudaSetDevice(h->device));
+        const size_t bytes = 3 * n_spins * sizeof(double);
+        if (h->p.precision == ASD_FP64_PLAIN && what != 2) {
+            CK(cudaMemcpyAsync(out, what == 0 ? h->p_s : h->p_det, bytes, cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+            return ASD_OK;
+        }
+        double* d = dalloc<double>(3 * n_spins);
+        cudaError_t e = what == 2 ? launch_field_only(h, d) : launch_convert_out(h, what, d);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, h->stream);
+        cudaError_t e2 = cudaStreamSynchronize(h->stream);
+        cudaFree(d);
+        CK(e);
+        CK(e2);
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_get_spins(asd_handle* h, double* s, size_t n) { return h ? read_back(h, 0, s, n) : ASD_EINVAL; }
+int asd_get_det_field(asd_handle* h, double* o, size_t n) { return h ? read_back(h, 1, o, n) : ASD_EINVAL; }
+int asd_get_field(asd_handle* h, double* o, size_t n) {
+    if (!h) return ASD_EINVAL;
+    try { CK(cudaSetDevice(h->device)); scatter_if_needed(h); } catch (const Fail& f) { return fail(h, f); }
+    return read_back(h, 2, o, n);
+}
+
+int asd_step(asd_handle* h, uint64_t nsteps) {
+    if (!h) return ASD_EINVAL;
+    try {
+        CK(cudaSetDevice(h->device));
+        run_steps(h, nsteps);
+        CK(cudaGetLastError());
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_get_step(const asd_handle* h, uint64_t* t) {
+    if (!h || !t) return ASD_EINVAL;
+    *t = h->step;
+    return ASD_OK;
+}
+
+int asd_set_step(asd_handle* h, uint64_t t) {
+    if (!h) return ASD_EINVAL;
+    try {
+        CK(cudaSetDevice(h->device));
+        CK(cudaMemcpyAsync(h->d_step, &t, sizeof(t), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->step = t;
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_sync(asd_handle* h) {
+    if (!h) return ASD_EINVAL;
+    try { CK(cudaSetDevice(h->device)); CK(cudaStreamSynchronize(h->stream)); } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_set_temperature(asd_handle* h, uint32_t replica, double T) {
+    if (!h) return ASD_EINVAL;
+    try {
+        REQUIRE(T >= 0 && std::isfinite(T), "temperature must be >= 0");
+        REQUIRE(replica == ASD_ALL_REPLICAS || replica < h->nrep, "replica out of range");
+        CK(cudaSetDevice(h->device));
+        for (uint32_t r = 0; r < h->nrep; r++) {
+            if (replica != ASD_ALL_REPLICAS && r != replica) continue;
+            h->h_rep_T[r] = T;
+            CK(launch_set_scalar(h, h->d_rep_sqrtT + r, sqrt(T)));
+        }
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_set_applied(asd_handle* h, const double applied[3]) {
+    if (!h || !applied) return ASD_EINVAL;
+    try {
+        CK(cudaSetDevice(h->device));
+        for (int a = 0; a < 3; a++) {
+            REQUIRE(std::isfinite(applied[a]), "non-finite applied field");
+            h->p.applied[a] = applied[a];
+            set_dyn(h, DYN_APPLIED + a, applied[a]);
+        }
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_set_site_field(asd_handle* h, const double* prof, size_t n_spins) {
+    if (!h) return ASD_EINVAL;
+    try {
+        REQUIRE(prof == nullptr || n_spins == h->n, "site field must hold 3*nspins doubles");
+        CK(cudaSetDevice(h->device));
+        const uint32_t n = h->n;
+        std::vector<double> v(3 * (size_t)n, 0.0);
+        if (prof) v.assign(prof, prof + 3 * (size_t)n);
+        if (h->p.precision == ASD_FP64_PLAIN) {
+            CK(cudaMemcpy(h->p_hinit, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+            CK(cudaMemcpy(h->p_hstg, v.data(), v.size() * 8, cudaMemcpyHostToDevice));
+        } else {
+            bool had = h->stagf[0] || h->stagd[0];
+            for (int c = 0; c < 3; c++) {
+                std::vector<double> comp(n);
+                for (uint32_t i = 0; i < n; i++) comp[i] = v[3 * (size_t)i + c];
+                if (h->p.precision == ASD_FP32) {
+                    std::vector<float> f(comp.begin(), comp.end());
+                    if (!h->stagf[c]) h->stagf[c] = dalloc<float>(n);
+                    CK(cudaMemcpy(h->stagf[c], f.data(), 4 * (size_t)n, cudaMemcpyHostToDevice));
+                } else {
+                    if (!h->stagd[c]) h->stagd[c] = dalloc<double>(n);
+                    CK(cudaMemcpy(h->stagd[c], comp.data(), 8 * (size_t)n, cudaMemcpyHostToDevice));
+                }
+            }
+            if (!had) build_graph(h, h->graph_steps ? h->graph_steps : 32);  // kernels now read the profile
+        }
+        // CsetStagFields resets the ramp: CHstg = CInitHstg
+        set_dyn(h, DYN_STAG_SCALE, 1.0);
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_set_site_field_scale(asd_handle* h, double rv) {
+    if (!h) return ASD_EINVAL;
+    try {
+        REQUIRE(std::isfinite(rv), "non-finite scale");
+        CK(cudaSetDevice(h->device));
+        if (h->p.precision == ASD_FP64_PLAIN) CK(launch_plain_ramp(h, rv));
+        else set_dyn(h, DYN_STAG_SCALE, rv);
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_magnetisation(asd_handle* h, double* out, size_t out_len) {
+    if (!h) return ASD_EINVAL;
+    try {
+        REQUIRE(out && out_len >= (size_t)h->nrep * h->nsub * 3, "output must hold nrep*nsub*3 doubles");
+        CK(cudaSetDevice(h->device));
+        CK(launch_magnetisation(h));
+        CK(cudaMemcpyAsync(out, h->d_mag, (size_t)h->nrep * h->nsub * 3 * 8, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_num_sublattices(const asd_handle* h, uint32_t* nsub) {
+    if (!h || !nsub) return ASD_EINVAL;
+    *nsub = h->nsub;
+    return ASD_OK;
+}
+
+int asd_time_steps(asd_handle* h, uint64_t nsteps, double* ms, uint64_t* launches) {
+    if (!h || !ms) return ASD_EINVAL;
+    try {
+        CK(cudaSetDevice(h->device));
+        CK(cudaStreamSynchronize(h->stream));
+        const uint64_t l0 = h->launches;
+        CK(cudaEventRecord(h->kev[0], h->stream));
+        run_steps(h, nsteps);
+        CK(cudaEventRecord(h->kev[1], h->stream));
+        CK(cudaEventSynchronize(h->kev[1]));
+        float f = 0.f;
+        CK(cudaEventElapsedTime(&f, h->kev[0], h->kev[1]));
+        *ms = f;
+        if (launches) *launches = h->launches - l0;
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_time_kernels(asd_handle* h, uint64_t nsteps) {
+    if (!h) return ASD_EINVAL;
+    try {
+        CK(cudaSetDevice(h->device));
+        CK(cudaStreamSynchronize(h->stream));
+        h->ktimer = KernelTimer{};
+        h->timing = true;
+        const uint32_t G = h->graph_steps;
+        h->graph_steps = 0;  // direct launches so each stage kernel is bracketed by events
+        try { run_steps(h, nsteps); } catch (...) { h->timing = false; h->graph_steps = G; throw; }
+        h->graph_steps = G;
+        h->timing = false;
+        CK(cudaStreamSynchronize(h->stream));
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_kernel_stats(const asd_handle* h, char* name, size_t name_len, double* avg_ms, uint64_t* count,
+                     double* bytes_per_launch) {
+    if (!h) return ASD_EINVAL;
+    if (name && name_len) {
+        snprintf(name, name_len, "%s", h->ktimer.name.c_str());
+    }
+    if (avg_ms) *avg_ms = h->ktimer.count ? h->ktimer.total_ms / h->ktimer.count : 0.0;
+    if (count) *count = h->ktimer.count;
+    if (bytes_per_launch) *bytes_per_launch = h->ktimer.bytes;
+    return ASD_OK;
+}
+
+int asd_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t nspins, double* out) {
+    if (!out || nspins == 0) return ASD_EINVAL;
+    double* d = nullptr;
+    if (cudaMalloc(&d, 3 * (size_t)nspins * sizeof(double)) != cudaSuccess) return ASD_ENOMEM;
+    cudaError_t e = launch_thermal_normals(seed, stream, step, nspins, d, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, 3 * (size_t)nspins * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? ASD_OK : ASD_ECUDA;
+}
+
+}  // extern "C"

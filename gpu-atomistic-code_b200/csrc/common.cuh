@@ -1,0 +1,162 @@
+// Shared device definitions: parameter blocks, the thermal-noise generator and
+// the per-spin field/torque arithmetic used by every stage kernel.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define ASD_MAX_MAT 16
+#define ASD_MAX_SUB 16
+
+namespace asd {
+
+// Per unit-cell atom constants (the reference expands these to per-spin arrays
+// Csigma/Cllgpf/Clambda/Ck1u/Ck1udir, src/cuda_util.cu:497-527; the fused
+// kernels read them from the parameter block instead).
+struct MatConst {
+    double llgpf;    // -1/(1+lambda^2)          (src/llg.cpp:592, 629)
+    double lambda;
+    double sigma;    // sqrt(2 kB lambda/(mu muB dt gamma gyro))  (src/llg.cpp:591)
+    double k1u;      // 2K/(mu muB)               (src/geom.cpp:244)
+    double k1udir[3];
+    uint32_t sub;
+    uint32_t pad;
+};
+
+// Kernel parameter block shared by all stage kernels (passed by value).
+struct StepConst {
+    uint32_t n;         // spins in the handle (all replicas)
+    uint32_t nmat;
+    uint32_t nrep;
+    uint32_t flags;
+    MatConst mat[ASD_MAX_MAT];
+    double rdt;         // dt * gyro (src/llg.cpp:306)
+    double k2perp_f, k2perpdir[3], k2par_f, k2pardir[3];   // 2K/basemm (src/cuint.cu:99)
+    double k4perp_f, k4perpdirs[9], k4par_f, k4pardirs[9];
+    uint64_t seed;
+    const uint32_t* atom;      // per-spin unit-cell atom or nullptr (-> i % nmat)
+    const uint32_t* rep_off;   // nrep+1
+    const double* rep_sqrtT;   // nrep: sqrt(T) per replica
+    const uint32_t* rep_stream;
+    const double* dyn;         // mutable scalars, see DYN_*
+    const uint64_t* step_base; // device step counter
+};
+
+// Layout of the mutable scalar block (device memory, updated between launches).
+enum { DYN_APPLIED = 0, DYN_STAG_SCALE = 3, DYN_DET_STEP = 4, DYN_COUNT = 8 };
+
+__device__ __forceinline__ uint32_t atom_of(const StepConst& c, uint32_t i) {
+    return c.atom ? c.atom[i] : (c.nmat == 1 ? 0u : i % c.nmat);
+}
+
+__device__ __forceinline__ uint32_t replica_of(const StepConst& c, uint32_t i) {
+    uint32_t lo = 0, hi = c.nrep;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(c.rep_off + mid) <= i) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// ---------------------------------------------------------------------------
+// Thermal noise.  Philox4x32-10 (Salmon et al., SC'11) keyed by the seed with
+// counter (spin-in-replica, step_lo, step_hi, stream), then Box-Muller on
+// (u0,u1) and (u2,u3).  log and sincos(2 pi u) are evaluated from their
+// series with correctly rounded intrinsics only (no contraction), so the
+// deviates are bit-identical on any IEEE-754 implementation of the same steps.
+
+__device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        const uint32_t lo0 = 0xD2511F53u * c[0];
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c[0]);
+        const uint32_t lo1 = 0xCD9E8D57u * c[2];
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c[2]);
+        const uint32_t n0 = hi1 ^ c[1] ^ k0;
+        const uint32_t n2 = hi0 ^ c[3] ^ k1;
+        c[0] = n0; c[1] = lo1; c[2] = n2; c[3] = lo0;
+        k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
+    }
+}
+
+// ln x for x in (0,1]: x = m 2^e, m in [sqrt(1/2), sqrt(2)), ln m = 2 atanh(f), f=(m-1)/(m+1).
+__device__ __forceinline__ double series_log(double x) {
+    int e;
+    double m = frexp(x, &e);
+    if (m < 0x1.6a09e667f3bcdp-1) { m = __dmul_rn(m, 2.0); e = e - 1; }
+    const double f = __ddiv_rn(__dsub_rn(m, 1.0), __dadd_rn(m, 1.0));
+    const double f2 = __dmul_rn(f, f);
+    double p = 0x1.642c8590b2164p-5;            // 1/23
+    p = __fma_rn(p, f2, 0x1.8618618618618p-5);  // 1/21
+    p = __fma_rn(p, f2, 0x1.af286bca1af28p-5);  // 1/19
+    p = __fma_rn(p, f2, 0x1.e1e1e1e1e1e1ep-5);  // 1/17
+    p = __fma_rn(p, f2, 0x1.1111111111111p-4);  // 1/15
+    p = __fma_rn(p, f2, 0x1.3b13b13b13b14p-4);  // 1/13
+    p = __fma_rn(p, f2, 0x1.745d1745d1746p-4);  // 1/11
+    p = __fma_rn(p, f2, 0x1.c71c71c71c71cp-4);  // 1/9
+    p = __fma_rn(p, f2, 0x1.2492492492492p-3);  // 1/7
+    p = __fma_rn(p, f2, 0x1.999999999999ap-3);  // 1/5
+    p = __fma_rn(p, f2, 0x1.5555555555555p-2);  // 1/3
+    p = __fma_rn(p, f2, 1.0);
+    const double lnm = __dmul_rn(2.0, __dmul_rn(f, p));
+    return __fma_rn((double)e, 0x1.62e42fefa39efp-1, lnm);
+}
+
+// sin, cos of 2 pi (x+0.5)/2^32: exact octant reduction, Taylor series on [0, pi/4].
+__device__ __forceinline__ void series_sincos_2pi(uint32_t x, double& sn, double& cs) {
+    const double v = __dmul_rn(__dadd_rn((double)x, 0.5), 0x1p-29);
+    const double qd = floor(v);
+    const int q = (int)qd;
+    const double r = __dsub_rn(v, qd);
+    const double psi = __dmul_rn((q & 1) ? __dsub_rn(1.0, r) : r, 0x1.921fb54442d18p-1);
+    const double p2 = __dmul_rn(psi, psi);
+    const double mp2 = -p2;
+    double sp = 0x1.2f49b46814157p-57;            // 1/19!
+    sp = __fma_rn(sp, mp2, 0x1.952c77030ad4ap-49); // 1/17!
+    sp = __fma_rn(sp, mp2, 0x1.ae7f3e733b81fp-41); // 1/15!
+    sp = __fma_rn(sp, mp2, 0x1.6124613a86d09p-33); // 1/13!
+    sp = __fma_rn(sp, mp2, 0x1.ae64567f544e4p-26); // 1/11!
+    sp = __fma_rn(sp, mp2, 0x1.71de3a556c734p-19); // 1/9!
+    sp = __fma_rn(sp, mp2, 0x1.a01a01a01a01ap-13); // 1/7!
+    sp = __fma_rn(sp, mp2, 0x1.1111111111111p-7);  // 1/5!
+    sp = __fma_rn(sp, mp2, 0x1.5555555555555p-3);  // 1/3!
+    sp = __fma_rn(sp, mp2, 1.0);
+    const double s = __dmul_rn(psi, sp);
+    double cp = 0x1.6827863b97d97p-53;            // 1/18!
+    cp = __fma_rn(cp, mp2, 0x1.ae7f3e733b81fp-45); // 1/16!
+    cp = __fma_rn(cp, mp2, 0x1.93974a8c07c9dp-37); // 1/14!
+    cp = __fma_rn(cp, mp2, 0x1.1eed8eff8d898p-29); // 1/12!
+    cp = __fma_rn(cp, mp2, 0x1.27e4fb7789f5cp-22); // 1/10!
+    cp = __fma_rn(cp, mp2, 0x1.a01a01a01a01ap-16); // 1/8!
+    cp = __fma_rn(cp, mp2, 0x1.6c16c16c16c17p-10); // 1/6!
+    cp = __fma_rn(cp, mp2, 0x1.5555555555555p-5);  // 1/4!
+    cp = __fma_rn(cp, mp2, 0x1.0000000000000p-1);  // 1/2!
+    const double c = __fma_rn(cp, mp2, 1.0);
+    switch (q) {
+    case 0: sn = s;  cs = c;  break;
+    case 1: sn = c;  cs = s;  break;
+    case 2: sn = c;  cs = -s; break;
+    case 3: sn = s;  cs = -c; break;
+    case 4: sn = -s; cs = -c; break;
+    case 5: sn = -c; cs = -s; break;
+    case 6: sn = -c; cs = s;  break;
+    default: sn = -s; cs = c; break;
+    }
+}
+
+__device__ __forceinline__ void thermal_normals(uint64_t seed, uint32_t stream, uint32_t spin, uint64_t step,
+                                                double out[3]) {
+    uint32_t c[4] = {spin, (uint32_t)step, (uint32_t)(step >> 32), stream};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const double u0 = __dmul_rn(__dadd_rn((double)c[0], 0.5), 0x1p-32);
+    const double u2 = __dmul_rn(__dadd_rn((double)c[2], 0.5), 0x1p-32);
+    const double r0 = __dsqrt_rn(__dmul_rn(-2.0, series_log(u0)));
+    const double r2 = __dsqrt_rn(__dmul_rn(-2.0, series_log(u2)));
+    double s1, c1, s3, c3;
+    series_sincos_2pi(c[1], s1, c1);
+    series_sincos_2pi(c[3], s3, c3);
+    out[0] = __dmul_rn(r0, c1);
+    out[1] = __dmul_rn(r0, s1);
+    out[2] = __dmul_rn(r2, c3);
+}
+
+}  // namespace asd

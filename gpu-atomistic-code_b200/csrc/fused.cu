@@ -1,0 +1,426 @@
+// Fused stage kernels: one bandwidth-bound pass per integrator stage that
+// gathers the exchange field (SELL-32 or DIA layout), adds the long-range,
+// site, thermal (in-kernel Philox), applied and anisotropy fields, forms the
+// LLG torque and writes the next stage spin renormalised in FP64.  The same
+// templates serve the FP32 form (R=float) and the fused FP64 form (R=double).
+//
+// Reference computation per stage: the field kernel CSpMV_* / CCopyFields
+// (src/cufields.cu:97-246, 386-407) followed by CHeun1/CHeun2
+// (src/cuint.cu:60-242) or CdetRK4k*/CdetRK5k* + CdetSnp1
+// (src/cuintRK4.cu:62-457, src/cuintRK5.cu:79-651).
+#include "internal.h"
+
+namespace asd {
+namespace {
+
+template <typename R>
+struct Vec3 { R* p[3]; };
+template <typename R>
+struct CVec3 { const R* p[3]; };
+
+struct LrArgs {
+    const float* hr;            // padded real field [3][P] to gather (nullptr: none)
+    float inv_p;
+    float* mr;                  // padded real input [3][P] to scatter the output spins into (nullptr: none)
+    const float* w;             // per-spin weight for the scatter
+    const uint32_t* idx;        // per-spin mesh index
+    size_t P;
+};
+
+template <typename R>
+struct StageArgs {
+    CVec3<R> src;        // spins the field is gathered from (S or a stage spin)
+    CVec3<R> base;       // S (hi part)
+    CVec3<float> base_lo;// S lo part (compensated storage) or nullptrs
+    Vec3<R> out;         // next stage spin or new S (hi)
+    Vec3<float> out_lo;  // new S lo part
+    Vec3<R> fn;          // Heun f_n (stage 1 writes, stage 2 reads)
+    Vec3<R> det;         // det field (stage 2, at the det step)
+    CVec3<R> stag;       // site-field profile or nullptrs
+    Vec3<R> k[6];        // RK stage increments
+    int kind;            // 1: Heun predictor, 2: Heun corrector, 10+st: RK stage st
+    int nst;             // RK stages
+    uint32_t rel;        // step offset inside a graph chunk
+    LrArgs lr;
+};
+
+template <typename T>
+__device__ __forceinline__ T ldcs(const T* p) { return __ldcs(p); }
+
+// Exchange field from the SELL-32 layout.
+template <typename R, bool FULL>
+__device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t n, uint32_t i, const CVec3<R>& s, R h[3]) {
+    const uint32_t sl = i >> 5, lane = i & 31u;
+    const uint32_t p0 = __ldg(m.slice_ptr + sl), p1 = __ldg(m.slice_ptr + sl + 1);
+    if constexpr (sizeof(R) == 4) {
+#pragma unroll 2
+        for (uint32_t e = p0 + lane; e < p1; e += 32) {
+            const float4 a = ldcs(m.a + e);
+            const int j = __float_as_int(a.x);
+            const float x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
+            if (!FULL) {
+                h[0] = fmaf(a.y, x, h[0]);
+                h[1] = fmaf(a.z, y, h[1]);
+                h[2] = fmaf(a.w, z, h[2]);
+            } else {
+                const float4 b = ldcs(m.b + e);
+                const float2 c = ldcs(m.c + e);
+                h[0] = fmaf(a.y, x, fmaf(a.z, y, fmaf(a.w, z, h[0])));
+                h[1] = fmaf(b.x, x, fmaf(b.y, y, fmaf(b.z, z, h[1])));
+                h[2] = fmaf(b.w, x, fmaf(c.x, y, fmaf(c.y, z, h[2])));
+            }
+        }
+    } else {
+        const uint32_t E = m.entries;
+        for (uint32_t e = p0 + lane; e < p1; e += 32) {
+            const int j = ldcs(m.col + e);
+            const double x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
+            if (!FULL) {
+                h[0] += ldcs(m.val + e) * x;
+                h[1] += ldcs(m.val + E + e) * y;
+                h[2] += ldcs(m.val + 2 * (size_t)E + e) * z;
+            } else {
+                const double* v = m.val;
+                h[0] += ldcs(v + e) * x + ldcs(v + E + e) * y + ldcs(v + 2 * (size_t)E + e) * z;
+                h[1] += ldcs(v + 3 * (size_t)E + e) * x + ldcs(v + 4 * (size_t)E + e) * y + ldcs(v + 5 * (size_t)E + e) * z;
+                h[2] += ldcs(v + 6 * (size_t)E + e) * x + ldcs(v + 7 * (size_t)E + e) * y + ldcs(v + 8 * (size_t)E + e) * z;
+            }
+        }
+    }
+    (void)n;
+}
+
+// Exchange field from the row-aligned DIA layout.
+template <typename R, bool FULL>
+__device__ __forceinline__ void gather_dia(const DiaDev& m, uint32_t n, uint32_t i, const CVec3<R>& s, R h[3]) {
+    const size_t ND = (size_t)m.ndiag * n;
+    const R* v;
+    if constexpr (sizeof(R) == 4) v = m.valf; else v = m.vald;
+    for (uint32_t d = 0; d < m.ndiag; d++) {
+        const int64_t col = (int64_t)i + __ldg(m.off + d);
+        if (col < 0 || col >= (int64_t)n) continue;
+        const size_t a = (size_t)d * n + i;
+        const R x = __ldg(s.p[0] + col), y = __ldg(s.p[1] + col), z = __ldg(s.p[2] + col);
+        if (!FULL) {
+            h[0] += ldcs(v + a) * x;
+            h[1] += ldcs(v + ND + a) * y;
+            h[2] += ldcs(v + 2 * ND + a) * z;
+        } else {
+            h[0] += ldcs(v + a) * x + ldcs(v + ND + a) * y + ldcs(v + 2 * ND + a) * z;
+            h[1] += ldcs(v + 3 * ND + a) * x + ldcs(v + 4 * ND + a) * y + ldcs(v + 5 * ND + a) * z;
+            h[2] += ldcs(v + 6 * ND + a) * x + ldcs(v + 7 * ND + a) * y + ldcs(v + 8 * ND + a) * z;
+        }
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void anis_field(const StepConst& c, const MatConst& mc, const R s[3], R h[3]) {
+    const R d0 = (R)mc.k1udir[0], d1 = (R)mc.k1udir[1], d2 = (R)mc.k1udir[2];
+    const R k1 = (R)mc.k1u * (s[0] * d0 + s[1] * d1 + s[2] * d2);
+    h[0] += k1 * d0; h[1] += k1 * d1; h[2] += k1 * d2;
+    if (c.k2perp_f != 0.0) {
+        const R* dd = nullptr; (void)dd;
+        const R a0 = (R)c.k2perpdir[0], a1 = (R)c.k2perpdir[1], a2 = (R)c.k2perpdir[2];
+        const R t = (R)c.k2perp_f * (s[0] * a0 + s[1] * a1 + s[2] * a2);
+        h[0] += t * a0; h[1] += t * a1; h[2] += t * a2;
+    }
+    if (c.k2par_f != 0.0) {
+        const R a0 = (R)c.k2pardir[0], a1 = (R)c.k2pardir[1], a2 = (R)c.k2pardir[2];
+        const R t = (R)c.k2par_f * (s[0] * a0 + s[1] * a1 + s[2] * a2);
+        h[0] += t * a0; h[1] += t * a1; h[2] += t * a2;
+    }
+    if (c.k4perp_f != 0.0 || c.k4par_f != 0.0) {
+#pragma unroll
+        for (int dir = 0; dir < 3; dir++) {
+            const R p0 = (R)c.k4perpdirs[3 * dir], p1 = (R)c.k4perpdirs[3 * dir + 1], p2 = (R)c.k4perpdirs[3 * dir + 2];
+            const R q0 = (R)c.k4pardirs[3 * dir], q1 = (R)c.k4pardirs[3 * dir + 1], q2 = (R)c.k4pardirs[3 * dir + 2];
+            const R tp = (R)c.k4perp_f * (s[0] * p0 + s[1] * p1 + s[2] * p2);
+            const R tq = (R)c.k4par_f * (s[0] * q0 + s[1] * q1 + s[2] * q2);
+            h[0] += tp * p0 + tq * q0; h[1] += tp * p1 + tq * q1; h[2] += tp * p2 + tq * q2;
+        }
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void llg_rhs(R llgpf, R lambda, const R s[3], const R h[3], R f[3]) {
+    const R a0 = s[1] * h[2] - s[2] * h[1], a1 = s[2] * h[0] - s[0] * h[2], a2 = s[0] * h[1] - s[1] * h[0];
+    const R b0 = s[1] * a2 - s[2] * a1, b1 = s[2] * a0 - s[0] * a2, b2 = s[0] * a1 - s[1] * a0;
+    f[0] = llgpf * (a0 + lambda * b0);
+    f[1] = llgpf * (a1 + lambda * b1);
+    f[2] = llgpf * (a2 + lambda * b2);
+}
+
+__device__ __forceinline__ void renorm(double v[3]) {
+    const double inv = 1.0 / sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    v[0] *= inv; v[1] *= inv; v[2] *= inv;
+}
+
+__constant__ double FRK5B[5][5] = {
+    {0.2, 0, 0, 0, 0},
+    {3.0 / 40.0, 9.0 / 40.0, 0, 0, 0},
+    {0.3, -0.9, 1.2, 0, 0},
+    {-11.0 / 54, 2.5, -70.0 / 27.0, 35.0 / 27.0, 0},
+    {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+__constant__ double FRK5C[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
+__constant__ double FRK4C[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
+
+template <typename R, int EX, bool FULL, bool COMP>
+__global__ void __launch_bounds__(256) stage_kernel(const StepConst c, const SellDev sell, const DiaDev dia,
+                                                     const StageArgs<R> a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    const uint64_t t = *c.step_base + a.rel;
+    R h[3] = {R(0), R(0), R(0)};
+    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, c.n, i, a.src, h);
+    if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, a.src, h);
+    uint32_t midx = 0;
+    if (a.lr.hr || a.lr.mr) midx = __ldg(a.lr.idx + i);
+    if (a.lr.hr) {
+        h[0] += (R)(__ldg(a.lr.hr + midx) * a.lr.inv_p);
+        h[1] += (R)(__ldg(a.lr.hr + a.lr.P + midx) * a.lr.inv_p);
+        h[2] += (R)(__ldg(a.lr.hr + 2 * a.lr.P + midx) * a.lr.inv_p);
+    }
+    const uint32_t at = atom_of(c, i);
+    const MatConst& mc = c.mat[at];
+    const uint32_t r = replica_of(c, i);
+    const double sqrtT = __ldg(c.rep_sqrtT + r);
+    R lrn[3] = {R(0), R(0), R(0)};
+    if (sqrtT > 0.0) {
+        double xi[3];
+        thermal_normals(c.seed, __ldg(c.rep_stream + r), i - __ldg(c.rep_off + r), t, xi);
+        const double tp = sqrtT * mc.sigma;
+        lrn[0] = (R)(xi[0] * tp); lrn[1] = (R)(xi[1] * tp); lrn[2] = (R)(xi[2] * tp);
+    }
+    const double* dyn = c.dyn;
+    if (a.stag.p[0]) {
+        const R sc = (R)dyn[DYN_STAG_SCALE];
+        h[0] += sc * a.stag.p[0][i]; h[1] += sc * a.stag.p[1][i]; h[2] += sc * a.stag.p[2][i];
+    }
+    h[0] += lrn[0] + (R)dyn[DYN_APPLIED];
+    h[1] += lrn[1] + (R)dyn[DYN_APPLIED + 1];
+    h[2] += lrn[2] + (R)dyn[DYN_APPLIED + 2];
+
+    // stage spin at this site
+    R sv[3] = {a.src.p[0][i], a.src.p[1][i], a.src.p[2][i]};
+    const int kind = a.kind;
+    if (kind >= 11 && (c.flags & ASD_FLAG_RK_STAGE_SPIN_MIXED)) { sv[1] = a.base.p[1][i]; sv[2] = a.base.p[2][i]; }
+    anis_field<R>(c, mc, sv, h);
+    R f[3];
+    llg_rhs<R>((R)mc.llgpf, (R)mc.lambda, sv, h, f);
+
+    // the new S needs the full-precision base; intermediate stage spins use the hi part
+    const bool final_spin = kind == 2 || (kind >= 10 && kind - 10 == a.nst - 1);
+    double S[3] = {(double)a.base.p[0][i], (double)a.base.p[1][i], (double)a.base.p[2][i]};
+    if constexpr (COMP) {
+        if (final_spin) { S[0] += (double)a.base_lo.p[0][i]; S[1] += (double)a.base_lo.p[1][i]; S[2] += (double)a.base_lo.p[2][i]; }
+    }
+    const double rdt = c.rdt;
+    double o[3];
+    if (kind == 1) {
+        for (int j = 0; j < 3; j++) { a.fn.p[j][i] = f[j]; o[j] = S[j] + rdt * (double)f[j]; }
+    } else if (kind == 2) {
+        for (int j = 0; j < 3; j++) o[j] = S[j] + 0.5 * rdt * ((double)a.fn.p[j][i] + (double)f[j]);
+        if ((double)t == dyn[DYN_DET_STEP])
+            for (int j = 0; j < 3; j++) a.det.p[j][i] = h[j] - lrn[j];
+    } else {
+        const int st = kind - 10, nst = a.nst;
+        const bool dbl = (c.flags & ASD_FLAG_RK_DOUBLE_RDT) != 0;
+        double k[3];
+        for (int j = 0; j < 3; j++) k[j] = rdt * (double)f[j];
+        if (st < nst - 1) {
+            for (int j = 0; j < 3; j++) a.k[st].p[j][i] = (R)k[j];
+            for (int j = 0; j < 3; j++) {
+                double inc;
+                if (nst == 4) {
+                    inc = k[j] * (st == 2 ? 1.0 : 0.5);
+                } else {
+                    inc = FRK5B[st][st] * k[j];
+                    for (int b = 0; b < st; b++) inc += FRK5B[st][b] * (double)a.k[b].p[j][i];
+                }
+                o[j] = S[j] + (dbl ? rdt * inc : inc);
+            }
+        } else {
+            const double* C = nst == 4 ? FRK4C : FRK5C;
+            for (int j = 0; j < 3; j++) {
+                double acc = C[st] * k[j];
+                for (int b = 0; b < st; b++) acc += C[b] * (double)a.k[b].p[j][i];
+                o[j] = S[j] + acc;
+            }
+        }
+    }
+    renorm(o);
+    for (int j = 0; j < 3; j++) {
+        const R hi = (R)o[j];
+        a.out.p[j][i] = hi;
+        if constexpr (COMP) { if (final_spin) a.out_lo.p[j][i] = (float)(o[j] - (double)hi); }
+    }
+    if (a.lr.mr) {
+        const float wv = __ldg(a.lr.w + i);
+        a.lr.mr[midx] = (float)o[0] * wv;
+        a.lr.mr[a.lr.P + midx] = (float)o[1] * wv;
+        a.lr.mr[2 * a.lr.P + midx] = (float)o[2] * wv;
+    }
+}
+
+__global__ void advance_k(uint64_t* step, uint32_t n) { *step += n; }
+
+template <typename R>
+Vec3<R> v3(R* const p[3]) { return Vec3<R>{{p[0], p[1], p[2]}}; }
+template <typename R>
+CVec3<R> c3(R* const p[3]) { return CVec3<R>{{p[0], p[1], p[2]}}; }
+
+// Bytes one stage launch must move (algorithmic: each array element once,
+// gathered neighbour spins counted once, the matrix at its nnz).
+template <typename R>
+double stage_bytes(const asd_handle* h, const StageArgs<R>& a, bool comp) {
+    const double vb = sizeof(R), n = h->n;
+    const double c = h->full ? 9.0 : 3.0;
+    double m = 0.0;
+    if (h->exch == ASD_EXCH_CSR) m = 4.0 + h->nnz_per_row * (4.0 + vb * c);
+    else if (h->exch == ASD_EXCH_DIA) m = h->nnz_per_row * vb * c;
+    double st = 3 * vb;                                  // src spin (gathered once)
+    const int kind = a.kind;
+    const bool final_spin = kind == 2 || (kind >= 10 && kind - 10 == a.nst - 1);
+    if (kind != 1 && kind != 10) st += 3 * vb;           // base S differs from src
+    st += 3 * vb;                                        // output spin
+    if (kind == 1) st += 3 * vb;                         // f_n written
+    if (kind == 2) st += 3 * vb;                         // f_n read
+    if (kind >= 10) {
+        const int s = kind - 10;
+        if (s < a.nst - 1) st += 3 * vb;                 // k_s written
+        const int reads = a.nst == 4 ? (s == a.nst - 1 ? s : 0) : s;
+        st += reads * 3 * vb;                            // earlier k read
+    }
+    if (comp && final_spin) st += 24;                    // lo part read + written
+    if (a.stag.p[0]) st += 3 * vb;
+    if (a.lr.hr) st += 12;
+    if (a.lr.mr) st += 12;
+    return n * (m + st);
+}
+
+template <typename R, int EX, bool FULL, bool COMP>
+cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
+    const int B = hd->block;
+    const unsigned grid = (hd->n + B - 1) / B;
+    if (hd->timing) cudaEventRecord(hd->kev[0], hd->stream);
+    stage_kernel<R, EX, FULL, COMP><<<grid, B, 0, hd->stream>>>(hd->sc, hd->sell, hd->dia, a);
+    hd->launches += 1;
+    if (hd->timing) {
+        cudaEventRecord(hd->kev[1], hd->stream);
+        cudaEventSynchronize(hd->kev[1]);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, hd->kev[0], hd->kev[1]);
+        KernelTimer& kt = hd->ktimer;
+        const double b = stage_bytes<R>(hd, a, COMP);
+        kt.bytes = (kt.bytes * kt.count + b) / (double)(kt.count + 1);
+        kt.total_ms += ms;
+        kt.count += 1;
+        kt.name = std::string("stage_kernel<") + (sizeof(R) == 4 ? "float" : "double") + "," +
+                  (EX == ASD_EXCH_CSR ? "SELL32" : EX == ASD_EXCH_DIA ? "DIA" : "NONE") + (FULL ? ",full" : ",diag") +
+                  (COMP ? ",comp>" : ">");
+    }
+    return cudaGetLastError();
+}
+
+template <typename R, bool COMP>
+cudaError_t launch_stage(asd_handle* hd, const StageArgs<R>& a) {
+    if (hd->exch == ASD_EXCH_CSR) {
+        return hd->full ? launch_stage_t<R, ASD_EXCH_CSR, true, COMP>(hd, a) : launch_stage_t<R, ASD_EXCH_CSR, false, COMP>(hd, a);
+    } else if (hd->exch == ASD_EXCH_DIA) {
+        return hd->full ? launch_stage_t<R, ASD_EXCH_DIA, true, COMP>(hd, a) : launch_stage_t<R, ASD_EXCH_DIA, false, COMP>(hd, a);
+    }
+    return launch_stage_t<R, ASD_EXCH_NONE, false, COMP>(hd, a);
+}
+
+template <typename R>
+void state_ptrs(asd_handle* h, R* const** s, R* const** es, R* const** fn, R* const** det, R* const** stag) {
+    if constexpr (sizeof(R) == 4) { *s = h->sf; *es = h->esf; *fn = h->fnf; *det = h->detf; *stag = h->stagf; }
+    else { *s = h->sd; *es = h->esd; *fn = h->fnd; *det = h->detd; *stag = h->stagd; }
+}
+
+template <typename R>
+cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
+    R* const* s; R* const* es; R* const* fn; R* const* det; R* const* stag;
+    state_ptrs<R>(h, &s, &es, &fn, &det, &stag);
+    const bool comp = sizeof(R) == 4 && (h->p.flags & ASD_FLAG_COMPENSATED);
+    StageArgs<R> a{};
+    a.base = c3<R>(s);
+    if (comp) a.base_lo = CVec3<float>{{h->sl[0], h->sl[1], h->sl[2]}};
+    if (stag[0]) a.stag = c3<R>(stag);
+    a.rel = rel;
+    const uint64_t t = h->step + rel;
+    const uint32_t upd = h->p.update ? h->p.update : 1;
+    LongRange& L = h->lr;
+    LrArgs none{};
+    none.P = L.P; none.idx = L.mesh_idx; none.w = L.w; none.inv_p = L.P ? 1.0f / (float)L.P : 0.f;
+    cudaError_t e;
+    auto run = [&](const StageArgs<R>& aa) { return comp ? launch_stage<R, true>(h, aa) : launch_stage<R, false>(h, aa); };
+    if (h->p.integrator == ASD_HEUN) {
+        // predictor
+        a.src = c3<R>(s); a.out = v3<R>(es); a.fn = v3<R>(fn); a.kind = 1;
+        a.lr = none;
+        if (L.mode == ASD_LR_FFT) {
+            if ((e = launch_lr_eval_f32(h)) != cudaSuccess) return e;   // field of S (scattered before)
+            a.lr.hr = L.r + 3 * L.P; a.lr.mr = L.r;                    // gather H(S), scatter S'
+        } else if (L.mode == ASD_LR_DIPOLE) {
+            if (t % upd == 0 && (e = launch_lr_eval_f32(h)) != cudaSuccess) return e;
+            a.lr.hr = L.r + 3 * L.P;
+        }
+        if ((e = run(a)) != cudaSuccess) return e;
+        // corrector
+        a.src = c3<R>(es); a.out = v3<R>(s); a.kind = 2; a.det = v3<R>(det);
+        if (comp) a.out_lo = Vec3<float>{{h->sl[0], h->sl[1], h->sl[2]}};
+        a.lr = none;
+        if (L.mode == ASD_LR_FFT) {
+            if ((e = launch_lr_eval_f32(h)) != cudaSuccess) return e;   // field of S'
+            a.lr.hr = L.r + 3 * L.P; a.lr.mr = L.r;                    // gather H(S'), scatter S_{n+1}
+        } else if (L.mode == ASD_LR_DIPOLE) {
+            a.lr.hr = L.r + 3 * L.P;
+            if ((t + 1) % upd == 0) a.lr.mr = L.r;                     // next step refreshes from S_{n+1}
+        }
+        return run(a);
+    }
+    const int nst = h->p.integrator == ASD_RK4 ? 4 : 6;
+    a.nst = nst;
+    R* const* pp[2] = {es, fn};  // stage spins ping-pong between the es and fn buffers
+    if (L.mode == ASD_LR_DIPOLE && t % upd == 0 && (e = launch_lr_eval_f32(h)) != cudaSuccess) return e;
+    for (int st = 0; st < nst; st++) {
+        a.kind = 10 + st;
+        a.src = st == 0 ? c3<R>(s) : c3<R>(pp[(st - 1) & 1]);
+        for (int q = 0; q < 6; q++) {
+            if constexpr (sizeof(R) == 4) a.k[q] = v3<R>(h->kf[q]); else a.k[q] = v3<R>(h->kd[q]);
+        }
+        a.lr = none;
+        if (L.mode == ASD_LR_FFT) {
+            if (st > 0 && (e = launch_lr_eval_f32(h)) != cudaSuccess) return e;
+            if (st == 0 && (e = launch_lr_eval_f32(h)) != cudaSuccess) return e;
+            a.lr.hr = L.r + 3 * L.P; a.lr.mr = L.r;
+        } else if (L.mode == ASD_LR_DIPOLE) {
+            a.lr.hr = L.r + 3 * L.P;
+            if (st == nst - 1 && (t + 1) % upd == 0) a.lr.mr = L.r;
+        }
+        if (st == nst - 1) {
+            a.out = v3<R>(s);
+            if (comp) a.out_lo = Vec3<float>{{h->sl[0], h->sl[1], h->sl[2]}};
+        } else {
+            a.out = v3<R>(pp[st & 1]);
+        }
+        if ((e = run(a)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t launch_fused_step(asd_handle* h, uint32_t rel, bool) {
+    if (h->p.precision == ASD_FP32) return fused_step_t<float>(h, rel);
+    return fused_step_t<double>(h, rel);
+}
+
+cudaError_t launch_step_advance(asd_handle* h, uint32_t nsteps) {
+    advance_k<<<1, 1, 0, h->stream>>>(h->d_step, nsteps);
+    h->launches += 1;
+    return cudaGetLastError();
+}
+
+}  // namespace asd

@@ -1,0 +1,144 @@
+// Host-side handle and the launch interface between api.cpp and the kernels.
+#pragma once
+#include "../../include/asd.h"
+#include "common.cuh"
+#include <cufft.h>
+#include <string>
+#include <vector>
+
+namespace asd {
+
+// Device layouts of the exchange matrix.
+//  SELL-32 (sliced ELLPACK, slice height = warp size) for CSR input: rows are
+//  grouped in slices of 32; entry (slice s, k, lane) sits at slice_ptr[s] + 32k + lane,
+//  so one warp reads 32 consecutive entries per k.  Padding entries point at the
+//  row itself with zero tensor.
+//  Float: diagonal form packs (col, xx, yy, zz) in one float4; full form packs
+//  (col, m00, m01, m02), (m10, m11, m12, m20), (m21, m22) in float4+float4+float2.
+//  Double: col[E] plus component-major values val[c][E].
+struct SellDev {
+    uint32_t nslices = 0, entries = 0;
+    uint32_t* slice_ptr = nullptr;
+    float4* a = nullptr;
+    float4* b = nullptr;
+    float2* c = nullptr;
+    int32_t* col = nullptr;
+    double* val = nullptr;
+};
+
+// Row-aligned DIA, values component-major val[c][d*N+row], c = 3 (diag) or 9.
+struct DiaDev {
+    uint32_t ndiag = 0;
+    int32_t* off = nullptr;
+    float* valf = nullptr;
+    double* vald = nullptr;
+};
+
+// Reference-structured CSR / DIA for the FP64 plain form (separate component arrays).
+struct PlainExch {
+    uint32_t* xadj = nullptr;
+    uint32_t* adjncy = nullptr;
+    double* v[9] = {nullptr};
+    uint32_t ndiag = 0;
+    int32_t* off = nullptr;
+};
+
+// Long-range field buffers (zero-padded mesh, FP32 R2C/C2R or FP64 C2C plain).
+struct LongRange {
+    int mode = ASD_LR_NONE;
+    uint32_t mesh[3] = {0, 0, 0};
+    size_t P = 0, Pk = 0;          // padded real sites, half-spectrum points
+    uint32_t ncomp = 6;            // 6 (symmetric) or 9 components of N_k
+    int nk_real = 1;               // N_k purely real (even N_r)
+    uint32_t* mesh_idx = nullptr;  // per spin linear mesh index
+    float* w = nullptr;            // per spin weight (mu for dipole, 1 for FFT exchange)
+    float* r = nullptr;            // [3][P] padded real input / output
+    float2* k = nullptr;           // [3][Pk]
+    float* nkr = nullptr;          // [ncomp][Pk] real N_k
+    float2* nkc = nullptr;         // [ncomp][Pk] complex N_k
+    cufftHandle r2c = 0, c2r = 0;
+    // FP64 plain: complex padded arrays [3][P] and full complex N_k [9][P]
+    double2 *zr = nullptr, *zk = nullptr, *zh = nullptr, *znk = nullptr;
+    cufftHandle z2z = 0;
+};
+
+struct KernelTimer {
+    std::string name;
+    double total_ms = 0.0;
+    uint64_t count = 0;
+    double bytes = 0.0;
+};
+
+}  // namespace asd
+
+struct asd_handle {
+    asd_params p{};
+    std::string err;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t n = 0, nrep = 0, nmat = 0, nsub = 1;
+    uint32_t exch = ASD_EXCH_NONE, full = 0;
+    uint64_t step = 0;
+    uint64_t launches = 0;
+    asd::StepConst sc{};
+    std::vector<uint32_t> h_rep_off;
+    std::vector<double> h_rep_T;
+    std::vector<uint32_t> h_atom;      // empty -> i % nmat
+    std::vector<uint32_t> h_sub_of_mat;
+    // device: replica tables, atoms, mutable scalars
+    uint32_t *d_rep_off = nullptr, *d_rep_stream = nullptr, *d_atom = nullptr;
+    double *d_rep_sqrtT = nullptr, *d_dyn = nullptr;
+    uint64_t* d_step = nullptr;
+    // FP32 / FP64-fused state, SoA
+    float *sf[3] = {nullptr}, *sl[3] = {nullptr}, *esf[3] = {nullptr}, *fnf[3] = {nullptr};
+    float *kf[6][3] = {{nullptr}};
+    float *detf[3] = {nullptr}, *stagf[3] = {nullptr};
+    double *sd[3] = {nullptr}, *esd[3] = {nullptr}, *fnd[3] = {nullptr}, *kd[6][3] = {{nullptr}};
+    double *detd[3] = {nullptr}, *stagd[3] = {nullptr};
+    asd::SellDev sell;
+    asd::DiaDev dia;
+    // FP64 plain (AoS [3i+c], reference-structured)
+    double *p_s = nullptr, *p_es = nullptr, *p_fn = nullptr, *p_ch = nullptr, *p_hdemag = nullptr, *p_rand = nullptr,
+           *p_det = nullptr, *p_hstg = nullptr, *p_hinit = nullptr, *p_k[6] = {nullptr};
+    double *p_sigma = nullptr, *p_llgpf = nullptr, *p_lambda = nullptr, *p_k1u = nullptr, *p_k1udir = nullptr;
+    asd::PlainExch pex;
+    asd::LongRange lr;
+    // reductions
+    double* d_magpart = nullptr;
+    size_t magpart_len = 0;
+    double* d_mag = nullptr;
+    double* d_inv_count = nullptr;
+    uint32_t* d_sub_of_atom = nullptr;
+    uint64_t graph_launches = 0;
+    bool lr_scattered = false;
+    double nnz_per_row = 0.0;
+    // CUDA graph of a chunk of FP32 steps
+    cudaGraphExec_t graph = nullptr;
+    uint32_t graph_steps = 0;
+    int block = 256;
+    // timing of the dominant kernel
+    bool timing = false;
+    asd::KernelTimer ktimer;
+    cudaEvent_t kev[2] = {nullptr, nullptr};
+};
+
+namespace asd {
+// launchers implemented in the .cu files; all return cudaError_t of the launch
+cudaError_t launch_plain_step(asd_handle* h, uint64_t t);
+cudaError_t launch_fused_step(asd_handle* h, uint32_t rel, bool in_capture);
+cudaError_t launch_step_advance(asd_handle* h, uint32_t nsteps);
+cudaError_t launch_lr_eval_f32(asd_handle* h);
+cudaError_t launch_lr_scatter_f32(asd_handle* h, const float* const s[3]);
+cudaError_t launch_lr_eval_plain(asd_handle* h, const double* s, double* out, bool overwrite_with_demag);
+cudaError_t launch_field_only(asd_handle* h, double* d_out);
+cudaError_t launch_plain_field(asd_handle* h, double* d_out);
+cudaError_t launch_plain_ramp(asd_handle* h, double rv);
+cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v);
+cudaError_t launch_magnetisation(asd_handle* h);
+cudaError_t launch_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, double* d_out,
+                                   cudaStream_t st);
+cudaError_t launch_convert_spins_in(asd_handle* h, const double* d_aos);
+cudaError_t launch_convert_out(asd_handle* h, int what, double* d_aos);
+cudaError_t build_nk_f32(asd_handle* h, const double* d_nr);
+cudaError_t build_nk_plain(asd_handle* h, const double* d_nr);
+}  // namespace asd

@@ -1,0 +1,268 @@
+// Magnetisation reduction, layout conversions at the host boundary, and the
+// field-only evaluation behind asd_get_field.
+#include "internal.h"
+#include <algorithm>
+
+namespace asd {
+namespace {
+
+inline unsigned nb(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
+constexpr int MAG_CHUNK = 8192;
+constexpr int MAG_BLOCK = 256;
+
+__device__ __forceinline__ double block_sum(double v, double* sm) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    __syncthreads();
+    if (l == 0) sm[w] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (w == 0) {
+        r = l < (int)(blockDim.x >> 5) ? sm[l] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    }
+    return r;
+}
+
+// Partial sums of S over one chunk of one replica, per sublattice, in FP64 and
+// a fixed reduction order (deterministic): part[((r*nchunk + c)*nsub + s)*3 + comp].
+template <typename R>
+__global__ void mag_partial(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
+                            const R* __restrict__ sx, const R* __restrict__ sy, const R* __restrict__ sz,
+                            const float* __restrict__ lx, const float* __restrict__ ly, const float* __restrict__ lz,
+                            uint32_t nchunk, double* __restrict__ part) {
+    __shared__ double sm[32];
+    const uint32_t r = blockIdx.y, ch = blockIdx.x;
+    const uint32_t beg = c.rep_off[r] + ch * MAG_CHUNK;
+    const uint32_t end = min(c.rep_off[r + 1], beg + MAG_CHUNK);
+    for (uint32_t s = 0; s < nsub; s++) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (uint32_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+            if (sub_of_atom[atom_of(c, i)] != s) continue;
+            a0 += (double)sx[i]; a1 += (double)sy[i]; a2 += (double)sz[i];
+            if (lx) { a0 += (double)lx[i]; a1 += (double)ly[i]; a2 += (double)lz[i]; }
+        }
+        const double t0 = block_sum(a0, sm), t1 = block_sum(a1, sm), t2 = block_sum(a2, sm);
+        if (threadIdx.x == 0) {
+            double* o = part + (((size_t)r * nchunk + ch) * nsub + s) * 3;
+            o[0] = t0; o[1] = t1; o[2] = t2;
+        }
+    }
+}
+
+// Plain form: AoS doubles.
+__global__ void mag_partial_aos(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
+                                const double* __restrict__ s3, uint32_t nchunk, double* __restrict__ part) {
+    __shared__ double sm[32];
+    const uint32_t r = blockIdx.y, ch = blockIdx.x;
+    const uint32_t beg = c.rep_off[r] + ch * MAG_CHUNK;
+    const uint32_t end = min(c.rep_off[r + 1], beg + MAG_CHUNK);
+    for (uint32_t s = 0; s < nsub; s++) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (uint32_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+            if (sub_of_atom[atom_of(c, i)] != s) continue;
+            a0 += s3[3 * (size_t)i]; a1 += s3[3 * (size_t)i + 1]; a2 += s3[3 * (size_t)i + 2];
+        }
+        const double t0 = block_sum(a0, sm), t1 = block_sum(a1, sm), t2 = block_sum(a2, sm);
+        if (threadIdx.x == 0) {
+            double* o = part + (((size_t)r * nchunk + ch) * nsub + s) * 3;
+            o[0] = t0; o[1] = t1; o[2] = t2;
+        }
+    }
+}
+
+__global__ void mag_final(uint32_t nrep, uint32_t nsub, uint32_t nchunk, const double* __restrict__ part,
+                          const double* __restrict__ inv_count, double* __restrict__ out) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nrep * nsub * 3) return;
+    const uint32_t comp = q % 3, s = (q / 3) % nsub, r = q / (3 * nsub);
+    double acc = 0.0;
+    for (uint32_t ch = 0; ch < nchunk; ch++) acc += part[(((size_t)r * nchunk + ch) * nsub + s) * 3 + comp];
+    out[q] = acc * inv_count[r * nsub + s];
+}
+
+template <typename R>
+__global__ void spins_in_k(uint32_t n, const double* __restrict__ aos, R* __restrict__ x, R* __restrict__ y,
+                           R* __restrict__ z, float* __restrict__ lx, float* __restrict__ ly, float* __restrict__ lz) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v[3] = {aos[3 * (size_t)i], aos[3 * (size_t)i + 1], aos[3 * (size_t)i + 2]};
+    const double m = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    v[0] /= m; v[1] /= m; v[2] /= m;
+    const R hx = (R)v[0], hy = (R)v[1], hz = (R)v[2];
+    x[i] = hx; y[i] = hy; z[i] = hz;
+    if (lx) { lx[i] = (float)(v[0] - (double)hx); ly[i] = (float)(v[1] - (double)hy); lz[i] = (float)(v[2] - (double)hz); }
+}
+
+template <typename R>
+__global__ void soa_out_k(uint32_t n, const R* __restrict__ x, const R* __restrict__ y, const R* __restrict__ z,
+                          const float* __restrict__ lx, const float* __restrict__ ly, const float* __restrict__ lz,
+                          double* __restrict__ aos) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v0 = (double)x[i], v1 = (double)y[i], v2 = (double)z[i];
+    if (lx) { v0 += (double)lx[i]; v1 += (double)ly[i]; v2 += (double)lz[i]; }
+    aos[3 * (size_t)i] = v0; aos[3 * (size_t)i + 1] = v1; aos[3 * (size_t)i + 2] = v2;
+}
+
+// Exchange (+ held long-range) field of the current spins, AoS double out.
+template <typename R, int EX, bool FULL>
+__global__ void field_k(StepConst c, SellDev sell, DiaDev dia, const R* __restrict__ sx, const R* __restrict__ sy,
+                        const R* __restrict__ sz, const float* __restrict__ hr, float inv_p, size_t P,
+                        const uint32_t* __restrict__ idx, double* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    double h[3] = {0.0, 0.0, 0.0};
+    if constexpr (EX == ASD_EXCH_CSR) {
+        const uint32_t sl = i >> 5, lane = i & 31u;
+        for (uint32_t e = sell.slice_ptr[sl] + lane; e < sell.slice_ptr[sl + 1]; e += 32) {
+            int j;
+            double m[9];
+            if constexpr (sizeof(R) == 4) {
+                const float4 a = sell.a[e];
+                j = __float_as_int(a.x);
+                if (FULL) {
+                    const float4 b = sell.b[e]; const float2 cc = sell.c[e];
+                    const double t[9] = {a.y, a.z, a.w, b.x, b.y, b.z, b.w, cc.x, cc.y};
+                    for (int q = 0; q < 9; q++) m[q] = t[q];
+                } else {
+                    for (int q = 0; q < 9; q++) m[q] = 0.0;
+                    m[0] = a.y; m[4] = a.z; m[8] = a.w;
+                }
+            } else {
+                j = sell.col[e];
+                const size_t E = sell.entries;
+                if (FULL) for (int q = 0; q < 9; q++) m[q] = sell.val[q * E + e];
+                else { for (int q = 0; q < 9; q++) m[q] = 0.0; m[0] = sell.val[e]; m[4] = sell.val[E + e]; m[8] = sell.val[2 * E + e]; }
+            }
+            const double s3[3] = {(double)sx[j], (double)sy[j], (double)sz[j]};
+            for (int a = 0; a < 3; a++) h[a] += m[3 * a] * s3[0] + m[3 * a + 1] * s3[1] + m[3 * a + 2] * s3[2];
+        }
+    }
+    if constexpr (EX == ASD_EXCH_DIA) {
+        const size_t ND = (size_t)dia.ndiag * c.n;
+        for (uint32_t d = 0; d < dia.ndiag; d++) {
+            const int64_t col = (int64_t)i + dia.off[d];
+            if (col < 0 || col >= (int64_t)c.n) continue;
+            const size_t a0 = (size_t)d * c.n + i;
+            const double s3[3] = {(double)sx[col], (double)sy[col], (double)sz[col]};
+            const int nc = FULL ? 9 : 3;
+            for (int q = 0; q < nc; q++) {
+                double v;
+                if constexpr (sizeof(R) == 4) v = dia.valf[q * ND + a0]; else v = dia.vald[q * ND + a0];
+                if (FULL) h[q / 3] += v * s3[q % 3];
+                else h[q] += v * s3[q];
+            }
+        }
+    }
+    if (hr) {
+        const uint32_t m = idx[i];
+        for (int a = 0; a < 3; a++) h[a] += (double)(hr[a * P + m] * inv_p);
+    }
+    out[3 * (size_t)i] = h[0]; out[3 * (size_t)i + 1] = h[1]; out[3 * (size_t)i + 2] = h[2];
+}
+
+template <typename R>
+void state(asd_handle* h, R** s) {
+    for (int c = 0; c < 3; c++) {
+        if constexpr (sizeof(R) == 4) s[c] = h->sf[c]; else s[c] = h->sd[c];
+    }
+}
+
+template <typename R>
+cudaError_t field_t(asd_handle* h, double* out) {
+    R* s[3];
+    state<R>(h, s);
+    const float* hr = nullptr;
+    if (h->lr.mode != ASD_LR_NONE) {
+        if (h->lr.mode == ASD_LR_FFT) {
+            cudaError_t e = launch_lr_eval_f32(h);
+            if (e != cudaSuccess) return e;
+        }
+        hr = h->lr.r + 3 * h->lr.P;
+    }
+    const float inv_p = h->lr.P ? 1.0f / (float)h->lr.P : 0.f;
+    const unsigned g = nb(h->n, 256);
+    if (h->exch == ASD_EXCH_CSR) {
+        if (h->full) field_k<R, ASD_EXCH_CSR, true><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        else field_k<R, ASD_EXCH_CSR, false><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+    } else if (h->exch == ASD_EXCH_DIA) {
+        if (h->full) field_k<R, ASD_EXCH_DIA, true><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        else field_k<R, ASD_EXCH_DIA, false><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+    } else {
+        field_k<R, ASD_EXCH_NONE, false><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+    }
+    h->launches += 1;
+    return cudaGetLastError();
+}
+
+__global__ void set_scalar_k(double* dst, double v) { *dst = v; }
+
+}  // namespace
+
+cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v) {
+    set_scalar_k<<<1, 1, 0, h->stream>>>(dst, v);
+    h->launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_field_only(asd_handle* h, double* d_out) {
+    if (h->p.precision == ASD_FP64_PLAIN) return launch_plain_field(h, d_out);
+    if (h->p.precision == ASD_FP32) return field_t<float>(h, d_out);
+    return field_t<double>(h, d_out);
+}
+
+cudaError_t launch_magnetisation(asd_handle* h) {
+    const uint32_t nsub = h->nsub;
+    uint32_t maxrep = 0;
+    for (uint32_t r = 0; r < h->nrep; r++) maxrep = std::max(maxrep, h->h_rep_off[r + 1] - h->h_rep_off[r]);
+    const uint32_t nchunk = (maxrep + MAG_CHUNK - 1) / MAG_CHUNK;
+    dim3 grid(nchunk ? nchunk : 1, h->nrep);
+    const uint32_t* sub_of_atom = h->d_sub_of_atom;
+    const double* inv_count = h->d_inv_count;
+    if (h->p.precision == ASD_FP64_PLAIN) {
+        mag_partial_aos<<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->p_s, grid.x, h->d_magpart);
+    } else if (h->p.precision == ASD_FP32) {
+        const bool comp = (h->p.flags & ASD_FLAG_COMPENSATED) != 0;
+        mag_partial<float><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1], h->sf[2],
+                                                             comp ? h->sl[0] : nullptr, comp ? h->sl[1] : nullptr,
+                                                             comp ? h->sl[2] : nullptr, grid.x, h->d_magpart);
+    } else {
+        mag_partial<double><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sd[0], h->sd[1], h->sd[2],
+                                                              nullptr, nullptr, nullptr, grid.x, h->d_magpart);
+    }
+    mag_final<<<nb(h->nrep * nsub * 3, 128), 128, 0, h->stream>>>(h->nrep, nsub, grid.x, h->d_magpart, inv_count, h->d_mag);
+    h->launches += 2;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_convert_spins_in(asd_handle* h, const double* d_aos) {
+    const unsigned g = nb(h->n, 256);
+    if (h->p.precision == ASD_FP32) {
+        const bool comp = (h->p.flags & ASD_FLAG_COMPENSATED) != 0;
+        spins_in_k<float><<<g, 256, 0, h->stream>>>(h->n, d_aos, h->sf[0], h->sf[1], h->sf[2], comp ? h->sl[0] : nullptr,
+                                                     comp ? h->sl[1] : nullptr, comp ? h->sl[2] : nullptr);
+    } else {
+        spins_in_k<double><<<g, 256, 0, h->stream>>>(h->n, d_aos, h->sd[0], h->sd[1], h->sd[2], nullptr, nullptr, nullptr);
+    }
+    h->launches += 1;
+    return cudaGetLastError();
+}
+
+// what: 0 spins, 1 det field
+cudaError_t launch_convert_out(asd_handle* h, int what, double* d_aos) {
+    const unsigned g = nb(h->n, 256);
+    if (h->p.precision == ASD_FP32) {
+        const bool comp = what == 0 && (h->p.flags & ASD_FLAG_COMPENSATED) != 0;
+        float* const* s = what == 0 ? h->sf : h->detf;
+        soa_out_k<float><<<g, 256, 0, h->stream>>>(h->n, s[0], s[1], s[2], comp ? h->sl[0] : nullptr,
+                                                   comp ? h->sl[1] : nullptr, comp ? h->sl[2] : nullptr, d_aos);
+    } else {
+        double* const* s = what == 0 ? h->sd : h->detd;
+        soa_out_k<double><<<g, 256, 0, h->stream>>>(h->n, s[0], s[1], s[2], nullptr, nullptr, nullptr, d_aos);
+    }
+    h->launches += 1;
+    return cudaGetLastError();
+}
+
+}  // namespace asd

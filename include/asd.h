@@ -1,0 +1,199 @@
+/*
+ * asd.h - C ABI of the B200-native stochastic Landau-Lifshitz-Gilbert step.
+ *
+ * Drop-in replacement for the integrator layer of tomostler13/gpu-atomistic-code
+ * (the reference).  Every entry point below names the reference interface it
+ * replaces (path:line inside the reference project).  Signatures use plain C
+ * types, pointers and sizes only; no C++ or PyTorch types cross this boundary.
+ *
+ * Conventions
+ *  - Spins, fields and other per-spin vectors cross the boundary as host arrays
+ *    of doubles in spin-major order [3*i+c], the layout of the reference's device
+ *    arrays (src/cuda.cu:239-252).  Replicas are concatenated in the order given
+ *    to asd_create.
+ *  - Every call returns ASD_OK (0) or a positive ASD_E* code and never exits the
+ *    process (the reference calls exit(0) on errors, src/error.cpp:19-28).  After
+ *    a failure asd_last_error() returns a message.
+ *  - A handle owns one CUDA stream on the device current at asd_create; calls on
+ *    one handle are not thread-safe, distinct handles are independent.
+ */
+#ifndef ASD_H
+#define ASD_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes */
+#define ASD_OK        0
+#define ASD_EINVAL    1  /* bad argument or inconsistent input */
+#define ASD_ECUDA     2  /* CUDA runtime error (message has the CUDA string) */
+#define ASD_ENOMEM    3  /* device allocation failed */
+#define ASD_ETIMEOUT  4  /* a bounded device-side wait ran out */
+#define ASD_ESTATE    5  /* call not valid in the handle's state */
+#define ASD_ECUFFT    6  /* cuFFT error */
+#define ASD_ENOTSUP   7  /* combination not supported */
+#define ASD_ENOTFINITE 8 /* a non-finite spin was produced or supplied */
+
+/* Integrators: llg::intscheme (src/llg.cpp:309-341). */
+#define ASD_HEUN 0
+#define ASD_RK4  1
+#define ASD_RK5  2
+
+/* Arithmetic forms of the step. */
+#define ASD_FP64_PLAIN 0  /* FP64, one thread per spin, separate noise/SpMV/stage launches (reference-structured) */
+#define ASD_FP32       1  /* FP32 state and fields, FP64 renormalisation, fused stage kernels, CUDA graph */
+#define ASD_FP64_FUSED 2  /* the fused stage kernels instantiated in FP64 */
+
+/* Exchange storage: config::exchm (src/config.cpp:139-159) plus "none". */
+#define ASD_EXCH_FFT  0   /* exchange folded into the k-space interaction matrix */
+#define ASD_EXCH_DIA  1
+#define ASD_EXCH_CSR  2
+#define ASD_EXCH_NONE 3
+
+/* Long-range (dipolar) field. */
+#define ASD_LR_NONE   0
+#define ASD_LR_DIPOLE 1   /* Include_dipole with CSR/DIA exchange, refreshed every `update` steps */
+#define ASD_LR_FFT    2   /* exchm==0: the whole field from the interaction matrix at every stage */
+
+/* Reference-compatibility switches (asd_params.flags).  Default 0 = the CUDA
+ * path's physics with its bugs fixed. */
+#define ASD_FLAG_RK_DOUBLE_RDT       (1u << 2)  /* src/cuintRK4.cu:141-142, src/cuintRK5.cu:158-159 */
+#define ASD_FLAG_RK_STAGE_SPIN_MIXED (1u << 3)  /* src/cuintRK4.cu:172: es={Cespin.x,Cspin.y,Cspin.z} */
+#define ASD_FLAG_GPU_CSR_DIP_STALE   (1u << 4)  /* src/cuda.cu:192-199 */
+#define ASD_FLAG_GPU_DZZ_FROM_DYY    (1u << 6)  /* src/cuda_util.cu:308-312,373-377 */
+#define ASD_FLAG_GPU_HDEMAG_FP32     (1u << 7)  /* CHDemag stored as float (src/cuda_glob.cu) */
+#define ASD_FLAG_COMPENSATED         (1u << 16) /* FP32 form: spins kept as float hi+lo pairs */
+#define ASD_FLAG_AUTOTUNE            (1u << 17) /* FP32 form: time block shapes at create */
+
+#define ASD_ALL_REPLICAS 0xFFFFFFFFu
+
+/* Per unit-cell atom (the reference's unitCellMembers, inc/unitcell.h). */
+typedef struct asd_material {
+    double mu;          /* moment [muB] (GetMu) */
+    double lambda;      /* Gilbert damping (GetDamping) */
+    double gamma;       /* gyromagnetic ratio relative to 1.76e11 (GetGamma) */
+    double k1u;         /* first-order uniaxial constant [J/atom] (GetK1U) */
+    double k1u_dir[3];  /* its unit axis (GetK1UDir) */
+    uint32_t sublattice;/* magnetic species (GetSublattice) */
+} asd_material;
+
+/* Run parameters: the llg{} and anis{} settings plus the RNG seed. */
+typedef struct asd_params {
+    uint32_t integrator;   /* ASD_HEUN / ASD_RK4 / ASD_RK5 */
+    uint32_t precision;    /* ASD_FP64_PLAIN / ASD_FP32 / ASD_FP64_FUSED */
+    double dt;             /* time step [s] (llg.dt) */
+    double applied[3];     /* applied field [T] (llg.applied) */
+    double k2perp, k2perpdir[3], k2par, k2pardir[3];        /* [J], unit axes (anis.*) */
+    double k4perp, k4perpdirs[9], k4par, k4pardirs[9];      /* 3 axes each, row-major */
+    uint64_t seed;         /* Philox key for the thermal field */
+    uint32_t update;       /* dipole refresh period in steps (llg.update); 0 -> 1 */
+    uint32_t flags;        /* ASD_FLAG_* */
+    double gyro, muB, kB;  /* 0 -> the reference constants 1.76e11, 9.27e-24, 1.38e-23 (src/llg.cpp:25) */
+} asd_params;
+
+/* One lattice (replica) and its interactions. */
+typedef struct asd_system {
+    uint32_t nspins;
+    uint32_t nmat;                  /* unit-cell atoms described by mat[] */
+    const asd_material* mat;
+    const uint32_t* atom;           /* unit-cell atom of each spin (geom::lu(i,4)); NULL -> i % nmat */
+    uint32_t exch;                  /* ASD_EXCH_* */
+    uint32_t exch_full;             /* 0: xx,yy,zz only; 1: full 3x3 (config::offdiag) */
+    /* CSR (exch == ASD_EXCH_CSR): exch::xadj / adjncy / data** */
+    const uint32_t* xadj;           /* nspins+1 */
+    const uint32_t* adjncy;         /* nnz */
+    uint32_t nnz;
+    const double* csr_val;          /* nnz x 9 [T], row-major (alpha,beta); diagonal form reads 0,4,8 */
+    /* DIA (exch == ASD_EXCH_DIA): exch::diagoffset / data**, row-aligned data[c][n*N+row] */
+    uint32_t ndiag;
+    const int32_t* dia_offset;      /* ndiag */
+    const double* dia_val;          /* 9 x ndiag x nspins [T] */
+    /* Long-range field on the zero-padded mesh (intmat::dipNrab / Nrab before the FFT). */
+    uint32_t lr;                    /* ASD_LR_* */
+    uint32_t mesh[3];               /* padded mesh 2*dim*Nm per axis */
+    const uint32_t* mesh_xyz;       /* 3 per spin: geom::lu(i,0..2) */
+    const double* nr;               /* real-space matrix [3][3][mesh0][mesh1][mesh2], FP64 */
+    double temperature;             /* [K] (llg::T) */
+    uint32_t stream;                /* Philox stream of this replica */
+    const double* site_field;       /* 3N staggered/site field [T] (fields::Hstag*), or NULL */
+} asd_system;
+
+typedef struct asd_handle asd_handle;
+
+/* cullg::cuinit (src/cuda.cu:261-402) + llg::initLLG prefactors (src/llg.cpp:585-631):
+ * uploads nsys replicas, derives sigma / llgpf / k1u per atom, builds device layouts,
+ * FFT plans and N_k. */
+int asd_create(const asd_params* p, const asd_system* sys, uint32_t nsys, asd_handle** out);
+/* cullg::deallocate_cuda_memory (src/cuda_util.cu:186-242). */
+int asd_destroy(asd_handle* h);
+const char* asd_last_error(const asd_handle* h);
+const char* asd_version(void);
+
+/* Initial spins (spins::Sx/Sy/Sz uploaded in allocate_memory_on_card, src/cuda_util.cu:536-537);
+ * s: 3*nspins_total doubles, normalised on upload. */
+int asd_set_spins(asd_handle* h, const double* s, size_t n_spins);
+/* Spin read-back (the D2H copy of src/cuda.cu:239-246). */
+int asd_get_spins(asd_handle* h, double* s, size_t n_spins);
+/* CDetFields read-back (src/cuda.cu:247-252): total field minus thermal at the last corrector. */
+int asd_get_det_field(asd_handle* h, double* hout, size_t n_spins);
+/* The field of the current spins without thermal, anisotropy, applied and site terms
+ * (CH after the stage-1 field kernels, src/cufields.cu:201-203, 405). */
+int asd_get_field(asd_handle* h, double* hout, size_t n_spins);
+
+/* llg::integrate(t) x nsteps (src/llg.cpp:639-664 -> cullg::llgGPU / llgGPURK4 / llgGPURK5). */
+int asd_step(asd_handle* h, uint64_t nsteps);
+int asd_get_step(const asd_handle* h, uint64_t* t);
+int asd_set_step(asd_handle* h, uint64_t t);
+int asd_sync(asd_handle* h);
+
+/* llg::T (passed per launch, src/cuda.cu:159); replica ASD_ALL_REPLICAS sets all. */
+int asd_set_temperature(asd_handle* h, uint32_t replica, double T);
+/* llg::applied (src/cuda.cu:159). */
+int asd_set_applied(asd_handle* h, const double applied[3]);
+/* cullg::CsetStagFields / CsetStagFieldsZero (src/cuda_util.cu:563-588): profile 3N [T], NULL zeroes it. */
+int asd_set_site_field(asd_handle* h, const double* profile, size_t n_spins);
+/* cullg::rampStag(rv) (src/cuda.cu:38-41): site field = rv * profile. */
+int asd_set_site_field_scale(asd_handle* h, double rv);
+
+/* util::calc_mag method 0 (src/util_mag.cpp:44-65) per replica: out[(r*nsub+s)*3+c], FP64 sums. */
+int asd_magnetisation(asd_handle* h, double* out, size_t out_len);
+/* Number of sublattices (GetNMS) of the handle. */
+int asd_num_sublattices(const asd_handle* h, uint32_t* nsub);
+
+/* Time nsteps asd_step calls on the device with CUDA events on the handle's stream;
+ * *ms = elapsed milliseconds, *launches = kernels this library launched. */
+int asd_time_steps(asd_handle* h, uint64_t nsteps, double* ms, uint64_t* launches);
+/* Per-kernel device time of the dominant field/stage kernel in the last asd_time_steps
+ * (CUDA events around each of its launches): average ms per launch and launch count. */
+int asd_kernel_stats(const asd_handle* h, char* name, size_t name_len, double* avg_ms, uint64_t* count,
+                     double* bytes_per_launch);
+
+/* The thermal normals the step uses for (seed, stream, step): 3 per spin for spins
+ * [0, nspins), computed by the device generator (Philox4x32-10 + Box-Muller). */
+int asd_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t nspins, double* out);
+
+/* --- set-up builders (host C++, FP64) ---------------------------------------- */
+/* Bond list -> CSR as exch::exchunitcell does (src/exch_unitcell.cpp:265-489): spins ordered
+ * (i,j,k,t) with t innermost (src/geom.cpp:214-266); bond b of unit-cell atom a_b to atom
+ * t_b in the cell offset vec_b (3 ints) with tensor J_b (9 doubles [J]); value J/(mu_a muB).
+ * Pass xadj/adjncy/val = NULL to get *nnz only. */
+int asd_build_csr(const uint32_t dim[3], const int pbc[3], uint32_t nauc, const double* mu,
+                  uint32_t nbond, const uint32_t* bond_atom, const uint32_t* bond_to, const int32_t* bond_vec,
+                  const double* bond_J, double muB, uint32_t* xadj, uint32_t* adjncy, double* val, uint32_t* nnz);
+/* matconv::csr_to_dia_* (src/matrix_conv.cpp:28-272): returns ndiag in *ndiag; pass
+ * offsets/data = NULL to count only. */
+int asd_csr_to_dia(uint32_t n, const uint32_t* xadj, const uint32_t* adjncy, const double* val9,
+                   int32_t* offsets, double* data9, uint32_t* ndiag);
+/* intmat::fillDipIntmat / fillIntmat (src/intmat.cpp:188-331): nr[3][3][2dim*nk] (+=). */
+int asd_build_dipole_nr(const uint32_t dim[3], const uint32_t nk[3], const double abc[3], double muB,
+                        double mu_scale, double* nr);
+/* exch::fft (src/exch_intmat.cpp:28-163): fold shell tensors into nr (+=); returns images in *count. */
+int asd_fold_exchange_nr(const uint32_t mesh[3], uint32_t nshell, const int32_t* shell_vec,
+                         const double* J9, double mu_muB, double* nr, uint32_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ASD_H */

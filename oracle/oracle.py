@@ -1,0 +1,325 @@
+"""ctypes wrappers of the checkers: liboracle.so (the FP64 CPU restatement) and
+_ref/libref_llgcpu*.so (the reference's own llgCPU compiled from source).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU legs of bench.py; never by the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libref_llgcpu.so")
+REF_REPLAY_SO = os.path.join(HERE, "_ref", "libref_llgcpu_replay.so")
+
+CPU_CORRECTOR_ACCUM = 1 << 0
+CPU_THERMAL_Z_FROM_X = 1 << 1
+RK_DOUBLE_RDT = 1 << 2
+RK_STAGE_SPIN_MIXED = 1 << 3
+GPU_CSR_DIP_STALE = 1 << 4
+CPU_SUM_ORDER = 1 << 5
+GPU_DZZ_FROM_DYY = 1 << 6
+GPU_HDEMAG_FP32 = 1 << 7
+EXCH_NONE, EXCH_DIA, EXCH_CSR = 0, 1, 2
+LR_NONE, LR_DIPOLE, LR_FFT = 0, 1, 2
+HEUN, RK4, RK5 = 0, 1, 2
+NOISE_PHILOX, NOISE_MWC, NOISE_BUFFER = 0, 1, 2
+MUB, KB, GYRO = 9.27e-24, 1.38e-23, 1.76e11
+
+dp = C.POINTER(C.c_double)
+u32p = C.POINTER(C.c_uint32)
+i32p = C.POINTER(C.c_int32)
+
+
+def build():
+    """Compile the checkers (the reference targets only where the reference tree exists)."""
+    targets = ["liboracle.so"]
+    if os.path.isdir("/root/reference/src"):
+        targets.append("ref")
+    subprocess.run(["make", "-C", HERE] + targets, check=True, capture_output=True)
+
+
+def _ptr(a, ct):
+    if a is None:
+        return C.cast(None, C.POINTER(ct))
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+_olib = None
+
+
+def olib():
+    global _olib
+    if _olib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        L.orc_create.restype = C.c_void_p
+        L.orc_create.argtypes = [C.c_uint32]
+        L.orc_destroy.argtypes = [C.c_void_p]
+        for name in ["orc_set_material", "orc_set_global_anis", "orc_set_dynamics", "orc_set_replicas",
+                     "orc_set_csr", "orc_set_dia", "orc_set_site_field", "orc_set_longrange", "orc_set_flags",
+                     "orc_set_noise", "orc_set_spins", "orc_get_spins", "orc_get_det_field", "orc_field", "orc_run",
+                     "orc_magnetisation"]:
+            getattr(L, name).restype = C.c_int
+        L.orc_set_material.argtypes = [C.c_void_p, dp, dp, dp, dp, dp]
+        L.orc_set_global_anis.argtypes = [C.c_void_p, C.c_double, dp, C.c_double, dp, C.c_double, dp, C.c_double, dp,
+                                          C.c_double]
+        L.orc_set_dynamics.argtypes = [C.c_void_p, C.c_int, C.c_double, dp]
+        L.orc_set_replicas.argtypes = [C.c_void_p, C.c_uint32, u32p, dp, u32p]
+        L.orc_set_csr.argtypes = [C.c_void_p, C.c_int, C.c_uint32, u32p, u32p, dp]
+        L.orc_set_dia.argtypes = [C.c_void_p, C.c_int, C.c_uint32, i32p, dp]
+        L.orc_set_site_field.argtypes = [C.c_void_p, dp, C.c_double]
+        L.orc_set_longrange.argtypes = [C.c_void_p, C.c_int, u32p, u32p, C.c_uint32, u32p, dp, dp, C.c_uint32]
+        L.orc_set_flags.argtypes = [C.c_void_p, C.c_uint32]
+        L.orc_set_noise.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_uint32, C.c_uint32, dp, C.c_size_t]
+        L.orc_set_spins.argtypes = [C.c_void_p, dp]
+        L.orc_get_spins.argtypes = [C.c_void_p, dp]
+        L.orc_get_det_field.argtypes = [C.c_void_p, dp]
+        L.orc_field.argtypes = [C.c_void_p, dp]
+        L.orc_run.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64]
+        L.orc_magnetisation.argtypes = [C.c_void_p, C.c_uint32, u32p, dp]
+        L.orc_philox4x32_10.argtypes = [u32p, u32p, u32p]
+        L.orc_thermal_normals.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, dp]
+        L.orc_log.restype = C.c_double
+        L.orc_log.argtypes = [C.c_double]
+        L.orc_sincos_2pi.argtypes = [C.c_uint32, dp, dp]
+        L.orc_mwc_seed.argtypes = [C.c_uint32, C.c_uint32]
+        L.orc_mwc_rand.restype = C.c_double
+        L.orc_mwc_normal.restype = C.c_double
+        L.orc_csr_to_dia.restype = C.c_int
+        L.orc_csr_to_dia.argtypes = [C.c_uint32, u32p, u32p, dp, i32p, dp]
+        L.orc_build_dipole_nr.argtypes = [u32p, u32p, dp, C.c_double, C.c_double, dp]
+        L.orc_fold_exchange_nr.restype = C.c_int
+        L.orc_fold_exchange_nr.argtypes = [u32p, C.c_uint32, i32p, dp, C.c_double, dp]
+        _olib = L
+    return _olib
+
+
+def a64(x):
+    return None if x is None else np.ascontiguousarray(x, dtype=np.float64)
+
+
+def au32(x):
+    return None if x is None else np.ascontiguousarray(x, dtype=np.uint32)
+
+
+class Oracle:
+    """FP64 CPU restatement of the step for one handle's worth of spins."""
+
+    def __init__(self, systems, integrator=HEUN, dt=1e-16, applied=(0, 0, 0), flags=0, seed=1, update=1,
+                 noise=NOISE_PHILOX, anis=None, noise_buf=None, mwc=(1, 101)):
+        if not isinstance(systems, (list, tuple)):
+            systems = [systems]
+        self.systems = systems
+        n = sum(s.nspins for s in systems)
+        self.n = n
+        L = olib()
+        self.c = L.orc_create(n)
+        # expand materials per spin (src/llg.cpp:591-592, src/geom.cpp:244)
+        llgpf, lam, sig, k1u = (np.zeros(n) for _ in range(4))
+        k1d = np.zeros((n, 3))
+        off = 0
+        sub = np.zeros(n, dtype=np.uint32)
+        for s in systems:
+            nm = len(s.materials)
+            atoms = s.atom if s.atom is not None else np.arange(s.nspins) % nm
+            for t, m in enumerate(s.materials):
+                sel = off + np.nonzero(atoms == t)[0]
+                llgpf[sel] = -1.0 / (1.0 + m.lam * m.lam)
+                lam[sel] = m.lam
+                sig[sel] = np.sqrt(2.0 * KB * m.lam / (m.mu * MUB * dt * m.gamma * GYRO))
+                k1u[sel] = 2.0 * m.k1u / (MUB * m.mu)
+                k1d[sel] = m.k1u_dir
+                sub[sel] = m.sublattice
+            off += s.nspins
+        self.sub = sub
+        self.nsub = int(sub.max()) + 1
+        self._keep = [llgpf, lam, sig, k1u, k1d]
+        L.orc_set_material(self.c, _ptr(llgpf, C.c_double), _ptr(lam, C.c_double), _ptr(sig, C.c_double),
+                           _ptr(k1u, C.c_double), _ptr(a64(k1d), C.c_double))
+        an = anis or {}
+        basemm = systems[0].materials[0].mu * MUB
+        vec = lambda k, m: a64(an.get(k, [0.0] * m))
+        self._an = [vec("k2perpdir", 3), vec("k2pardir", 3), vec("k4perpdirs", 9), vec("k4pardirs", 9)]
+        L.orc_set_global_anis(self.c, an.get("k2perp", 0.0), _ptr(self._an[0], C.c_double), an.get("k2par", 0.0),
+                              _ptr(self._an[1], C.c_double), an.get("k4perp", 0.0), _ptr(self._an[2], C.c_double),
+                              an.get("k4par", 0.0), _ptr(self._an[3], C.c_double), basemm)
+        ap = a64(applied)
+        L.orc_set_dynamics(self.c, integrator, dt * GYRO, _ptr(ap, C.c_double))
+        roff = au32(np.concatenate([[0], np.cumsum([s.nspins for s in systems])]))
+        T = a64([s.temperature for s in systems])
+        st = au32([s.stream for s in systems])
+        L.orc_set_replicas(self.c, len(systems), _ptr(roff, C.c_uint32), _ptr(T, C.c_double), _ptr(st, C.c_uint32))
+        s0 = systems[0]
+        if s0.exch == 2:  # CSR (asd_b200.EXCH_CSR)
+            xs, ads, vs = [np.zeros(1, dtype=np.uint32)], [], []
+            base = 0
+            for r, s in enumerate(systems):
+                xs.append(s.xadj[1:] + base)
+                ads.append(s.adjncy + roff[r])
+                vs.append(s.csr_val)
+                base += len(s.adjncy)
+            xadj = au32(np.concatenate(xs))
+            adj = au32(np.concatenate(ads))
+            val = a64(np.concatenate(vs))
+            self._keep += [xadj, adj, val]
+            L.orc_set_csr(self.c, 1 if s0.full else 0, len(adj), _ptr(xadj, C.c_uint32), _ptr(adj, C.c_uint32),
+                          _ptr(val, C.c_double))
+        elif s0.exch == 1:  # DIA
+            doff = np.ascontiguousarray(s0.dia_offset, dtype=np.int32)
+            dval = a64(s0.dia_val)
+            self._keep += [doff, dval]
+            L.orc_set_dia(self.c, 1 if s0.full else 0, len(doff), _ptr(doff, C.c_int32), _ptr(dval, C.c_double))
+        if s0.site_field is not None:
+            hs = a64(np.concatenate([s.site_field if s.site_field is not None else np.zeros((s.nspins, 3))
+                                     for s in systems]))
+            self._keep.append(hs)
+            L.orc_set_site_field(self.c, _ptr(hs, C.c_double), 1.0)
+        if s0.lr:
+            mesh = au32(s0.mesh)
+            mxyz = au32(s0.mesh_xyz)
+            nr = a64(s0.nr)
+            atoms = s0.atom if s0.atom is not None else np.arange(s0.nspins) % len(s0.materials)
+            w = a64([s0.materials[a].mu for a in atoms]) if s0.lr == LR_DIPOLE else None
+            self._keep += [mesh, mxyz, nr, w]
+            L.orc_set_longrange(self.c, s0.lr, _ptr(mesh, C.c_uint32), _ptr(mxyz, C.c_uint32), 1, None,
+                                _ptr(nr, C.c_double), _ptr(w, C.c_double), update)
+        L.orc_set_flags(self.c, flags)
+        nb = a64(noise_buf)
+        L.orc_set_noise(self.c, noise, seed, mwc[0], mwc[1], _ptr(nb, C.c_double), 0 if nb is None else len(nb))
+        self.t = 0
+
+    def __del__(self):
+        try:
+            olib().orc_destroy(self.c)
+        except Exception:
+            pass
+
+    def set_spins(self, s):
+        s = a64(s).reshape(-1)
+        olib().orc_set_spins(self.c, _ptr(s, C.c_double))
+
+    def spins(self):
+        out = np.empty(3 * self.n)
+        olib().orc_get_spins(self.c, _ptr(out, C.c_double))
+        return out.reshape(self.n, 3)
+
+    def det_field(self):
+        out = np.empty(3 * self.n)
+        olib().orc_get_det_field(self.c, _ptr(out, C.c_double))
+        return out.reshape(self.n, 3)
+
+    def field(self):
+        out = np.empty(3 * self.n)
+        olib().orc_field(self.c, _ptr(out, C.c_double))
+        return out.reshape(self.n, 3)
+
+    def step(self, k):
+        olib().orc_run(self.c, self.t, k)
+        self.t += k
+
+    def magnetisation(self):
+        out = np.empty(len(self.systems) * self.nsub * 3)
+        sub = au32(self.sub)
+        olib().orc_magnetisation(self.c, self.nsub, _ptr(sub, C.c_uint32), _ptr(out, C.c_double))
+        return out.reshape(len(self.systems), self.nsub, 3)
+
+
+def philox(ctr, key):
+    c = au32(ctr)
+    k = au32(key)
+    o = np.zeros(4, dtype=np.uint32)
+    olib().orc_philox4x32_10(_ptr(c, C.c_uint32), _ptr(k, C.c_uint32), _ptr(o, C.c_uint32))
+    return o
+
+
+def thermal_normals(seed, stream, n, step):
+    out = np.zeros((n, 3))
+    L = olib()
+    buf = (C.c_double * 3)()
+    for i in range(n):
+        L.orc_thermal_normals(seed, stream, i, step, buf)
+        out[i] = buf[:]
+    return out
+
+
+class RefLLGCPU:
+    """The reference's own llgCPU::llgCPU (src/llgCPU.cpp:56-361) behind ref_harness.cpp."""
+
+    def __init__(self, system, dt=1e-16, applied=(0, 0, 0), replay=False, seed=(1, 101)):
+        path = REF_REPLAY_SO if replay else REF_SO
+        if not os.path.exists(path):
+            build()
+        # each instance gets its own copy of the globals: load a private copy of the library
+        self.L = C.CDLL(path, mode=os.RTLD_LOCAL)
+        L = self.L
+        L.refh_init.argtypes = [C.c_uint, C.c_uint, dp, dp, dp, u32p, C.c_double, C.c_double, dp]
+        L.refh_set_anis.argtypes = [dp, dp, C.c_double, dp, C.c_double, dp, C.c_double, dp, C.c_double, dp]
+        L.refh_set_csr.argtypes = [C.c_int, C.c_uint, u32p, u32p, dp]
+        L.refh_set_dia.argtypes = [C.c_int, C.c_uint, i32p, dp, C.c_uint]
+        L.refh_set_site_fields.argtypes = [dp, dp]
+        L.refh_set_spins.argtypes = [dp]
+        L.refh_get_spins.argtypes = [dp]
+        L.refh_get_field.argtypes = [dp]
+        L.refh_seed.argtypes = [C.c_uint, C.c_uint]
+        L.refh_run.argtypes = [C.c_uint, C.c_uint]
+        L.refh_set_temperature.argtypes = [C.c_double]
+        L.refh_normal.restype = C.c_double
+        if replay:
+            L.refh_set_noise.argtypes = [dp, C.c_size_t]
+        s = system
+        self.n = s.nspins
+        mats = s.materials
+        mu = a64([m.mu for m in mats])
+        lam = a64([m.lam for m in mats])
+        gam = a64([m.gamma for m in mats])
+        atoms = au32(s.atom if s.atom is not None else np.arange(s.nspins) % len(mats))
+        ap = a64(applied)
+        L.refh_init(s.nspins, len(mats), _ptr(mu, C.c_double), _ptr(lam, C.c_double), _ptr(gam, C.c_double),
+                    _ptr(atoms, C.c_uint32), dt, s.temperature, _ptr(ap, C.c_double))
+        k1u = a64([2.0 * mats[a].k1u / (MUB * mats[a].mu) for a in atoms])
+        k1d = a64([mats[a].k1u_dir for a in atoms])
+        L.refh_set_anis(_ptr(k1u, C.c_double), _ptr(k1d, C.c_double), 0.0, None, 0.0, None, 0.0, None, 0.0, None)
+        if s.exch == 2:
+            xadj, adj, val = au32(s.xadj), au32(s.adjncy), a64(s.csr_val)
+            self._keep = [xadj, adj, val]
+            L.refh_set_csr(1 if s.full else 0, len(adj), _ptr(xadj, C.c_uint32), _ptr(adj, C.c_uint32),
+                           _ptr(val, C.c_double))
+        elif s.exch == 1:
+            off = np.ascontiguousarray(s.dia_offset, dtype=np.int32)
+            val = a64(s.dia_val)
+            self._keep = [off, val]
+            L.refh_set_dia(1 if s.full else 0, len(off), _ptr(off, C.c_int32), _ptr(val, C.c_double),
+                           len(off))
+        if s.site_field is not None:
+            hs = a64(s.site_field)
+            self._keep.append(hs)
+            L.refh_set_site_fields(_ptr(hs, C.c_double), None)
+        if not replay:
+            L.refh_seed(*seed)
+        self.t = 0
+
+    def set_noise(self, xi):
+        x = a64(xi).reshape(-1)
+        self._noise = x
+        self.L.refh_set_noise(_ptr(x, C.c_double), len(x))
+
+    def set_spins(self, s):
+        s = a64(s).reshape(-1)
+        self.L.refh_set_spins(_ptr(s, C.c_double))
+
+    def spins(self):
+        out = np.empty(3 * self.n)
+        self.L.refh_get_spins(_ptr(out, C.c_double))
+        return out.reshape(self.n, 3)
+
+    def step(self, k):
+        rc = self.L.refh_run(self.t, k)
+        self.t += k
+        return rc
