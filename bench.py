@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of the sLLG step: spin-updates/s on one B200 (or N replicas on N GPUs).
+
+Default workload: the body-centred-tetragonal 2-sublattice antiferromagnet,
+64x64x64 cells (524,288 spins), 26 neighbours/site with full 3x3 tensors in
+CSR (SELL-32 on the device), Heun, T=300 K, FP32 state with FP64
+renormalisation.  Prints one JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+"""
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "gpu-atomistic-code_b200")
+for p in (REPO, PKG):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+METRIC = "spin-updates/s on 1 B200: FP32 batched vs FP64 plain at stated err vs FP64"
+PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+def ncu_traffic(workload):
+    """Per-launch DRAM bytes of the stage kernel from the committed ncu summary, if any."""
+    d = os.path.join(REPO, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for fn in sorted(os.listdir(d)):
+        if not fn.endswith(".md"):
+            continue
+        for line in open(os.path.join(d, fn)):
+            m = re.match(r"\s*bench-traffic\s+(\S+)\s+([0-9.eE+]+)", line)
+            if m and m.group(1) == workload:
+                return float(m.group(2))
+    return None
+
+
+def make_workload(name):
+    import asd_b200 as A
+    import asd_lattice as LT
+    if name == "bct2_64":
+        s = LT.bct2_antiferromagnet(64, layout="csr", T=300.0)
+        return [s], dict(integrator=A.HEUN, dt=1e-16), {"lattice": "bct2 64x64x64 cells", "nspins": s.nspins,
+                                                         "neighbours": 26, "tensor": "full 3x3", "exchange": "CSR",
+                                                         "integrator": "heun", "T_K": 300.0}
+    if name == "bct2_64_dia":
+        s = LT.bct2_antiferromagnet(64, layout="dia", T=300.0)
+        return [s], dict(integrator=A.HEUN, dt=1e-16), {"lattice": "bct2 64^3 cells", "nspins": s.nspins,
+                                                         "exchange": "DIA", "integrator": "heun", "T_K": 300.0}
+    if name == "sc16":
+        s = LT.sc_ferromagnet(16, T=300.0)
+        return [s], dict(integrator=A.HEUN, dt=1e-16), {"lattice": "sc 16^3", "nspins": s.nspins, "T_K": 300.0}
+    if name == "replicas96":
+        reps, L, Ts = LT.replica_batch(96)
+        return reps, dict(integrator=A.HEUN, dt=1e-16), {"lattice": "96 sc replicas, edges U{16..64} seed 4",
+                                                          "nspins": int(sum(r.nspins for r in reps)),
+                                                          "T_K": "0..1.2*104"}
+    if name == "sc128_fft":
+        s = LT.sc_fft(128)
+        return [s], dict(integrator=A.HEUN, dt=1e-16), {"lattice": "sc 128^3 open, pad 256^3", "nspins": s.nspins,
+                                                         "field": "dipole+exchange via R2C/C2R FFT", "T_K": 0.0}
+    if name == "northstar":
+        s = LT.sc_ferromagnet((128, 128, 64), pbc=(0, 0, 0), dipole=True)
+        return [s], dict(integrator=A.HEUN, dt=1e-16, update=1), {"lattice": "sc 128x128x64 open", "nspins": s.nspins,
+                                                                   "field": "CSR NN exchange + FFT dipole every step",
+                                                                   "T_K": 0.0}
+    if name == "film_rk4":
+        s = LT.film_dia(1024, 1024, 4)
+        return [s], dict(integrator=A.RK4, dt=5e-16, update=1), {"lattice": "film 1024x1024x4", "nspins": s.nspins,
+                                                                  "exchange": "DIA J1+J2", "integrator": "rk4"}
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, max, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.out.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(k)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- reference arm
+def _ref_worker(args):
+    """One process: the reference llgCPU on a BCT-2 sample lattice, timed per step."""
+    cells, steps, warmup, seed = args
+    sys.path[:0] = [REPO, PKG]
+    import numpy as np  # noqa: F401
+    import asd_lattice as LT
+    from oracle import oracle as O
+    s = LT.bct2_antiferromagnet(cells, layout="csr", T=300.0)
+    r = O.RefLLGCPU(s, seed=(seed, seed + 100))
+    r.set_spins(LT.random_spins(s.nspins, seed))
+    r.step(warmup)
+    t0 = time.perf_counter()
+    r.step(steps)
+    return s.nspins, steps, time.perf_counter() - t0
+
+
+def cpu_reference(cells, steps, warmup, procs):
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_ref_worker, [(cells, steps, warmup, 1 + k) for k in range(procs)])
+    wall = max(r[2] for r in res)
+    total = sum(r[0] * r[1] for r in res)
+    return total / wall, res
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    procs = os.cpu_count() or 1
+    cells = 12
+    rate, res = cpu_reference(cells, args.steps, args.warmup, procs)
+    n = res[0][0]
+    line = {"metric": METRIC, "value": rate, "unit": "spin-updates/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * max(r[2] for r in res) / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "bct2_64 (CPU sample)", "nspins_per_process": n, "processes": procs},
+            "cpu_baseline": {"value": rate, "unit": "spin-updates/s", "cores": procs, "kind": "reference",
+                             "sample": f"reference llgCPU (src/llgCPU.cpp, compiled from source) on BCT-2 {cells}^3 "
+                                       f"cells ({n} spins, 26 nbrs, full 3x3 CSR, T=300 K), one independent "
+                                       f"replica per process x {procs} processes, {args.steps} steps each"},
+            "e2e": {"value": rate, "unit": "spin-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args):
+    import numpy as np
+    import asd_b200 as A
+    import asd_lattice as LT
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    else:
+        try:
+            import ctypes
+            ctypes.CDLL("libcudart.so.12").cudaSetDevice(local)
+        except OSError:
+            pass
+
+    systems, kw, cfg = make_workload(args.workload)
+    n = sum(s.nspins for s in systems)
+    S0 = LT.random_spins(n, 0)
+    flags = A.FLAG_COMPENSATED
+    p32 = A.RunParams(precision=A.FP32, seed=1 + rank, flags=flags, **kw)
+    h = A.Handle(p32, systems)
+    h.set_spins(S0)
+    h.step(args.warmup)
+    h.sync()
+
+    def barrier():
+        if dist:
+            import torch
+            t = torch.zeros(1, device="cuda")
+            dist.all_reduce(t)
+            torch.cuda.synchronize()
+
+    def allmax(v):
+        if not dist:
+            return v
+        import torch
+        t = torch.tensor([v], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    barrier()
+    with ClockSampler(local) as clk:
+        ms, launches = h.time_steps(args.steps)
+    barrier()
+    ms = allmax(ms)
+    value = n * world * args.steps / (ms * 1e-3)
+
+    # dominant kernel: per-launch CUDA-event time of the fused stage kernel
+    ks = h.time_kernels(max(4, min(args.steps, 20)))
+    peak, peak_kind = hbm_peak()
+    achieved = ks["bytes"] / (ks["avg_ms"] * 1e-3) / 1e9 if ks["avg_ms"] > 0 else None
+    traffic = ncu_traffic(args.workload)
+
+    # end to end through the C ABI with host buffers: upload spins, per step set the
+    # applied field (H2D) + step + magnetisation read-back (D2H), download spins
+    nsub_out = h.nrep * h.nsub * 3
+    he = A.Handle(p32, systems)
+    he.step(1)
+    he.sync()
+    barrier()
+    t0 = time.perf_counter()
+    he.set_spins(S0)
+    field = np.zeros(3)
+    for k in range(args.steps):
+        he.set_applied(field)
+        he.step(1)
+        he.magnetisation()
+    out = he.get_spins()
+    e2e_s = allmax(time.perf_counter() - t0)
+    barrier()
+    he.close()
+    e2e = {"value": n * world * args.steps / e2e_s, "unit": "spin-updates/s",
+           "h2d_bytes_per_step": (24 * n + 24 * args.steps) / args.steps,
+           "d2h_bytes_per_step": (24 * n + 8 * nsub_out * args.steps) / args.steps,
+           "calls_per_step": "asd_set_applied + asd_step(1) + asd_magnetisation", "host_buffers": "pageable numpy"}
+
+    # FP64 plain form on the same input, and the FP32 error against it on the same noise
+    plain = None
+    err = None
+    if not args.no_plain:
+        pp = A.RunParams(precision=A.FP64_PLAIN, seed=1 + rank, **kw)
+        hp = A.Handle(pp, systems)
+        hp.set_spins(S0)
+        kp = max(3, args.steps // 2)
+        hp.step(min(3, kp))
+        hp.sync()
+        msp, lp = hp.time_steps(kp)
+        msp = allmax(msp)
+        plain = {"value": n * world * kp / (msp * 1e-3), "ms_per_step": msp / kp, "steps": kp, "gpu_launches": lp}
+        hp.close()
+        ne = args.err_steps
+        ha = A.Handle(p32, systems)
+        hb = A.Handle(pp, systems)
+        ha.set_spins(S0)
+        hb.set_spins(S0)
+        ha.step(ne)
+        hb.step(ne)
+        err = {"max_abs_dS": float(np.abs(ha.get_spins() - hb.get_spins()).max()), "steps": ne,
+               "vs": "FP64 plain form, same initial spins and same Philox noise"}
+        ha.close()
+        hb.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            rate, res = cpu_reference(16, args.cpu_steps, 2, 1)
+            cpu = {"value": rate, "unit": "spin-updates/s", "cores": 1, "kind": "reference",
+                   "sample": f"reference llgCPU (src/llgCPU.cpp compiled from source) on BCT-2 16^3 cells "
+                             f"({res[0][0]} spins, same 26-neighbour full-tensor CSR, T=300 K), {args.cpu_steps} "
+                             f"steps, 1 thread"}
+        except Exception as e:  # the harness library is built by __graft_entry__.build()
+            cpu = {"value": None, "unit": "spin-updates/s", "cores": 1, "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "spin-updates/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict({"workload": args.workload}, **cfg, parallelism=f"replicas x{world}",
+                               l2="inputs larger than L2 (exchange matrix streamed every stage)",
+                               state="FP32 hi+lo spins, FP64 renormalisation"),
+                "e2e": e2e,
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                             "kernel": ks["name"], "kernel_avg_ms": ks["avg_ms"],
+                             "alg_bytes_per_launch": ks["bytes"], "peak_source": peak_kind},
+                "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
+                "fp64_plain": plain, "error_vs_fp64": err,
+                "speedup_vs_fp64_plain": (value / plain["value"]) if plain else None}
+        print(json.dumps(line), flush=True)
+    h.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="bct2_64")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=1500)
+    ap.add_argument("--err-steps", type=int, default=100)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -175,15 +175,25 @@ void setup_lr(asd_handle* h, const asd_system& s, bool plain) {
     }
     L.mesh_idx = dupload(idx.data(), idx.size());
     L.w = dupload(w.data(), w.size());
-    // symmetry of N_r decides 6 or 9 stored components
+    // symmetry of N_r (up to rounding of (3 e_a) e_b) decides 6 or 9 stored components;
+    // a symmetric matrix is stored as the mean of each (a,b),(b,a) pair
+    double amax = 0.0;
+    for (size_t q = 0; q < 9 * L.P; q++) amax = std::max(amax, std::fabs(s.nr[q]));
     bool sym = true;
-    for (size_t c = 0; c < L.P && sym; c++) {
-        if (s.nr[1 * L.P + c] != s.nr[3 * L.P + c] || s.nr[2 * L.P + c] != s.nr[6 * L.P + c] ||
-            s.nr[5 * L.P + c] != s.nr[7 * L.P + c])
-            sym = false;
-    }
+    const int pairs[3][2] = {{1, 3}, {2, 6}, {5, 7}};
+    for (size_t c = 0; c < L.P && sym; c++)
+        for (auto& pr : pairs)
+            if (std::fabs(s.nr[pr[0] * L.P + c] - s.nr[pr[1] * L.P + c]) > 1e-13 * amax) sym = false;
     L.ncomp = sym ? 6 : 9;
-    double* d_nr = dupload(s.nr, 9 * L.P);
+    std::vector<double> nrs(s.nr, s.nr + 9 * L.P);
+    if (sym)
+        for (size_t c = 0; c < L.P; c++)
+            for (auto& pr : pairs) {
+                const double m = 0.5 * (nrs[pr[0] * L.P + c] + nrs[pr[1] * L.P + c]);
+                nrs[pr[0] * L.P + c] = m;
+                nrs[pr[1] * L.P + c] = m;
+            }
+    double* d_nr = dupload(plain ? s.nr : nrs.data(), 9 * L.P);
     int dims[3] = {(int)L.mesh[0], (int)L.mesh[1], (int)L.mesh[2]};
     cudaError_t e;
     if (plain) {
@@ -224,11 +234,16 @@ void build_graph(asd_handle* h, uint32_t steps) {
     destroy_graph(h);
     cudaGraph_t g;
     const uint64_t before = h->launches;
+    // the captured launch pattern depends only on the step phase modulo the dipole
+    // refresh period; chunks are replayed from phase 0 (see run_steps)
+    const uint64_t saved = h->step;
+    h->step = 0;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
     for (uint32_t r = 0; r < steps && e == cudaSuccess; r++) e = launch_fused_step(h, r, true);
     if (e == cudaSuccess) e = launch_step_advance(h, steps);
     cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+    h->step = saved;
     h->graph_launches = h->launches - before;
     h->launches = before;
     CK(e);

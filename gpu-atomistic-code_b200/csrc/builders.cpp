@@ -62,7 +62,8 @@ int asd_build_csr(const uint32_t dim[3], const int pbc[3], uint32_t nauc, const 
 
 // Row-aligned DIA (data[c][d*N+row] = A[row][row+off[d]]), offsets ascending, built from
 // the occupied diagonals of the CSR pattern (src/matrix_conv.cpp:28-272,
-// src/exch_unitcell.cpp:374-391).  Offset N-1 is not representable there and is rejected.
+// src/exch_unitcell.cpp:374-391).  The reference's diagonal scan stops before offset N-1
+// (src/matrix_conv.cpp:43, src/exch_unitcell.cpp:413) and so drops that diagonal; it is kept here.
 int asd_csr_to_dia(uint32_t n, const uint32_t* xadj, const uint32_t* adjncy, const double* val9, int32_t* offsets,
                    double* data9, uint32_t* ndiag_out) {
     if (!xadj || !adjncy || !ndiag_out || n == 0) return ASD_EINVAL;
@@ -72,9 +73,8 @@ int asd_csr_to_dia(uint32_t n, const uint32_t* xadj, const uint32_t* adjncy, con
             if (adjncy[k] >= n) return ASD_EINVAL;
             occ[(size_t)n + adjncy[k] - i]++;
         }
-    if (occ[2 * (size_t)n - 1]) return ASD_ENOTSUP;
     std::vector<int32_t> off;
-    for (size_t q = 0; q + 1 < 2 * (size_t)n; q++)
+    for (size_t q = 0; q < 2 * (size_t)n; q++)
         if (occ[q]) off.push_back((int32_t)((int64_t)q - n));
     *ndiag_out = (uint32_t)off.size();
     if (!offsets) return ASD_OK;

@@ -165,8 +165,12 @@ int asd_num_sublattices(const asd_handle* h, uint32_t* nsub);
 /* Time nsteps asd_step calls on the device with CUDA events on the handle's stream;
  * *ms = elapsed milliseconds, *launches = kernels this library launched. */
 int asd_time_steps(asd_handle* h, uint64_t nsteps, double* ms, uint64_t* launches);
-/* Per-kernel device time of the dominant field/stage kernel in the last asd_time_steps
- * (CUDA events around each of its launches): average ms per launch and launch count. */
+/* Advance nsteps with direct (un-graphed) launches, bracketing every fused stage-kernel
+ * launch with CUDA events on the handle's stream; results via asd_kernel_stats.
+ * Measurement aid with no reference counterpart. */
+int asd_time_kernels(asd_handle* h, uint64_t nsteps);
+/* Per-kernel device time of the fused stage kernel in the last asd_time_kernels:
+ * average ms per launch, launch count and algorithmic bytes per launch. */
 int asd_kernel_stats(const asd_handle* h, char* name, size_t name_len, double* avg_ms, uint64_t* count,
                      double* bytes_per_launch);
 

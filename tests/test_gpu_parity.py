@@ -1,0 +1,234 @@
+"""Parity of the CUDA path (through the C ABI) with the FP64 oracle on the same seeded inputs.
+
+Tolerances:
+  FP64 plain form: bit-exact (identical operation order, no FMA contraction, same noise);
+  fused FP64 form: max|dS| <= 1e-10;
+  FP32 form:       max|dS| <= 1e-5 (north-star bound for the FP32 state vs FP64);
+  FFT paths (cuFFT rounding): FP64 <= 1e-10, FP32 <= 1e-5.
+"""
+import numpy as np
+import pytest
+
+import asd_b200 as A
+import asd_lattice as LT
+from helpers import maxdiff
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def pair(systems, steps, precision, integrator=A.HEUN, flags=0, dt=1e-16, seed=1, update=1, applied=(0, 0, 0),
+         spins=None, oracle_flags=None):
+    if not isinstance(systems, list):
+        systems = [systems]
+    n = sum(s.nspins for s in systems)
+    S0 = LT.random_spins(n, 0) if spins is None else spins
+    p = A.RunParams(integrator=integrator, precision=precision, dt=dt, seed=seed, update=update, flags=flags,
+                    applied=applied)
+    with A.Handle(p, systems) as h:
+        h.set_spins(S0)
+        h.step(steps)
+        g = h.get_spins()
+        det = h.get_det_field()
+    o = O.Oracle(systems, integrator=integrator, dt=dt, seed=seed, update=update, applied=applied,
+                 flags=(flags & 0xFFFF) if oracle_flags is None else oracle_flags)
+    o.set_spins(S0)
+    o.step(steps)
+    return g, o.spins(), det, o.det_field()
+
+
+def test_thermal_normals_bit_exact(gpu):
+    for seed, stream, step in [(1, 0, 0), (12345678901, 7, 2**33 + 5), (0, 95, 19999)]:
+        g = A.thermal_normals(seed, stream, step, 3000)
+        o = O.thermal_normals(seed, stream, 3000, step)
+        assert np.array_equal(g, o)
+
+
+@pytest.mark.parametrize("T", [0.0, 300.0])
+def test_plain_heun_csr_bit_exact(gpu, T):
+    s = LT.sc_ferromagnet(8, T=T)
+    g, o, dg, do = pair(s, 200, A.FP64_PLAIN)
+    assert np.array_equal(g, o), maxdiff(g, o)
+    assert np.array_equal(dg, do), maxdiff(dg, do)
+
+
+def test_plain_full_tensor_csr_and_dia_bit_exact(gpu):
+    s = LT.bct2_antiferromagnet(3, T=100.0)
+    g, o, _, _ = pair(s, 60, A.FP64_PLAIN)
+    assert np.array_equal(g, o), maxdiff(g, o)
+    s = LT.bct2_antiferromagnet(3, layout="dia", T=100.0)
+    g2, o2, _, _ = pair(s, 60, A.FP64_PLAIN)
+    assert np.array_equal(g2, o2), maxdiff(g2, o2)
+    s = LT.sc_ferromagnet(6, exch="dia", pbc=(1, 0, 1))
+    g3, o3, _, _ = pair(s, 100, A.FP64_PLAIN)
+    assert np.array_equal(g3, o3), maxdiff(g3, o3)
+
+
+def test_plain_gpu_quirk_flags_bit_exact(gpu):
+    s = LT.bct2_antiferromagnet(3)
+    g, o, _, _ = pair(s, 40, A.FP64_PLAIN, flags=A.FLAG_GPU_DZZ_FROM_DYY)
+    assert np.array_equal(g, o), maxdiff(g, o)
+    g0, _, _, _ = pair(s, 40, A.FP64_PLAIN)
+    assert maxdiff(g, g0) > 1e-8      # the Cdzz<-datayy upload bug changes the dynamics
+
+
+@pytest.mark.parametrize("integ", [A.RK4, A.RK5])
+@pytest.mark.parametrize("flags", [0, A.FLAG_RK_DOUBLE_RDT | A.FLAG_RK_STAGE_SPIN_MIXED])
+def test_plain_rk_bit_exact(gpu, integ, flags):
+    s = LT.sc_ferromagnet(6, J2=-2e-22, exch="dia", pbc=(1, 1, 0), T=50.0)
+    g, o, _, _ = pair(s, 50, A.FP64_PLAIN, integrator=integ, flags=flags, dt=5e-16)
+    assert np.array_equal(g, o), maxdiff(g, o)
+
+
+def test_fused_fp64_close(gpu):
+    s = LT.sc_ferromagnet(8, T=0.0)
+    g, o, _, _ = pair(s, 300, A.FP64_FUSED)
+    assert maxdiff(g, o) <= 1e-10
+    s = LT.bct2_antiferromagnet(3, T=0.0)
+    g, o, _, _ = pair(s, 100, A.FP64_FUSED)
+    assert maxdiff(g, o) <= 1e-10
+
+
+@pytest.mark.parametrize("flags", [0, A.FLAG_COMPENSATED])
+def test_fp32_sc_close(gpu, flags):
+    s = LT.sc_ferromagnet(10, T=0.0)
+    g, o, _, _ = pair(s, 1000, A.FP32, flags=flags)
+    assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
+
+
+def test_fp32_bct_full_csr_and_dia_close(gpu):
+    for layout in ("csr", "dia"):
+        s = LT.bct2_antiferromagnet(4, layout=layout, T=0.0)
+        g, o, _, _ = pair(s, 300, A.FP32, flags=A.FLAG_COMPENSATED)
+        assert maxdiff(g, o) <= 1e-5, (layout, maxdiff(g, o))
+
+
+@pytest.mark.parametrize("integ", [A.RK4, A.RK5])
+def test_fp32_rk_close(gpu, integ):
+    s = LT.sc_ferromagnet(8, J2=-2e-22, exch="dia", pbc=(1, 1, 0), T=0.0)
+    g, o, _, _ = pair(s, 200, A.FP32, integrator=integ, dt=5e-16, flags=A.FLAG_COMPENSATED)
+    assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
+
+
+def test_dipole_csr_plain_and_fp32(gpu):
+    s = LT.sc_ferromagnet(6, pbc=(0, 0, 0), dipole=True)
+    g, o, _, _ = pair(s, 40, A.FP64_PLAIN, update=1)
+    assert maxdiff(g, o) <= 1e-10, maxdiff(g, o)
+    g, o, _, _ = pair(s, 40, A.FP32, update=1, flags=A.FLAG_COMPENSATED)
+    assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
+    g, o, _, _ = pair(s, 40, A.FP32, update=5, flags=A.FLAG_COMPENSATED)
+    assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
+
+
+def test_fft_exchange_mode_plain_and_fp32(gpu):
+    s = LT.sc_fft(6)
+    g, o, _, _ = pair(s, 40, A.FP64_PLAIN)
+    assert maxdiff(g, o) <= 1e-10, maxdiff(g, o)
+    g, o, _, _ = pair(s, 40, A.FP32, flags=A.FLAG_COMPENSATED)
+    assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
+
+
+def test_field_readback_matches_oracle(gpu):
+    s = LT.bct2_antiferromagnet(3)
+    S0 = LT.random_spins(s.nspins, 4)
+    o = O.Oracle(s)
+    o.set_spins(S0)
+    ho = o.field()
+    for prec, tol in [(A.FP64_PLAIN, 0.0), (A.FP64_FUSED, 1e-12), (A.FP32, 1e-5)]:
+        with A.Handle(A.RunParams(precision=prec), s) as h:
+            h.set_spins(S0)
+            hg = h.get_field()
+        assert maxdiff(hg, ho) <= tol * np.abs(ho).max(), (prec, maxdiff(hg, ho))
+
+
+def test_replicas_batched_equal_individual(gpu):
+    reps = [LT.sc_ferromagnet(4, T=10.0, stream=0), LT.sc_ferromagnet(5, T=200.0, stream=1),
+            LT.sc_ferromagnet(3, T=0.0, stream=2)]
+    for prec in (A.FP64_PLAIN, A.FP32):
+        S = [LT.random_spins(r.nspins, 10 + k) for k, r in enumerate(reps)]
+        p = A.RunParams(precision=prec, seed=9)
+        with A.Handle(p, reps) as h:
+            h.set_spins(np.concatenate(S))
+            h.step(70)
+            gb = h.get_spins()
+            m = h.magnetisation()
+        off = 0
+        for k, r in enumerate(reps):
+            with A.Handle(p, r) as h1:
+                h1.set_spins(S[k])
+                h1.step(70)
+                g1 = h1.get_spins()
+            assert np.array_equal(gb[off:off + r.nspins], g1)
+            assert np.allclose(m[k, 0], g1.mean(axis=0), rtol=0, atol=1e-14)
+            off += r.nspins
+    o = O.Oracle(reps, seed=9)
+    o.set_spins(np.concatenate(S))
+    o.step(70)
+    with A.Handle(A.RunParams(precision=A.FP64_PLAIN, seed=9), reps) as h:
+        h.set_spins(np.concatenate(S))
+        h.step(70)
+        assert np.array_equal(h.get_spins(), o.spins())
+
+
+def test_site_field_ramp_bit_exact(gpu):
+    s = LT.sc_ferromagnet(5)
+    prof = np.random.default_rng(3).normal(size=(s.nspins, 3)) * 5.0
+    s.site_field = prof
+    S0 = LT.random_spins(s.nspins, 1)
+    o = O.Oracle(s)
+    o.set_spins(S0)
+    O.olib().orc_set_site_field(o.c, O._ptr(O.a64(prof), O.C.c_double), 0.25)
+    o.step(30)
+    with A.Handle(A.RunParams(precision=A.FP64_PLAIN), s) as h:
+        h.set_spins(S0)
+        h.set_site_field_scale(0.25)
+        h.step(30)
+        assert np.array_equal(h.get_spins(), o.spins())
+    with A.Handle(A.RunParams(precision=A.FP32, flags=A.FLAG_COMPENSATED), s) as h:
+        h.set_spins(S0)
+        h.set_site_field_scale(0.25)
+        h.step(30)
+        assert maxdiff(h.get_spins(), o.spins()) <= 1e-5
+
+
+def test_edge_cases(gpu):
+    # one spin, no exchange
+    s = A.SpinSystem(nspins=1, materials=[A.MaterialSpec()], exch=A.EXCH_NONE)
+    g, o, _, _ = pair(s, 50, A.FP64_PLAIN, applied=(0, 0, 3.0), spins=np.array([[1.0, 0, 0]]))
+    assert np.array_equal(g, o)
+    # ragged rows (open boundaries), rows with no neighbours, N not a multiple of 32
+    s = LT.sc_ferromagnet((3, 5, 7), pbc=(0, 0, 0))
+    xadj = s.xadj.copy()
+    adj = list(s.adjncy)
+    val = list(s.csr_val)
+    # isolate spin 0: drop its row entries and the entries pointing at it
+    keep = []
+    rows = []
+    for i in range(s.nspins):
+        r = [(j, v) for j, v in zip(adj[xadj[i]:xadj[i + 1]], val[xadj[i]:xadj[i + 1]]) if i != 0 and j != 0]
+        rows.append(r)
+    s.xadj = np.concatenate([[0], np.cumsum([len(r) for r in rows])]).astype(np.uint32)
+    s.adjncy = np.array([j for r in rows for j, _ in r], dtype=np.uint32)
+    s.csr_val = np.array([v for r in rows for _, v in r])
+    for prec, tol in [(A.FP64_PLAIN, 0.0), (A.FP32, 1e-5)]:
+        g, o, _, _ = pair(s, 100, prec)
+        assert maxdiff(g, o) <= tol
+
+
+def test_errors_are_reported_not_fatal(gpu):
+    s = LT.sc_ferromagnet(4)
+    with A.Handle(A.RunParams(precision=A.FP32), s) as h:
+        bad = LT.random_spins(s.nspins, 0)
+        bad[3, 1] = np.nan
+        with pytest.raises(A.AsdError) as e:
+            h.set_spins(bad)
+        assert e.value.code == A.ASD_ENOTFINITE
+        with pytest.raises(A.AsdError):
+            h.set_spins(np.zeros((s.nspins, 3)))
+        h.step(3)               # the handle is still usable
+    s2 = LT.sc_ferromagnet(4)
+    s2.adjncy = s2.adjncy.copy()
+    s2.adjncy[5] = 10**6
+    with pytest.raises(A.AsdError) as e:
+        A.Handle(A.RunParams(), s2)
+    assert e.value.code == A.ASD_EINVAL
