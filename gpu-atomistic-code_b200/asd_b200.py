@@ -112,7 +112,7 @@ def load_library(path: str = LIB_PATH):
         "asd_thermal_normals": ([C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, dp], C.c_int),
         "asd_build_csr": ([u32p, C.POINTER(C.c_int), C.c_uint32, dp, C.c_uint32, u32p, u32p, i32p, dp, C.c_double,
                            u32p, u32p, dp, u32p], C.c_int),
-        "asd_csr_to_dia": ([C.c_uint32, u32p, u32p, dp, i32p, dp, u32p], C.c_int),
+        "asd_csr_to_dia": ([C.c_uint32, u32p, u32p, dp, C.c_uint32, i32p, dp, u32p], C.c_int),
         "asd_build_dipole_nr": ([u32p, u32p, dp, C.c_double, C.c_double, dp], C.c_int),
         "asd_fold_exchange_nr": ([u32p, C.c_uint32, i32p, dp, C.c_double, dp, u32p], C.c_int),
     }
@@ -161,7 +161,7 @@ class SpinSystem:
     adjncy: Optional[np.ndarray] = None
     csr_val: Optional[np.ndarray] = None       # nnz x 9 [T]
     dia_offset: Optional[np.ndarray] = None
-    dia_val: Optional[np.ndarray] = None       # 9 x ndiag x n [T]
+    dia_val: Optional[np.ndarray] = None       # c x ndiag x n [T], c = 9 if full else 3 (xx,yy,zz)
     lr: int = LR_NONE
     mesh: Sequence[int] = (0, 0, 0)
     mesh_xyz: Optional[np.ndarray] = None      # n x 3

@@ -63,16 +63,17 @@ def build_csr(dim, pbc, mus, bond_atom, bond_to, bond_vec, bond_J):
     return xadj, adj[: nnz.value], val[: nnz.value]
 
 
-def csr_to_dia(n, xadj, adjncy, val9):
+def csr_to_dia(n, xadj, adjncy, val9, ncomp=9):
+    """CSR -> row-aligned DIA with ncomp (3: xx,yy,zz; 9: full) components per diagonal entry."""
     lib = A.load_library()
     xadj, adjncy = _u32(xadj), _u32(adjncy)
     val9 = np.ascontiguousarray(val9, dtype=np.float64)
     nd = C.c_uint32()
-    A._check(lib.asd_csr_to_dia(n, A._p(xadj, C.c_uint32), A._p(adjncy, C.c_uint32), A._p(val9, C.c_double),
+    A._check(lib.asd_csr_to_dia(n, A._p(xadj, C.c_uint32), A._p(adjncy, C.c_uint32), A._p(val9, C.c_double), ncomp,
                                 None, None, C.byref(nd)))
     off = np.zeros(nd.value, dtype=np.int32)
-    data = np.zeros((9, nd.value, n), dtype=np.float64)
-    A._check(lib.asd_csr_to_dia(n, A._p(xadj, C.c_uint32), A._p(adjncy, C.c_uint32), A._p(val9, C.c_double),
+    data = np.zeros((ncomp, nd.value, n), dtype=np.float64)
+    A._check(lib.asd_csr_to_dia(n, A._p(xadj, C.c_uint32), A._p(adjncy, C.c_uint32), A._p(val9, C.c_double), ncomp,
                                 A._p(off, C.c_int32), A._p(data, C.c_double), C.byref(nd)))
     return off, data
 
@@ -128,7 +129,7 @@ def sc_ferromagnet(L, J=J_SC, mu=MU_SC, lam=0.1, k1u=K1U_SC, pbc=(1, 1, 1), T=0.
     if exch == "csr":
         s.exch, s.xadj, s.adjncy, s.csr_val = A.EXCH_CSR, xadj, adj, val
     elif exch == "dia":
-        off, data = csr_to_dia(n, xadj, adj, val)
+        off, data = csr_to_dia(n, xadj, adj, val, ncomp=3)
         s.exch, s.dia_offset, s.dia_val = A.EXCH_DIA, off, data
     s.meta = {"dim": L, "pbc": tuple(pbc), "nnz": len(adj), "kind": "sc"}
     if dipole:
@@ -206,7 +207,7 @@ def film_dia(Lx, Ly, Lz, J1=1e-21, J2=-2e-22, mu=MU_SC, lam=1e-4, k1u=0.0, dipol
     Js = [_iso(J1)] * 6 + [_iso(J2)] * 12
     xadj, adj, val = build_csr(L, (1, 1, 0), [mu], [0] * 18, [0] * 18, vecs, Js)
     n = L[0] * L[1] * L[2]
-    off, data = csr_to_dia(n, xadj, adj, val)
+    off, data = csr_to_dia(n, xadj, adj, val, ncomp=3)
     s = A.SpinSystem(nspins=n, materials=[A.MaterialSpec(mu=mu, lam=lam, k1u=k1u)], exch=A.EXCH_DIA,
                      dia_offset=off, dia_val=data)
     xyz = sc_mesh_xyz(L).astype(np.float64)

@@ -423,7 +423,11 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
             REQUIRE(nsys == 1, "DIA exchange supports one replica per handle");
             REQUIRE(s0.ndiag == 0 || (s0.dia_offset && s0.dia_val), "DIA arrays missing");
             doff.assign(s0.dia_offset, s0.dia_offset + s0.ndiag);
-            dval.assign(s0.dia_val, s0.dia_val + 9 * (size_t)s0.ndiag * n);
+            // expand to the 9-component working copy (xx,yy,zz in 0,4,8 for the diagonal form)
+            const size_t m9 = (size_t)s0.ndiag * n;
+            dval.assign(9 * m9, 0.0);
+            if (h->full) std::copy(s0.dia_val, s0.dia_val + 9 * m9, dval.begin());
+            else for (int q = 0; q < 3; q++) std::copy(s0.dia_val + q * m9, s0.dia_val + (q + 1) * m9, dval.begin() + 4 * q * m9);
             size_t nz = 0;
             for (uint32_t d = 0; d < s0.ndiag; d++)
                 for (uint32_t i = 0; i < n; i++) {

@@ -64,9 +64,10 @@ int asd_build_csr(const uint32_t dim[3], const int pbc[3], uint32_t nauc, const 
 // the occupied diagonals of the CSR pattern (src/matrix_conv.cpp:28-272,
 // src/exch_unitcell.cpp:374-391).  The reference's diagonal scan stops before offset N-1
 // (src/matrix_conv.cpp:43, src/exch_unitcell.cpp:413) and so drops that diagonal; it is kept here.
-int asd_csr_to_dia(uint32_t n, const uint32_t* xadj, const uint32_t* adjncy, const double* val9, int32_t* offsets,
-                   double* data9, uint32_t* ndiag_out) {
-    if (!xadj || !adjncy || !ndiag_out || n == 0) return ASD_EINVAL;
+int asd_csr_to_dia(uint32_t n, const uint32_t* xadj, const uint32_t* adjncy, const double* val9, uint32_t ncomp,
+                   int32_t* offsets, double* data9, uint32_t* ndiag_out) {
+    if (!xadj || !adjncy || !ndiag_out || n == 0 || (ncomp != 3 && ncomp != 9)) return ASD_EINVAL;
+    static const int q3[3] = {0, 4, 8};
     std::vector<uint32_t> occ(2 * (size_t)n, 0);
     for (uint32_t i = 0; i < n; i++)
         for (uint32_t k = xadj[i]; k < xadj[i + 1]; k++) {
@@ -81,14 +82,15 @@ int asd_csr_to_dia(uint32_t n, const uint32_t* xadj, const uint32_t* adjncy, con
     if (!data9 || !val9) return ASD_EINVAL;
     memcpy(offsets, off.data(), off.size() * sizeof(int32_t));
     const size_t m = off.size() * (size_t)n;
-    memset(data9, 0, 9 * m * sizeof(double));
+    memset(data9, 0, ncomp * m * sizeof(double));
     std::vector<int32_t> slot(2 * (size_t)n, -1);
     for (size_t d = 0; d < off.size(); d++) slot[(size_t)((int64_t)off[d] + n)] = (int32_t)d;
     for (uint32_t i = 0; i < n; i++)
         for (uint32_t k = xadj[i]; k < xadj[i + 1]; k++) {
             const size_t d = (size_t)slot[(size_t)n + adjncy[k] - i];
             // a later entry for the same column replaces an earlier one (as the reference scan does)
-            for (int q = 0; q < 9; q++) data9[(size_t)q * m + d * n + i] = val9[9 * (size_t)k + q];
+            for (uint32_t q = 0; q < ncomp; q++)
+                data9[(size_t)q * m + d * n + i] = val9[9 * (size_t)k + (ncomp == 3 ? q3[q] : (int)q)];
         }
     return ASD_OK;
 }

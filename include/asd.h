@@ -109,7 +109,7 @@ typedef struct asd_system {
     /* DIA (exch == ASD_EXCH_DIA): exch::diagoffset / data**, row-aligned data[c][n*N+row] */
     uint32_t ndiag;
     const int32_t* dia_offset;      /* ndiag */
-    const double* dia_val;          /* 9 x ndiag x nspins [T] */
+    const double* dia_val;          /* c x ndiag x nspins [T]: c=3 (xx,yy,zz) if !exch_full, else 9 */
     /* Long-range field on the zero-padded mesh (intmat::dipNrab / Nrab before the FFT). */
     uint32_t lr;                    /* ASD_LR_* */
     uint32_t mesh[3];               /* padded mesh 2*dim*Nm per axis */
@@ -186,10 +186,11 @@ int asd_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t 
 int asd_build_csr(const uint32_t dim[3], const int pbc[3], uint32_t nauc, const double* mu,
                   uint32_t nbond, const uint32_t* bond_atom, const uint32_t* bond_to, const int32_t* bond_vec,
                   const double* bond_J, double muB, uint32_t* xadj, uint32_t* adjncy, double* val, uint32_t* nnz);
-/* matconv::csr_to_dia_* (src/matrix_conv.cpp:28-272): returns ndiag in *ndiag; pass
- * offsets/data = NULL to count only. */
-int asd_csr_to_dia(uint32_t n, const uint32_t* xadj, const uint32_t* adjncy, const double* val9,
-                   int32_t* offsets, double* data9, uint32_t* ndiag);
+/* matconv::csr_to_dia_diag / csr_to_dia_offdiag (src/matrix_conv.cpp:28-272): returns ndiag in
+ * *ndiag; data is ncomp x ndiag x n with ncomp 3 (xx,yy,zz) or 9; pass offsets/data = NULL to
+ * count only. */
+int asd_csr_to_dia(uint32_t n, const uint32_t* xadj, const uint32_t* adjncy, const double* val9, uint32_t ncomp,
+                   int32_t* offsets, double* data, uint32_t* ndiag);
 /* intmat::fillDipIntmat / fillIntmat (src/intmat.cpp:188-331): nr[3][3][2dim*nk] (+=). */
 int asd_build_dipole_nr(const uint32_t dim[3], const uint32_t nk[3], const double abc[3], double muB,
                         double mu_scale, double* nr);

@@ -324,7 +324,18 @@ int orc_set_noise(orc_ctx* c, int mode, uint64_t seed, uint32_t mwc_a, uint32_t 
     return 0;
 }
 
-int orc_set_spins(orc_ctx* c, const double* s) { memcpy(c->s, s, 3 * (size_t)c->n * sizeof(double)); return 0; }
+static void normalise(double v[3]);
+
+/* Spins are normalised on entry, s/|s| with |s| = sqrt(x*x+y*y+z*z), as the
+ * reference does for spins read from a file (src/spins.cpp:388-392). */
+int orc_set_spins(orc_ctx* c, const double* s) {
+    for (uint32_t i = 0; i < c->n; i++) {
+        double v[3] = {s[3 * (size_t)i], s[3 * (size_t)i + 1], s[3 * (size_t)i + 2]};
+        normalise(v);
+        memcpy(c->s + 3 * (size_t)i, v, sizeof(v));
+    }
+    return 0;
+}
 int orc_get_spins(const orc_ctx* c, double* s) { memcpy(s, c->s, 3 * (size_t)c->n * sizeof(double)); return 0; }
 int orc_get_det_field(const orc_ctx* c, double* h) { memcpy(h, c->det, 3 * (size_t)c->n * sizeof(double)); return 0; }
 

@@ -109,6 +109,16 @@ def au32(x):
     return None if x is None else np.ascontiguousarray(x, dtype=np.uint32)
 
 
+def expand_dia(s):
+    """9-component DIA values (the diagonal form carries xx,yy,zz only)."""
+    v = np.asarray(s.dia_val)
+    if v.shape[0] == 9:
+        return v
+    out = np.zeros((9,) + v.shape[1:])
+    out[[0, 4, 8]] = v
+    return out
+
+
 class Oracle:
     """FP64 CPU restatement of the step for one handle's worth of spins."""
 
@@ -173,7 +183,7 @@ class Oracle:
                           _ptr(val, C.c_double))
         elif s0.exch == 1:  # DIA
             doff = np.ascontiguousarray(s0.dia_offset, dtype=np.int32)
-            dval = a64(s0.dia_val)
+            dval = a64(expand_dia(s0))
             self._keep += [doff, dval]
             L.orc_set_dia(self.c, 1 if s0.full else 0, len(doff), _ptr(doff, C.c_int32), _ptr(dval, C.c_double))
         if s0.site_field is not None:
@@ -293,7 +303,7 @@ class RefLLGCPU:
                            _ptr(val, C.c_double))
         elif s.exch == 1:
             off = np.ascontiguousarray(s.dia_offset, dtype=np.int32)
-            val = a64(s.dia_val)
+            val = a64(expand_dia(s))
             self._keep = [off, val]
             L.refh_set_dia(1 if s.full else 0, len(off), _ptr(off, C.c_int32), _ptr(val, C.c_double),
                            len(off))

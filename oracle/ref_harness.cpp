@@ -222,9 +222,13 @@ int refh_set_site_fields(const double* hstag, const double* hdemag) {
     return 0;
 }
 
+// Initial spins as the reference's restart_text reader stores them: each
+// vector divided by its length (src/spins.cpp:384-392).
 int refh_set_spins(const double* s) {
     for (unsigned i = 0; i < geom::nspins; i++) {
         spins::Sx[i] = s[3 * i]; spins::Sy[i] = s[3 * i + 1]; spins::Sz[i] = s[3 * i + 2];
+        const double mods = sqrt(spins::Sx[i] * spins::Sx[i] + spins::Sy[i] * spins::Sy[i] + spins::Sz[i] * spins::Sz[i]);
+        spins::Sx[i] /= mods; spins::Sy[i] /= mods; spins::Sz[i] /= mods;
     }
     return 0;
 }

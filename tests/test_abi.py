@@ -116,6 +116,8 @@ def test_csr_to_dia_matches_oracle_restatement():
         L.orc_csr_to_dia(n, O._ptr(xadj, C.c_uint32), O._ptr(adj, C.c_uint32), O._ptr(val, C.c_double),
                          O._ptr(off2, C.c_int32), O._ptr(data2, C.c_double))
         assert np.array_equal(off, off2) and np.array_equal(data, data2)
+        off3, data3 = LT.csr_to_dia(n, s.xadj, s.adjncy, s.csr_val, ncomp=3)
+        assert np.array_equal(off3, off2) and np.array_equal(data3, data2[[0, 4, 8]])
 
 
 def test_dipole_nr_matches_oracle_restatement():
@@ -155,4 +157,4 @@ def test_builder_rejects_bad_input():
     xadj = np.array([0, 1], np.uint32)
     adj = np.array([5], np.uint32)  # out of range
     nd = C.c_uint32()
-    assert lib.asd_csr_to_dia(1, A._p(xadj, C.c_uint32), A._p(adj, C.c_uint32), None, None, None, C.byref(nd)) == A.ASD_EINVAL
+    assert lib.asd_csr_to_dia(1, A._p(xadj, C.c_uint32), A._p(adj, C.c_uint32), None, 9, None, None, C.byref(nd)) == A.ASD_EINVAL
