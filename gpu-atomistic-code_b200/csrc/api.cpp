@@ -398,7 +398,6 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         std::vector<uint32_t> xadj(1, 0), adj;
         std::vector<double> val9;
         std::vector<int32_t> doff;
-        std::vector<double> dval;  // 9 x ndiag x n
         if (h->exch == ASD_EXCH_CSR) {
             for (uint32_t r = 0; r < nsys; r++) {
                 const asd_system& s = sys[r];
@@ -423,24 +422,28 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
             REQUIRE(nsys == 1, "DIA exchange supports one replica per handle");
             REQUIRE(s0.ndiag == 0 || (s0.dia_offset && s0.dia_val), "DIA arrays missing");
             doff.assign(s0.dia_offset, s0.dia_offset + s0.ndiag);
-            // expand to the 9-component working copy (xx,yy,zz in 0,4,8 for the diagonal form)
-            const size_t m9 = (size_t)s0.ndiag * n;
-            dval.assign(9 * m9, 0.0);
-            if (h->full) std::copy(s0.dia_val, s0.dia_val + 9 * m9, dval.begin());
-            else for (int q = 0; q < 3; q++) std::copy(s0.dia_val + q * m9, s0.dia_val + (q + 1) * m9, dval.begin() + 4 * q * m9);
             size_t nz = 0;
+            const size_t m = (size_t)s0.ndiag * n;
+            const int nc = h->full ? 9 : 3;
             for (uint32_t d = 0; d < s0.ndiag; d++)
                 for (uint32_t i = 0; i < n; i++) {
                     const int64_t col = (int64_t)i + doff[d];
                     if (col < 0 || col >= (int64_t)n) continue;
                     bool any = false;
-                    for (int q = 0; q < 9; q++) any |= dval[(size_t)q * s0.ndiag * n + (size_t)d * n + i] != 0.0;
+                    for (int q = 0; q < nc; q++) any |= s0.dia_val[(size_t)q * m + (size_t)d * n + i] != 0.0;
                     nz += any;
                 }
             h->nnz_per_row = (double)nz / n;
         }
         const bool plain = p.precision == ASD_FP64_PLAIN;
         const bool zz_yy = (p.flags & ASD_FLAG_GPU_DZZ_FROM_DYY) != 0;
+        // component q (row-major alpha,beta) of the caller's DIA values; the diagonal form
+        // carries only xx, yy, zz (q = 0, 4, 8)
+        const size_t mdia = (size_t)s0.ndiag * n;
+        auto dia_comp = [&](int q) -> const double* {
+            if (h->full) return s0.dia_val + (size_t)q * mdia;
+            return (q % 4 == 0) ? s0.dia_val + (size_t)(q / 4) * mdia : nullptr;
+        };
         if (plain) {
             // reference-structured arrays: per-spin parameters, separate component arrays
             std::vector<double> sig(n), lpf(n), lam(n), k1(n), k1d(3 * (size_t)n);
@@ -468,8 +471,8 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
             } else if (h->exch == ASD_EXCH_DIA) {
                 h->pex.ndiag = s0.ndiag;
                 h->pex.off = dupload(doff.data(), doff.size());
-                const size_t m = (size_t)s0.ndiag * n;
-                for (int q = 0; q < 9; q++) h->pex.v[q] = dupload(dval.data() + q * m, m);
+                for (int q = 0; q < 9; q++)
+                    if (dia_comp(q)) h->pex.v[q] = dupload(dia_comp(q), mdia);
             }
             (void)zz_yy;  // applied inside the plain kernels
         } else {
@@ -499,14 +502,16 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
                     std::vector<float> v(nc * m);
                     for (int q = 0; q < nc; q++) {
                         int src = h->full ? (q == 8 && zz_yy ? 4 : q) : qmap3[q];
-                        for (size_t k = 0; k < m; k++) v[q * m + k] = (float)dval[(size_t)src * m + k];
+                        const double* sp = dia_comp(src);
+                        for (size_t k = 0; k < m; k++) v[q * m + k] = (float)sp[k];
                     }
                     h->dia.valf = dupload(v.data(), v.size());
                 } else {
                     std::vector<double> v(nc * m);
                     for (int q = 0; q < nc; q++) {
                         int src = h->full ? (q == 8 && zz_yy ? 4 : q) : qmap3[q];
-                        for (size_t k = 0; k < m; k++) v[q * m + k] = dval[(size_t)src * m + k];
+                        const double* sp = dia_comp(src);
+                        for (size_t k = 0; k < m; k++) v[q * m + k] = sp[k];
                     }
                     h->dia.vald = dupload(v.data(), v.size());
                 }
