@@ -110,6 +110,8 @@ def load_library(path: str = LIB_PATH):
         "asd_time_kernels": ([P, C.c_uint64], C.c_int),
         "asd_kernel_stats": ([P, C.c_char_p, C.c_size_t, dp, C.POINTER(C.c_uint64), dp], C.c_int),
         "asd_thermal_normals": ([C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, dp], C.c_int),
+        "asd_magnetisation_noalloc": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p],
+                                      C.c_int),
         "asd_build_csr": ([u32p, C.POINTER(C.c_int), C.c_uint32, dp, C.c_uint32, u32p, u32p, i32p, dp, C.c_double,
                            u32p, u32p, dp, u32p], C.c_int),
         "asd_csr_to_dia": ([C.c_uint32, u32p, u32p, dp, C.c_uint32, i32p, dp, u32p], C.c_int),
