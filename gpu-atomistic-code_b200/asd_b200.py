@@ -29,6 +29,7 @@ FLAG_GPU_DZZ_FROM_DYY = 1 << 6
 FLAG_GPU_HDEMAG_FP32 = 1 << 7
 FLAG_COMPENSATED = 1 << 16
 FLAG_AUTOTUNE = 1 << 17
+FLAG_STREAMED_EXCHANGE = 1 << 18
 ALL_REPLICAS = 0xFFFFFFFF
 
 MUB, KB, GYRO = 9.27e-24, 1.38e-23, 1.76e11  # reference constants (src/llg.cpp:25)
@@ -112,6 +113,7 @@ def load_library(path: str = LIB_PATH):
         "asd_thermal_normals": ([C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, dp], C.c_int),
         "asd_magnetisation_noalloc": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p],
                                       C.c_int),
+        "asd_thermal_normals_f32": ([C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(C.c_float)], C.c_int),
         "asd_build_csr": ([u32p, C.POINTER(C.c_int), C.c_uint32, dp, C.c_uint32, u32p, u32p, i32p, dp, C.c_double,
                            u32p, u32p, dp, u32p], C.c_int),
         "asd_csr_to_dia": ([C.c_uint32, u32p, u32p, dp, C.c_uint32, i32p, dp, u32p], C.c_int),
@@ -347,6 +349,12 @@ class Handle:
 def thermal_normals(seed: int, stream: int, step: int, nspins: int) -> np.ndarray:
     out = np.empty(3 * nspins, dtype=np.float64)
     _check(load_library().asd_thermal_normals(seed, stream, step, nspins, _p(out, C.c_double)))
+    return out.reshape(nspins, 3)
+
+
+def thermal_normals_f32(seed: int, stream: int, step: int, nspins: int) -> np.ndarray:
+    out = np.empty(3 * nspins, dtype=np.float32)
+    _check(load_library().asd_thermal_normals_f32(seed, stream, step, nspins, out.ctypes.data_as(C.POINTER(C.c_float))))
     return out.reshape(nspins, 3)
 
 

@@ -3,6 +3,8 @@
 // CUDA-graph chunks for the fused forms), read-backs and timing.
 #include "internal.h"
 #include <algorithm>
+#include <array>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -64,7 +66,8 @@ void free_all(asd_handle* h) {
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
-    F(h->dia.off); F(h->dia.valf); F(h->dia.vald);
+    F(h->sell.typed); F(h->sell.tab_f); F(h->sell.tab_d);
+    F(h->dia.off); F(h->dia.valf); F(h->dia.vald); F(h->dia.dtype); F(h->dia.tab_f); F(h->dia.tab_d);
     F(h->p_s); F(h->p_es); F(h->p_fn); F(h->p_ch); F(h->p_hdemag); F(h->p_rand); F(h->p_det); F(h->p_hstg); F(h->p_hinit);
     for (int q = 0; q < 6; q++) F(h->p_k[q]);
     F(h->p_sigma); F(h->p_llgpf); F(h->p_lambda); F(h->p_k1u); F(h->p_k1udir);
@@ -81,6 +84,48 @@ void free_all(asd_handle* h) {
     if (h->kev[1]) cudaEventDestroy(h->kev[1]);
     if (h->stream) cudaStreamDestroy(h->stream);
 }
+
+// Distinct tensors of an exchange matrix (id 0 = the zero tensor), at most 256.
+struct TensorTable {
+    int nc;
+    std::map<std::array<double, 9>, uint32_t> ids;
+    std::vector<std::array<double, 9>> list;
+    std::array<double, 9> last{};
+    int64_t last_id = 0;
+    explicit TensorTable(int ncomp) : nc(ncomp) {
+        std::array<double, 9> z{};
+        ids[z] = 0;
+        list.push_back(z);
+    }
+    int64_t id(const std::array<double, 9>& key) {
+        if (key == last) return last_id;
+        auto it = ids.find(key);
+        int64_t t;
+        if (it != ids.end()) t = it->second;
+        else {
+            if (list.size() >= 256) return -1;
+            t = (int64_t)list.size();
+            ids[key] = (uint32_t)t;
+            list.push_back(key);
+        }
+        last = key;
+        last_id = t;
+        return t;
+    }
+    uint32_t size() const { return (uint32_t)list.size(); }
+    uint32_t bits() const {
+        uint32_t b = 1;
+        while ((1u << b) < list.size()) b++;
+        return b;
+    }
+    template <typename T>
+    std::vector<T> table() const {   // component-major [nc][ntypes]
+        std::vector<T> t((size_t)nc * list.size());
+        for (size_t k = 0; k < list.size(); k++)
+            for (int q = 0; q < nc; q++) t[(size_t)q * list.size() + k] = (T)list[k][q];
+        return t;
+    }
+};
 
 // CSR (all replicas concatenated) -> SELL-32 device layout.
 void build_sell(asd_handle* h, const std::vector<uint32_t>& xadj, const std::vector<uint32_t>& adj,
@@ -103,6 +148,45 @@ void build_sell(asd_handle* h, const std::vector<uint32_t>& xadj, const std::vec
         if (q == 8 && zz_yy) q = 4;
         return val9[9 * (size_t)k + q];
     };
+    // typed layout: (column, tensor id) in one word when the matrix has few distinct tensors
+    if (!(h->p.flags & ASD_FLAG_STREAMED_EXCHANGE)) {
+        const int nc = full ? 9 : 3;
+        const int qmap[9] = {0, 4, 8, 0, 0, 0, 0, 0, 0};
+        TensorTable tt(nc);
+        std::vector<uint32_t> id(adj.size());
+        bool ok = true;
+        for (size_t k = 0; k < adj.size() && ok; k++) {
+            std::array<double, 9> key{};
+            for (int q = 0; q < nc; q++) key[q] = value((uint32_t)k, full ? q : qmap[q]);
+            const int64_t t = tt.id(key);
+            if (t < 0) ok = false; else id[k] = (uint32_t)t;
+        }
+        const uint32_t tb = tt.bits();
+        if (ok && (uint64_t)n <= (1ull << (32 - tb))) {
+            std::vector<uint32_t> w(E);
+            for (uint32_t s = 0; s < ns; s++) {
+                const uint32_t wd = (sp[s + 1] - sp[s]) / 32;
+                for (uint32_t k = 0; k < wd; k++)
+                    for (uint32_t lane = 0; lane < 32; lane++) {
+                        const uint32_t r = 32 * s + lane, e = sp[s] + 32 * k + lane;
+                        uint32_t col = r < n ? r : 0, t = 0;
+                        if (r < n && k < xadj[r + 1] - xadj[r]) { col = adj[xadj[r] + k]; t = id[xadj[r] + k]; }
+                        w[e] = col | (t << (32 - tb));
+                    }
+            }
+            h->sell.typed = dupload(w.data(), w.size());
+            h->sell.colbits = 32 - tb;
+            h->sell.ntypes = tt.size();
+            if (h->p.precision == ASD_FP32) {
+                std::vector<float> tf = tt.table<float>();
+                h->sell.tab_f = dupload(tf.data(), tf.size());
+            } else {
+                std::vector<double> td = tt.table<double>();
+                h->sell.tab_d = dupload(td.data(), td.size());
+            }
+            return;
+        }
+    }
     if (h->p.precision == ASD_FP32) {
         std::vector<float4> a(E), b(full ? E : 0);
         std::vector<float2> c(full ? E : 0);
@@ -498,7 +582,30 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
                 const size_t m = (size_t)s0.ndiag * n;
                 const int nc = h->full ? 9 : 3;
                 const int qmap3[3] = {0, 4, zz_yy ? 4 : 8};
-                if (bytes == 4) {
+                bool typed = false;
+                if (!(p.flags & ASD_FLAG_STREAMED_EXCHANGE)) {
+                    // typed DIA: one id byte per (diagonal, row) into the distinct tensors
+                    TensorTable tt(nc);
+                    std::vector<uint8_t> ids(m, 0);
+                    const double* comp[9];
+                    for (int q = 0; q < nc; q++) comp[q] = dia_comp(h->full ? (q == 8 && zz_yy ? 4 : q) : qmap3[q]);
+                    bool ok = true;
+                    for (size_t k = 0; k < m && ok; k++) {
+                        std::array<double, 9> key{};
+                        for (int q = 0; q < nc; q++) key[q] = comp[q][k];
+                        const int64_t t = tt.id(key);
+                        if (t < 0) ok = false; else ids[k] = (uint8_t)t;
+                    }
+                    if (ok) {
+                        h->dia.dtype = dupload(ids.data(), ids.size());
+                        h->dia.ntypes = tt.size();
+                        if (bytes == 4) { std::vector<float> tf = tt.table<float>(); h->dia.tab_f = dupload(tf.data(), tf.size()); }
+                        else { std::vector<double> td = tt.table<double>(); h->dia.tab_d = dupload(td.data(), td.size()); }
+                        typed = true;
+                    }
+                }
+                if (typed) {
+                } else if (bytes == 4) {
                     std::vector<float> v(nc * m);
                     for (int q = 0; q < nc; q++) {
                         int src = h->full ? (q == 8 && zz_yy ? 4 : q) : qmap3[q];
@@ -835,6 +942,16 @@ int asd_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t 
     if (cudaMalloc(&d, 3 * (size_t)nspins * sizeof(double)) != cudaSuccess) return ASD_ENOMEM;
     cudaError_t e = launch_thermal_normals(seed, stream, step, nspins, d, 0);
     if (e == cudaSuccess) e = cudaMemcpy(out, d, 3 * (size_t)nspins * sizeof(double), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? ASD_OK : ASD_ECUDA;
+}
+
+int asd_thermal_normals_f32(uint64_t seed, uint32_t stream, uint64_t step, uint32_t nspins, float* out) {
+    if (!out || nspins == 0) return ASD_EINVAL;
+    float* d = nullptr;
+    if (cudaMalloc(&d, 3 * (size_t)nspins * sizeof(float)) != cudaSuccess) return ASD_ENOMEM;
+    cudaError_t e = launch_thermal_normals_f(seed, stream, step, nspins, d, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d, 3 * (size_t)nspins * sizeof(float), cudaMemcpyDeviceToHost);
     cudaFree(d);
     return e == cudaSuccess ? ASD_OK : ASD_ECUDA;
 }

@@ -159,4 +159,73 @@ __device__ __forceinline__ void thermal_normals(uint64_t seed, uint32_t stream, 
     out[2] = __dmul_rn(r2, c3);
 }
 
+// Single-precision variant for the FP32 form: the same Philox draw, 23-bit uniforms
+// u = ((x >> 9) + 0.5) 2^-23 (exact in float), and shorter series evaluated with
+// correctly rounded float operations (ln: terms to f^11; sin to psi^11, cos to psi^12),
+// accurate to a few float ulps and reproducible on any IEEE-754 float implementation.
+__device__ __forceinline__ float series_logf(float x) {
+    int e;
+    float m = frexpf(x, &e);
+    if (m < 0x1.6a09e6p-1f) { m = __fmul_rn(m, 2.0f); e = e - 1; }
+    const float f = __fdiv_rn(__fsub_rn(m, 1.0f), __fadd_rn(m, 1.0f));
+    const float f2 = __fmul_rn(f, f);
+    float p = 0x1.745d18p-4f;               // 1/11
+    p = __fmaf_rn(p, f2, 0x1.c71c72p-4f);   // 1/9
+    p = __fmaf_rn(p, f2, 0x1.24924ap-3f);   // 1/7
+    p = __fmaf_rn(p, f2, 0x1.99999ap-3f);   // 1/5
+    p = __fmaf_rn(p, f2, 0x1.555556p-2f);   // 1/3
+    p = __fmaf_rn(p, f2, 1.0f);
+    const float lnm = __fmul_rn(2.0f, __fmul_rn(f, p));
+    return __fmaf_rn((float)e, 0x1.62e430p-1f, lnm);
+}
+
+__device__ __forceinline__ void series_sincos_2pi_f(uint32_t x, float& sn, float& cs) {
+    const float v = __fmul_rn(__fadd_rn((float)(x >> 9), 0.5f), 0x1p-20f);   // 8u, exact
+    const float qd = floorf(v);
+    const int q = (int)qd;
+    const float r = __fsub_rn(v, qd);
+    const float psi = __fmul_rn((q & 1) ? __fsub_rn(1.0f, r) : r, 0x1.921fb6p-1f);
+    const float mp2 = -__fmul_rn(psi, psi);
+    float sp = 0x1.ae6456p-26f;               // 1/11!
+    sp = __fmaf_rn(sp, mp2, 0x1.71de3ap-19f); // 1/9!
+    sp = __fmaf_rn(sp, mp2, 0x1.a01a02p-13f); // 1/7!
+    sp = __fmaf_rn(sp, mp2, 0x1.111112p-7f);  // 1/5!
+    sp = __fmaf_rn(sp, mp2, 0x1.555556p-3f);  // 1/3!
+    sp = __fmaf_rn(sp, mp2, 1.0f);
+    const float s = __fmul_rn(psi, sp);
+    float cp = 0x1.1eed8ep-29f;               // 1/12!
+    cp = __fmaf_rn(cp, mp2, 0x1.27e4fcp-22f); // 1/10!
+    cp = __fmaf_rn(cp, mp2, 0x1.a01a02p-16f); // 1/8!
+    cp = __fmaf_rn(cp, mp2, 0x1.6c16c2p-10f); // 1/6!
+    cp = __fmaf_rn(cp, mp2, 0x1.555556p-5f);  // 1/4!
+    cp = __fmaf_rn(cp, mp2, 0x1.000000p-1f);  // 1/2!
+    const float c = __fmaf_rn(cp, mp2, 1.0f);
+    switch (q) {
+    case 0: sn = s;  cs = c;  break;
+    case 1: sn = c;  cs = s;  break;
+    case 2: sn = c;  cs = -s; break;
+    case 3: sn = s;  cs = -c; break;
+    case 4: sn = -s; cs = -c; break;
+    case 5: sn = -c; cs = -s; break;
+    case 6: sn = -c; cs = s;  break;
+    default: sn = -s; cs = c; break;
+    }
+}
+
+__device__ __forceinline__ void thermal_normals_f(uint64_t seed, uint32_t stream, uint32_t spin, uint64_t step,
+                                                  float out[3]) {
+    uint32_t c[4] = {spin, (uint32_t)step, (uint32_t)(step >> 32), stream};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const float u0 = __fmul_rn(__fadd_rn((float)(c[0] >> 9), 0.5f), 0x1p-23f);
+    const float u2 = __fmul_rn(__fadd_rn((float)(c[2] >> 9), 0.5f), 0x1p-23f);
+    const float r0 = __fsqrt_rn(__fmul_rn(-2.0f, series_logf(u0)));
+    const float r2 = __fsqrt_rn(__fmul_rn(-2.0f, series_logf(u2)));
+    float s1, c1, s3, c3;
+    series_sincos_2pi_f(c[1], s1, c1);
+    series_sincos_2pi_f(c[3], s3, c3);
+    out[0] = __fmul_rn(r0, c1);
+    out[1] = __fmul_rn(r0, s1);
+    out[2] = __fmul_rn(r2, c3);
+}
+
 }  // namespace asd

@@ -1,22 +1,18 @@
 // Fused stage kernels: one bandwidth-bound pass per integrator stage that
-// gathers the exchange field (SELL-32 or DIA layout), adds the long-range,
-// site, thermal (in-kernel Philox), applied and anisotropy fields, forms the
-// LLG torque and writes the next stage spin renormalised in FP64.  The same
-// templates serve the FP32 form (R=float) and the fused FP64 form (R=double).
+// gathers the exchange field (SELL-32 or DIA layout, streamed or typed), adds
+// the long-range, site, thermal (in-kernel Philox), applied and anisotropy
+// fields, forms the LLG torque and writes the next stage spin renormalised in
+// FP64.  The same templates serve the FP32 form (R=float) and the fused FP64
+// form (R=double).
 //
 // Reference computation per stage: the field kernel CSpMV_* / CCopyFields
 // (src/cufields.cu:97-246, 386-407) followed by CHeun1/CHeun2
 // (src/cuint.cu:60-242) or CdetRK4k*/CdetRK5k* + CdetSnp1
 // (src/cuintRK4.cu:62-457, src/cuintRK5.cu:79-651).
-#include "internal.h"
+#include "gather.cuh"
 
 namespace asd {
 namespace {
-
-template <typename R>
-struct Vec3 { R* p[3]; };
-template <typename R>
-struct CVec3 { const R* p[3]; };
 
 struct LrArgs {
     const float* hr;            // padded real field [3][P] to gather (nullptr: none)
@@ -44,82 +40,12 @@ struct StageArgs {
     LrArgs lr;
 };
 
-template <typename T>
-__device__ __forceinline__ T ldcs(const T* p) { return __ldcs(p); }
-
-// Exchange field from the SELL-32 layout.
-template <typename R, bool FULL>
-__device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t n, uint32_t i, const CVec3<R>& s, R h[3]) {
-    const uint32_t sl = i >> 5, lane = i & 31u;
-    const uint32_t p0 = __ldg(m.slice_ptr + sl), p1 = __ldg(m.slice_ptr + sl + 1);
-    if constexpr (sizeof(R) == 4) {
-#pragma unroll 2
-        for (uint32_t e = p0 + lane; e < p1; e += 32) {
-            const float4 a = ldcs(m.a + e);
-            const int j = __float_as_int(a.x);
-            const float x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
-            if (!FULL) {
-                h[0] = fmaf(a.y, x, h[0]);
-                h[1] = fmaf(a.z, y, h[1]);
-                h[2] = fmaf(a.w, z, h[2]);
-            } else {
-                const float4 b = ldcs(m.b + e);
-                const float2 c = ldcs(m.c + e);
-                h[0] = fmaf(a.y, x, fmaf(a.z, y, fmaf(a.w, z, h[0])));
-                h[1] = fmaf(b.x, x, fmaf(b.y, y, fmaf(b.z, z, h[1])));
-                h[2] = fmaf(b.w, x, fmaf(c.x, y, fmaf(c.y, z, h[2])));
-            }
-        }
-    } else {
-        const uint32_t E = m.entries;
-        for (uint32_t e = p0 + lane; e < p1; e += 32) {
-            const int j = ldcs(m.col + e);
-            const double x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
-            if (!FULL) {
-                h[0] += ldcs(m.val + e) * x;
-                h[1] += ldcs(m.val + E + e) * y;
-                h[2] += ldcs(m.val + 2 * (size_t)E + e) * z;
-            } else {
-                const double* v = m.val;
-                h[0] += ldcs(v + e) * x + ldcs(v + E + e) * y + ldcs(v + 2 * (size_t)E + e) * z;
-                h[1] += ldcs(v + 3 * (size_t)E + e) * x + ldcs(v + 4 * (size_t)E + e) * y + ldcs(v + 5 * (size_t)E + e) * z;
-                h[2] += ldcs(v + 6 * (size_t)E + e) * x + ldcs(v + 7 * (size_t)E + e) * y + ldcs(v + 8 * (size_t)E + e) * z;
-            }
-        }
-    }
-    (void)n;
-}
-
-// Exchange field from the row-aligned DIA layout.
-template <typename R, bool FULL>
-__device__ __forceinline__ void gather_dia(const DiaDev& m, uint32_t n, uint32_t i, const CVec3<R>& s, R h[3]) {
-    const size_t ND = (size_t)m.ndiag * n;
-    const R* v;
-    if constexpr (sizeof(R) == 4) v = m.valf; else v = m.vald;
-    for (uint32_t d = 0; d < m.ndiag; d++) {
-        const int64_t col = (int64_t)i + __ldg(m.off + d);
-        if (col < 0 || col >= (int64_t)n) continue;
-        const size_t a = (size_t)d * n + i;
-        const R x = __ldg(s.p[0] + col), y = __ldg(s.p[1] + col), z = __ldg(s.p[2] + col);
-        if (!FULL) {
-            h[0] += ldcs(v + a) * x;
-            h[1] += ldcs(v + ND + a) * y;
-            h[2] += ldcs(v + 2 * ND + a) * z;
-        } else {
-            h[0] += ldcs(v + a) * x + ldcs(v + ND + a) * y + ldcs(v + 2 * ND + a) * z;
-            h[1] += ldcs(v + 3 * ND + a) * x + ldcs(v + 4 * ND + a) * y + ldcs(v + 5 * ND + a) * z;
-            h[2] += ldcs(v + 6 * ND + a) * x + ldcs(v + 7 * ND + a) * y + ldcs(v + 8 * ND + a) * z;
-        }
-    }
-}
-
 template <typename R>
 __device__ __forceinline__ void anis_field(const StepConst& c, const MatConst& mc, const R s[3], R h[3]) {
     const R d0 = (R)mc.k1udir[0], d1 = (R)mc.k1udir[1], d2 = (R)mc.k1udir[2];
     const R k1 = (R)mc.k1u * (s[0] * d0 + s[1] * d1 + s[2] * d2);
     h[0] += k1 * d0; h[1] += k1 * d1; h[2] += k1 * d2;
     if (c.k2perp_f != 0.0) {
-        const R* dd = nullptr; (void)dd;
         const R a0 = (R)c.k2perpdir[0], a1 = (R)c.k2perpdir[1], a2 = (R)c.k2perpdir[2];
         const R t = (R)c.k2perp_f * (s[0] * a0 + s[1] * a1 + s[2] * a2);
         h[0] += t * a0; h[1] += t * a1; h[2] += t * a2;
@@ -164,15 +90,28 @@ __constant__ double FRK5B[5][5] = {
 __constant__ double FRK5C[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
 __constant__ double FRK4C[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
 
+// FP32 kernels are capped at 51 registers (5 blocks of 256 per SM, no spills);
+// the FP64 kernels keep the default cap.
+template <typename R>
+struct MinBlocks { static constexpr int value = sizeof(R) == 4 ? 5 : 1; };
+
 template <typename R, int EX, bool FULL, bool COMP>
-__global__ void __launch_bounds__(256) stage_kernel(const StepConst c, const SellDev sell, const DiaDev dia,
-                                                     const StageArgs<R> a) {
+__global__ void __launch_bounds__(256, MinBlocks<R>::value)
+    stage_kernel(const StepConst c, const SellDev sell, const DiaDev dia, const StageArgs<R> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* tab = reinterpret_cast<R*>(smem_raw);
+    if constexpr (EX == ASD_EXCH_CSR) {
+        if (sell.typed) load_table<R>(table_of<R>(sell), (FULL ? 9u : 3u) * sell.ntypes, tab);
+    }
+    if constexpr (EX == ASD_EXCH_DIA) {
+        if (dia.dtype) load_table<R>(table_of<R>(dia), (FULL ? 9u : 3u) * dia.ntypes, tab);
+    }
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
     const uint64_t t = *c.step_base + a.rel;
     R h[3] = {R(0), R(0), R(0)};
-    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, c.n, i, a.src, h);
-    if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, a.src, h);
+    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, a.src, tab, h);
+    if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, a.src, tab, h);
     uint32_t midx = 0;
     if (a.lr.hr || a.lr.mr) midx = __ldg(a.lr.idx + i);
     if (a.lr.hr) {
@@ -186,10 +125,18 @@ __global__ void __launch_bounds__(256) stage_kernel(const StepConst c, const Sel
     const double sqrtT = __ldg(c.rep_sqrtT + r);
     R lrn[3] = {R(0), R(0), R(0)};
     if (sqrtT > 0.0) {
-        double xi[3];
-        thermal_normals(c.seed, __ldg(c.rep_stream + r), i - __ldg(c.rep_off + r), t, xi);
-        const double tp = sqrtT * mc.sigma;
-        lrn[0] = (R)(xi[0] * tp); lrn[1] = (R)(xi[1] * tp); lrn[2] = (R)(xi[2] * tp);
+        const uint32_t stream = __ldg(c.rep_stream + r), local = i - __ldg(c.rep_off + r);
+        if constexpr (sizeof(R) == 4) {
+            float xi[3];
+            thermal_normals_f(c.seed, stream, local, t, xi);
+            const float tp = (float)(sqrtT * mc.sigma);
+            lrn[0] = xi[0] * tp; lrn[1] = xi[1] * tp; lrn[2] = xi[2] * tp;
+        } else {
+            double xi[3];
+            thermal_normals(c.seed, stream, local, t, xi);
+            const double tp = sqrtT * mc.sigma;
+            lrn[0] = xi[0] * tp; lrn[1] = xi[1] * tp; lrn[2] = xi[2] * tp;
+        }
     }
     const double* dyn = c.dyn;
     if (a.stag.p[0]) {
@@ -270,14 +217,14 @@ template <typename R>
 CVec3<R> c3(R* const p[3]) { return CVec3<R>{{p[0], p[1], p[2]}}; }
 
 // Bytes one stage launch must move (algorithmic: each array element once,
-// gathered neighbour spins counted once, the matrix at its nnz).
+// gathered neighbour spins counted once, the matrix at its nnz in the layout used).
 template <typename R>
 double stage_bytes(const asd_handle* h, const StageArgs<R>& a, bool comp) {
     const double vb = sizeof(R), n = h->n;
     const double c = h->full ? 9.0 : 3.0;
     double m = 0.0;
-    if (h->exch == ASD_EXCH_CSR) m = 4.0 + h->nnz_per_row * (4.0 + vb * c);
-    else if (h->exch == ASD_EXCH_DIA) m = h->nnz_per_row * vb * c;
+    if (h->exch == ASD_EXCH_CSR) m = 4.0 + h->nnz_per_row * (h->sell.typed ? 4.0 : 4.0 + vb * c);
+    else if (h->exch == ASD_EXCH_DIA) m = h->nnz_per_row * (h->dia.dtype ? 1.0 : vb * c);
     double st = 3 * vb;                                  // src spin (gathered once)
     const int kind = a.kind;
     const bool final_spin = kind == 2 || (kind >= 10 && kind - 10 == a.nst - 1);
@@ -302,8 +249,11 @@ template <typename R, int EX, bool FULL, bool COMP>
 cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
     const int B = hd->block;
     const unsigned grid = (hd->n + B - 1) / B;
+    size_t smem = 0;
+    if (EX == ASD_EXCH_CSR && hd->sell.typed) smem = sizeof(R) * (FULL ? 9 : 3) * hd->sell.ntypes;
+    if (EX == ASD_EXCH_DIA && hd->dia.dtype) smem = sizeof(R) * (FULL ? 9 : 3) * hd->dia.ntypes;
     if (hd->timing) cudaEventRecord(hd->kev[0], hd->stream);
-    stage_kernel<R, EX, FULL, COMP><<<grid, B, 0, hd->stream>>>(hd->sc, hd->sell, hd->dia, a);
+    stage_kernel<R, EX, FULL, COMP><<<grid, B, smem, hd->stream>>>(hd->sc, hd->sell, hd->dia, a);
     hd->launches += 1;
     if (hd->timing) {
         cudaEventRecord(hd->kev[1], hd->stream);
@@ -315,9 +265,10 @@ cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
         kt.bytes = (kt.bytes * kt.count + b) / (double)(kt.count + 1);
         kt.total_ms += ms;
         kt.count += 1;
+        const bool typed = (EX == ASD_EXCH_CSR && hd->sell.typed) || (EX == ASD_EXCH_DIA && hd->dia.dtype);
         kt.name = std::string("stage_kernel<") + (sizeof(R) == 4 ? "float" : "double") + "," +
-                  (EX == ASD_EXCH_CSR ? "SELL32" : EX == ASD_EXCH_DIA ? "DIA" : "NONE") + (FULL ? ",full" : ",diag") +
-                  (COMP ? ",comp>" : ">");
+                  (EX == ASD_EXCH_CSR ? "SELL32" : EX == ASD_EXCH_DIA ? "DIA" : "NONE") + (typed ? "-typed" : "") +
+                  (FULL ? ",full" : ",diag") + (COMP ? ",comp>" : ">");
     }
     return cudaGetLastError();
 }
@@ -392,8 +343,7 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
         }
         a.lr = none;
         if (L.mode == ASD_LR_FFT) {
-            if (st > 0 && (e = launch_lr_eval_f32(h)) != cudaSuccess) return e;
-            if (st == 0 && (e = launch_lr_eval_f32(h)) != cudaSuccess) return e;
+            if ((e = launch_lr_eval_f32(h)) != cudaSuccess) return e;   // field of this stage's spins
             a.lr.hr = L.r + 3 * L.P; a.lr.mr = L.r;
         } else if (L.mode == ASD_LR_DIPOLE) {
             a.lr.hr = L.r + 3 * L.P;

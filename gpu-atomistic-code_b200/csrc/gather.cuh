@@ -1,0 +1,145 @@
+// Exchange-field gathers shared by the stage kernels and the field read-back.
+//
+// Two device layouts per storage scheme:
+//  * streamed values: each matrix entry carries its tensor (SELL-32 float4/float2 packing or
+//    component-major doubles; DIA component-major values);
+//  * typed: each entry carries a small tensor id into a table of the distinct tensors of the
+//    matrix (the reference builds every value from a per-(sublattice pair, shell) tensor,
+//    src/exch_unitcell.cpp:399, so a lattice has few); SELL entries pack (column, id) into
+//    one 32-bit word, DIA stores one id byte per (diagonal, row); id 0 is the zero tensor.
+//    The table is staged in shared memory, component-major [c][ntypes].
+#pragma once
+#include "internal.h"
+
+namespace asd {
+
+template <typename R>
+struct Vec3 { R* p[3]; };
+template <typename R>
+struct CVec3 { const R* p[3]; };
+
+template <typename T>
+__device__ __forceinline__ T ldcs(const T* p) { return __ldcs(p); }
+
+// Copy the tensor table (ncomp x ntypes) into shared memory; all threads of the block take part.
+template <typename R>
+__device__ __forceinline__ void load_table(const R* __restrict__ tab, uint32_t count, R* smem) {
+    for (uint32_t q = threadIdx.x; q < count; q += blockDim.x) smem[q] = tab[q];
+    __syncthreads();
+}
+
+template <typename R>
+__device__ __forceinline__ const R* table_of(const SellDev& m) {
+    if constexpr (sizeof(R) == 4) return m.tab_f; else return m.tab_d;
+}
+template <typename R>
+__device__ __forceinline__ const R* table_of(const DiaDev& m) {
+    if constexpr (sizeof(R) == 4) return m.tab_f; else return m.tab_d;
+}
+
+// h += sum over the row's entries of J_e S_col(e), SELL-32 layout (one warp per slice).
+template <typename R, bool FULL>
+__device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const CVec3<R>& s, const R* tab, R h[3]) {
+    const uint32_t sl = i >> 5, lane = i & 31u;
+    const uint32_t p0 = __ldg(m.slice_ptr + sl), p1 = __ldg(m.slice_ptr + sl + 1);
+    if (m.typed) {
+        const uint32_t nt = m.ntypes, mask = (1u << m.colbits) - 1u, cb = m.colbits;
+#pragma unroll 4
+        for (uint32_t e = p0 + lane; e < p1; e += 32) {
+            const uint32_t w = ldcs(m.typed + e);
+            const uint32_t j = w & mask, t = w >> cb;
+            const R x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
+            if (!FULL) {
+                h[0] += tab[t] * x;
+                h[1] += tab[nt + t] * y;
+                h[2] += tab[2 * nt + t] * z;
+            } else {
+                h[0] += tab[t] * x + tab[nt + t] * y + tab[2 * nt + t] * z;
+                h[1] += tab[3 * nt + t] * x + tab[4 * nt + t] * y + tab[5 * nt + t] * z;
+                h[2] += tab[6 * nt + t] * x + tab[7 * nt + t] * y + tab[8 * nt + t] * z;
+            }
+        }
+        return;
+    }
+    if constexpr (sizeof(R) == 4) {
+#pragma unroll 2
+        for (uint32_t e = p0 + lane; e < p1; e += 32) {
+            const float4 a = ldcs(m.a + e);
+            const int j = __float_as_int(a.x);
+            const float x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
+            if (!FULL) {
+                h[0] = fmaf(a.y, x, h[0]);
+                h[1] = fmaf(a.z, y, h[1]);
+                h[2] = fmaf(a.w, z, h[2]);
+            } else {
+                const float4 b = ldcs(m.b + e);
+                const float2 c = ldcs(m.c + e);
+                h[0] = fmaf(a.y, x, fmaf(a.z, y, fmaf(a.w, z, h[0])));
+                h[1] = fmaf(b.x, x, fmaf(b.y, y, fmaf(b.z, z, h[1])));
+                h[2] = fmaf(b.w, x, fmaf(c.x, y, fmaf(c.y, z, h[2])));
+            }
+        }
+    } else {
+        const uint32_t E = m.entries;
+        for (uint32_t e = p0 + lane; e < p1; e += 32) {
+            const int j = ldcs(m.col + e);
+            const double x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
+            const double* v = m.val;
+            if (!FULL) {
+                h[0] += ldcs(v + e) * x;
+                h[1] += ldcs(v + E + e) * y;
+                h[2] += ldcs(v + 2 * (size_t)E + e) * z;
+            } else {
+                h[0] += ldcs(v + e) * x + ldcs(v + E + e) * y + ldcs(v + 2 * (size_t)E + e) * z;
+                h[1] += ldcs(v + 3 * (size_t)E + e) * x + ldcs(v + 4 * (size_t)E + e) * y + ldcs(v + 5 * (size_t)E + e) * z;
+                h[2] += ldcs(v + 6 * (size_t)E + e) * x + ldcs(v + 7 * (size_t)E + e) * y + ldcs(v + 8 * (size_t)E + e) * z;
+            }
+        }
+    }
+}
+
+// h += sum over diagonals d with 0 <= i+off[d] < n of J_{d,i} S_{i+off[d]}, row-aligned DIA.
+template <typename R, bool FULL>
+__device__ __forceinline__ void gather_dia(const DiaDev& m, uint32_t n, uint32_t i, const CVec3<R>& s, const R* tab,
+                                           R h[3]) {
+    if (m.dtype) {
+        const uint32_t nt = m.ntypes;
+        for (uint32_t d = 0; d < m.ndiag; d++) {
+            const int64_t col = (int64_t)i + __ldg(m.off + d);
+            if (col < 0 || col >= (int64_t)n) continue;
+            const uint32_t t = ldcs(m.dtype + (size_t)d * n + i);
+            if (t == 0) continue;
+            const R x = __ldg(s.p[0] + col), y = __ldg(s.p[1] + col), z = __ldg(s.p[2] + col);
+            if (!FULL) {
+                h[0] += tab[t] * x;
+                h[1] += tab[nt + t] * y;
+                h[2] += tab[2 * nt + t] * z;
+            } else {
+                h[0] += tab[t] * x + tab[nt + t] * y + tab[2 * nt + t] * z;
+                h[1] += tab[3 * nt + t] * x + tab[4 * nt + t] * y + tab[5 * nt + t] * z;
+                h[2] += tab[6 * nt + t] * x + tab[7 * nt + t] * y + tab[8 * nt + t] * z;
+            }
+        }
+        return;
+    }
+    const size_t ND = (size_t)m.ndiag * n;
+    const R* v;
+    if constexpr (sizeof(R) == 4) v = m.valf; else v = m.vald;
+    for (uint32_t d = 0; d < m.ndiag; d++) {
+        const int64_t col = (int64_t)i + __ldg(m.off + d);
+        if (col < 0 || col >= (int64_t)n) continue;
+        const size_t a = (size_t)d * n + i;
+        const R x = __ldg(s.p[0] + col), y = __ldg(s.p[1] + col), z = __ldg(s.p[2] + col);
+        if (!FULL) {
+            h[0] += ldcs(v + a) * x;
+            h[1] += ldcs(v + ND + a) * y;
+            h[2] += ldcs(v + 2 * ND + a) * z;
+        } else {
+            h[0] += ldcs(v + a) * x + ldcs(v + ND + a) * y + ldcs(v + 2 * ND + a) * z;
+            h[1] += ldcs(v + 3 * ND + a) * x + ldcs(v + 4 * ND + a) * y + ldcs(v + 5 * ND + a) * z;
+            h[2] += ldcs(v + 6 * ND + a) * x + ldcs(v + 7 * ND + a) * y + ldcs(v + 8 * ND + a) * z;
+        }
+    }
+}
+
+}  // namespace asd

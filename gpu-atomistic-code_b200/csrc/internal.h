@@ -24,14 +24,24 @@ struct SellDev {
     float2* c = nullptr;
     int32_t* col = nullptr;
     double* val = nullptr;
+    // typed layout: entry word = col | id << colbits; table [ncomp][ntypes]
+    uint32_t* typed = nullptr;
+    uint32_t colbits = 0, ntypes = 0;
+    float* tab_f = nullptr;
+    double* tab_d = nullptr;
 };
 
-// Row-aligned DIA, values component-major val[c][d*N+row], c = 3 (diag) or 9.
+// Row-aligned DIA, values component-major val[c][d*N+row], c = 3 (diag) or 9;
+// typed layout: one id byte per (diagonal, row), table [ncomp][ntypes].
 struct DiaDev {
     uint32_t ndiag = 0;
     int32_t* off = nullptr;
     float* valf = nullptr;
     double* vald = nullptr;
+    uint8_t* dtype = nullptr;
+    uint32_t ntypes = 0;
+    float* tab_f = nullptr;
+    double* tab_d = nullptr;
 };
 
 // Reference-structured CSR / DIA for the FP64 plain form (separate component arrays).
@@ -137,6 +147,8 @@ cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v);
 cudaError_t launch_magnetisation(asd_handle* h);
 cudaError_t launch_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, double* d_out,
                                    cudaStream_t st);
+cudaError_t launch_thermal_normals_f(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, float* d_out,
+                                     cudaStream_t st);
 cudaError_t launch_convert_spins_in(asd_handle* h, const double* d_aos);
 cudaError_t launch_convert_out(asd_handle* h, int what, double* d_aos);
 cudaError_t build_nk_f32(asd_handle* h, const double* d_nr);

@@ -395,4 +395,18 @@ cudaError_t launch_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step
     return cudaGetLastError();
 }
 
+__global__ void normals_f_k(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float xi[3];
+    thermal_normals_f(seed, stream, i, step, xi);
+    out[3 * i] = xi[0]; out[3 * i + 1] = xi[1]; out[3 * i + 2] = xi[2];
+}
+
+cudaError_t launch_thermal_normals_f(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, float* d_out,
+                                     cudaStream_t st) {
+    normals_f_k<<<nb(n, 256), 256, 0, st>>>(seed, stream, step, n, d_out);
+    return cudaGetLastError();
+}
+
 }  // namespace asd

@@ -1,6 +1,6 @@
 // Magnetisation reduction, layout conversions at the host boundary, and the
 // field-only evaluation behind asd_get_field.
-#include "internal.h"
+#include "gather.cuh"
 #include <algorithm>
 
 namespace asd {
@@ -110,51 +110,21 @@ template <typename R, int EX, bool FULL>
 __global__ void field_k(StepConst c, SellDev sell, DiaDev dia, const R* __restrict__ sx, const R* __restrict__ sy,
                         const R* __restrict__ sz, const float* __restrict__ hr, float inv_p, size_t P,
                         const uint32_t* __restrict__ idx, double* __restrict__ out) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
-    double h[3] = {0.0, 0.0, 0.0};
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    R* tab = reinterpret_cast<R*>(smem_raw);
     if constexpr (EX == ASD_EXCH_CSR) {
-        const uint32_t sl = i >> 5, lane = i & 31u;
-        for (uint32_t e = sell.slice_ptr[sl] + lane; e < sell.slice_ptr[sl + 1]; e += 32) {
-            int j;
-            double m[9];
-            if constexpr (sizeof(R) == 4) {
-                const float4 a = sell.a[e];
-                j = __float_as_int(a.x);
-                if (FULL) {
-                    const float4 b = sell.b[e]; const float2 cc = sell.c[e];
-                    const double t[9] = {a.y, a.z, a.w, b.x, b.y, b.z, b.w, cc.x, cc.y};
-                    for (int q = 0; q < 9; q++) m[q] = t[q];
-                } else {
-                    for (int q = 0; q < 9; q++) m[q] = 0.0;
-                    m[0] = a.y; m[4] = a.z; m[8] = a.w;
-                }
-            } else {
-                j = sell.col[e];
-                const size_t E = sell.entries;
-                if (FULL) for (int q = 0; q < 9; q++) m[q] = sell.val[q * E + e];
-                else { for (int q = 0; q < 9; q++) m[q] = 0.0; m[0] = sell.val[e]; m[4] = sell.val[E + e]; m[8] = sell.val[2 * E + e]; }
-            }
-            const double s3[3] = {(double)sx[j], (double)sy[j], (double)sz[j]};
-            for (int a = 0; a < 3; a++) h[a] += m[3 * a] * s3[0] + m[3 * a + 1] * s3[1] + m[3 * a + 2] * s3[2];
-        }
+        if (sell.typed) load_table<R>(table_of<R>(sell), (FULL ? 9u : 3u) * sell.ntypes, tab);
     }
     if constexpr (EX == ASD_EXCH_DIA) {
-        const size_t ND = (size_t)dia.ndiag * c.n;
-        for (uint32_t d = 0; d < dia.ndiag; d++) {
-            const int64_t col = (int64_t)i + dia.off[d];
-            if (col < 0 || col >= (int64_t)c.n) continue;
-            const size_t a0 = (size_t)d * c.n + i;
-            const double s3[3] = {(double)sx[col], (double)sy[col], (double)sz[col]};
-            const int nc = FULL ? 9 : 3;
-            for (int q = 0; q < nc; q++) {
-                double v;
-                if constexpr (sizeof(R) == 4) v = dia.valf[q * ND + a0]; else v = dia.vald[q * ND + a0];
-                if (FULL) h[q / 3] += v * s3[q % 3];
-                else h[q] += v * s3[q];
-            }
-        }
+        if (dia.dtype) load_table<R>(table_of<R>(dia), (FULL ? 9u : 3u) * dia.ntypes, tab);
     }
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    R hr3[3] = {R(0), R(0), R(0)};
+    const CVec3<R> src{{sx, sy, sz}};
+    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, src, tab, hr3);
+    if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, src, tab, hr3);
+    double h[3] = {(double)hr3[0], (double)hr3[1], (double)hr3[2]};
     if (hr) {
         const uint32_t m = idx[i];
         for (int a = 0; a < 3; a++) h[a] += (double)(hr[a * P + m] * inv_p);
@@ -183,12 +153,15 @@ cudaError_t field_t(asd_handle* h, double* out) {
     }
     const float inv_p = h->lr.P ? 1.0f / (float)h->lr.P : 0.f;
     const unsigned g = nb(h->n, 256);
+    const size_t cs = sizeof(R) * (h->full ? 9 : 3);
     if (h->exch == ASD_EXCH_CSR) {
-        if (h->full) field_k<R, ASD_EXCH_CSR, true><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
-        else field_k<R, ASD_EXCH_CSR, false><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        const size_t sm = h->sell.typed ? cs * h->sell.ntypes : 0;
+        if (h->full) field_k<R, ASD_EXCH_CSR, true><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        else field_k<R, ASD_EXCH_CSR, false><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
     } else if (h->exch == ASD_EXCH_DIA) {
-        if (h->full) field_k<R, ASD_EXCH_DIA, true><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
-        else field_k<R, ASD_EXCH_DIA, false><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        const size_t sm = h->dia.dtype ? cs * h->dia.ntypes : 0;
+        if (h->full) field_k<R, ASD_EXCH_DIA, true><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        else field_k<R, ASD_EXCH_DIA, false><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
     } else {
         field_k<R, ASD_EXCH_NONE, false><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
     }

@@ -66,6 +66,8 @@ extern "C" {
 #define ASD_FLAG_GPU_HDEMAG_FP32     (1u << 7)  /* CHDemag stored as float (src/cuda_glob.cu) */
 #define ASD_FLAG_COMPENSATED         (1u << 16) /* FP32 form: spins kept as float hi+lo pairs */
 #define ASD_FLAG_AUTOTUNE            (1u << 17) /* FP32 form: time block shapes at create */
+#define ASD_FLAG_STREAMED_EXCHANGE   (1u << 18) /* fused forms: keep every tensor in the matrix stream
+                                                   instead of the typed (column, tensor-id) layout */
 
 #define ASD_ALL_REPLICAS 0xFFFFFFFFu
 
@@ -195,6 +197,9 @@ int asd_kernel_stats(const asd_handle* h, char* name, size_t name_len, double* a
 /* The thermal normals the step uses for (seed, stream, step): 3 per spin for spins
  * [0, nspins), computed by the device generator (Philox4x32-10 + Box-Muller). */
 int asd_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t nspins, double* out);
+/* The FP32 form's normals for the same (seed, stream, step): the same Philox draw through
+ * the single-precision Box-Muller series. */
+int asd_thermal_normals_f32(uint64_t seed, uint32_t stream, uint64_t step, uint32_t nspins, float* out);
 
 /* --- set-up builders (host C++, FP64) ---------------------------------------- */
 /* Bond list -> CSR as exch::exchunitcell does (src/exch_unitcell.cpp:265-489): spins ordered

@@ -145,6 +145,74 @@ void orc_thermal_normals(uint64_t seed, uint32_t stream, uint32_t spin, uint64_t
     out[2] = r2 * c3;
 }
 
+/* Single-precision variant (the FP32 form's generator): 23-bit uniforms
+ * ((x>>9)+0.5)/2^23, ln to f^11, sin to psi^11, cos to psi^12, float fma. */
+static float logf_series(float x) {
+    int e;
+    float m = frexpf(x, &e);
+    if (m < 0x1.6a09e6p-1f) { m = m * 2.0f; e = e - 1; }
+    const float f = (m - 1.0f) / (m + 1.0f);
+    const float f2 = f * f;
+    float p = 0x1.745d18p-4f;
+    p = fmaf(p, f2, 0x1.c71c72p-4f);
+    p = fmaf(p, f2, 0x1.24924ap-3f);
+    p = fmaf(p, f2, 0x1.99999ap-3f);
+    p = fmaf(p, f2, 0x1.555556p-2f);
+    p = fmaf(p, f2, 1.0f);
+    const float lnm = 2.0f * (f * p);
+    return fmaf((float)e, 0x1.62e430p-1f, lnm);
+}
+
+static void sincosf_series(uint32_t x, float* sn, float* cs) {
+    const float v = ((float)(x >> 9) + 0.5f) * 0x1p-20f;
+    const float qd = floorf(v);
+    const int q = (int)qd;
+    const float r = v - qd;
+    const float psi = ((q & 1) ? (1.0f - r) : r) * 0x1.921fb6p-1f;
+    const float mp2 = -(psi * psi);
+    float sp = 0x1.ae6456p-26f;
+    sp = fmaf(sp, mp2, 0x1.71de3ap-19f);
+    sp = fmaf(sp, mp2, 0x1.a01a02p-13f);
+    sp = fmaf(sp, mp2, 0x1.111112p-7f);
+    sp = fmaf(sp, mp2, 0x1.555556p-3f);
+    sp = fmaf(sp, mp2, 1.0f);
+    const float s = psi * sp;
+    float cp = 0x1.1eed8ep-29f;
+    cp = fmaf(cp, mp2, 0x1.27e4fcp-22f);
+    cp = fmaf(cp, mp2, 0x1.a01a02p-16f);
+    cp = fmaf(cp, mp2, 0x1.6c16c2p-10f);
+    cp = fmaf(cp, mp2, 0x1.555556p-5f);
+    cp = fmaf(cp, mp2, 0x1.000000p-1f);
+    const float c = fmaf(cp, mp2, 1.0f);
+    switch (q) {
+    case 0: *sn = s;  *cs = c;  break;
+    case 1: *sn = c;  *cs = s;  break;
+    case 2: *sn = c;  *cs = -s; break;
+    case 3: *sn = s;  *cs = -c; break;
+    case 4: *sn = -s; *cs = -c; break;
+    case 5: *sn = -c; *cs = -s; break;
+    case 6: *sn = -c; *cs = s;  break;
+    default: *sn = -s; *cs = c; break;
+    }
+}
+
+void orc_thermal_normals_f(uint64_t seed, uint32_t stream, uint32_t spin, uint64_t step, float out[3]) {
+    uint32_t ctr[4] = {spin, (uint32_t)step, (uint32_t)(step >> 32), stream};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t x[4];
+    orc_philox4x32_10(ctr, key, x);
+    const float u0 = ((float)(x[0] >> 9) + 0.5f) * 0x1p-23f;
+    const float u2 = ((float)(x[2] >> 9) + 0.5f) * 0x1p-23f;
+    const float r0 = sqrtf(-2.0f * logf_series(u0));
+    const float r2 = sqrtf(-2.0f * logf_series(u2));
+    float s1, c1, s3, c3;
+    sincosf_series(x[1], &s1, &c1);
+    sincosf_series(x[3], &s3, &c3);
+    out[0] = r0 * c1;
+    out[1] = r0 * s1;
+    out[2] = r2 * c3;
+}
+
 /* MWC1616 and Marsaglia's polar method, restating src/random.cpp:17-64. */
 static uint32_t mwc_x = 1, mwc_y = 1;
 static int mwc_sw = 0;

@@ -95,6 +95,7 @@ int orc_magnetisation(const orc_ctx* c, uint32_t nsub, const uint32_t* sublattic
 /* Noise generators, exposed for known-answer tests. */
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void orc_thermal_normals(uint64_t seed, uint32_t stream, uint32_t spin, uint64_t step, double out[3]);
+void orc_thermal_normals_f(uint64_t seed, uint32_t stream, uint32_t spin, uint64_t step, float out[3]);
 double orc_log(double x);
 void orc_sincos_2pi(uint32_t x, double* s, double* co);
 void orc_mwc_seed(uint32_t a, uint32_t b);

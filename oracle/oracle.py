@@ -249,6 +249,18 @@ def philox(ctr, key):
     return o
 
 
+def thermal_normals_f(seed, stream, n, step):
+    """The FP32 form's normals (single-precision series on the same Philox draw)."""
+    L = olib()
+    L.orc_thermal_normals_f.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(C.c_float)]
+    out = np.zeros((n, 3), dtype=np.float32)
+    buf = (C.c_float * 3)()
+    for i in range(n):
+        L.orc_thermal_normals_f(seed, stream, i, step, buf)
+        out[i] = buf[:]
+    return out
+
+
 def thermal_normals(seed, stream, n, step):
     out = np.zeros((n, 3))
     L = olib()

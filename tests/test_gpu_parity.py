@@ -44,6 +44,15 @@ def test_thermal_normals_bit_exact(gpu):
         assert np.array_equal(g, o)
 
 
+def test_thermal_normals_f32_bit_exact(gpu):
+    for seed, stream, step in [(1, 0, 0), (987654321, 3, 2**40 + 1)]:
+        g = A.thermal_normals_f32(seed, stream, step, 2000)
+        o = O.thermal_normals_f(seed, stream, 2000, step)
+        assert np.array_equal(g, o)
+        d = O.thermal_normals(seed, stream, 2000, step)
+        assert np.quantile(np.abs(g - d), 0.999) < 1e-5   # same Philox draw, float series
+
+
 @pytest.mark.parametrize("T", [0.0, 300.0])
 def test_plain_heun_csr_bit_exact(gpu, T):
     s = LT.sc_ferromagnet(8, T=T)
@@ -80,33 +89,58 @@ def test_plain_rk_bit_exact(gpu, integ, flags):
     assert np.array_equal(g, o), maxdiff(g, o)
 
 
-def test_fused_fp64_close(gpu):
+LAYOUTS = [0, A.FLAG_STREAMED_EXCHANGE]   # typed (column, tensor id) and streamed tensors
+
+
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_fused_fp64_close(gpu, layout):
     s = LT.sc_ferromagnet(8, T=0.0)
-    g, o, _, _ = pair(s, 300, A.FP64_FUSED)
+    g, o, _, _ = pair(s, 300, A.FP64_FUSED, flags=layout)
     assert maxdiff(g, o) <= 1e-10
     s = LT.bct2_antiferromagnet(3, T=0.0)
-    g, o, _, _ = pair(s, 100, A.FP64_FUSED)
+    g, o, _, _ = pair(s, 100, A.FP64_FUSED, flags=layout)
+    assert maxdiff(g, o) <= 1e-10
+    s = LT.bct2_antiferromagnet(3, layout="dia", T=0.0)
+    g, o, _, _ = pair(s, 100, A.FP64_FUSED, flags=layout)
     assert maxdiff(g, o) <= 1e-10
 
 
-@pytest.mark.parametrize("flags", [0, A.FLAG_COMPENSATED])
+@pytest.mark.parametrize("flags", [0, A.FLAG_COMPENSATED, A.FLAG_COMPENSATED | A.FLAG_STREAMED_EXCHANGE])
 def test_fp32_sc_close(gpu, flags):
     s = LT.sc_ferromagnet(10, T=0.0)
     g, o, _, _ = pair(s, 1000, A.FP32, flags=flags)
     assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
 
 
-def test_fp32_bct_full_csr_and_dia_close(gpu):
-    for layout in ("csr", "dia"):
-        s = LT.bct2_antiferromagnet(4, layout=layout, T=0.0)
-        g, o, _, _ = pair(s, 300, A.FP32, flags=A.FLAG_COMPENSATED)
-        assert maxdiff(g, o) <= 1e-5, (layout, maxdiff(g, o))
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_fp32_bct_full_csr_and_dia_close(gpu, layout):
+    for kind in ("csr", "dia"):
+        s = LT.bct2_antiferromagnet(4, layout=kind, T=0.0)
+        g, o, _, _ = pair(s, 300, A.FP32, flags=A.FLAG_COMPENSATED | layout)
+        assert maxdiff(g, o) <= 1e-5, (kind, maxdiff(g, o))
+
+
+def test_fp32_many_distinct_tensors_fall_back_to_streamed(gpu):
+    s = LT.sc_ferromagnet(7, T=0.0)
+    rng = np.random.default_rng(8)
+    s.csr_val = s.csr_val * rng.uniform(0.5, 1.5, size=(len(s.adjncy), 1))   # > 256 distinct tensors
+    for prec, tol in ((A.FP32, 1e-5), (A.FP64_FUSED, 1e-10)):
+        g, o, _, _ = pair(s, 200, prec, flags=A.FLAG_COMPENSATED)
+        assert maxdiff(g, o) <= tol
 
 
 @pytest.mark.parametrize("integ", [A.RK4, A.RK5])
-def test_fp32_rk_close(gpu, integ):
+@pytest.mark.parametrize("layout", LAYOUTS)
+def test_fp32_rk_close(gpu, integ, layout):
     s = LT.sc_ferromagnet(8, J2=-2e-22, exch="dia", pbc=(1, 1, 0), T=0.0)
-    g, o, _, _ = pair(s, 200, A.FP32, integrator=integ, dt=5e-16, flags=A.FLAG_COMPENSATED)
+    g, o, _, _ = pair(s, 200, A.FP32, integrator=integ, dt=5e-16, flags=A.FLAG_COMPENSATED | layout)
+    assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
+
+
+def test_fp32_finite_temperature_close(gpu):
+    """FP32 noise is the float series on the same Philox draw: the trajectory stays within 1e-5."""
+    s = LT.sc_ferromagnet(8, T=300.0)
+    g, o, _, _ = pair(s, 100, A.FP32, flags=A.FLAG_COMPENSATED)
     assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
 
 
@@ -134,8 +168,9 @@ def test_field_readback_matches_oracle(gpu):
     o = O.Oracle(s)
     o.set_spins(S0)
     ho = o.field()
-    for prec, tol in [(A.FP64_PLAIN, 0.0), (A.FP64_FUSED, 1e-12), (A.FP32, 1e-5)]:
-        with A.Handle(A.RunParams(precision=prec), s) as h:
+    for prec, tol, fl in [(A.FP64_PLAIN, 0.0, 0), (A.FP64_FUSED, 1e-12, 0), (A.FP32, 1e-5, 0),
+                          (A.FP32, 1e-5, A.FLAG_STREAMED_EXCHANGE)]:
+        with A.Handle(A.RunParams(precision=prec, flags=fl), s) as h:
             h.set_spins(S0)
             hg = h.get_field()
         assert maxdiff(hg, ho) <= tol * np.abs(ho).max(), (prec, maxdiff(hg, ho))

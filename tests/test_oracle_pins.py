@@ -120,3 +120,13 @@ def test_magnetisation_oracle():
     o.set_spins(S)
     m = o.magnetisation()
     assert np.allclose(m[0, 0], S.mean(axis=0), atol=1e-15)
+
+
+def test_float_normals_statistics_and_closeness():
+    xf = O.thermal_normals_f(11, 3, 20000, 7)
+    xd = O.thermal_normals(11, 3, 20000, 7)
+    # 23-bit uniforms: away from the extreme tail (u < 2^-14) the float and double draws agree
+    d = np.abs(xf - xd)
+    assert np.quantile(d, 0.999) < 1e-5 and d.max() < 0.1
+    v = xf.reshape(-1).astype(np.float64)
+    assert abs(v.mean()) < 0.02 and abs(v.var() - 1.0) < 0.03
