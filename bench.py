@@ -215,10 +215,11 @@ def run_ours(args):
         except OSError:
             pass
 
-    systems, kw, cfg = make_workload(args.workload)
+    streamed = args.workload.endswith("_streamed")      # keep every tensor in the matrix stream
+    systems, kw, cfg = make_workload(args.workload[: -len("_streamed")] if streamed else args.workload)
     n = sum(s.nspins for s in systems)
     S0 = LT.random_spins(n, 0)
-    flags = A.FLAG_COMPENSATED
+    flags = A.FLAG_COMPENSATED | (A.FLAG_STREAMED_EXCHANGE if streamed else 0)
     p32 = A.RunParams(precision=A.FP32, seed=1 + rank, flags=flags, **kw)
     h = A.Handle(p32, systems)
     h.set_spins(S0)
