@@ -60,6 +60,7 @@ int fail(asd_handle* h, const Fail& f) {
 void free_all(asd_handle* h) {
     auto F = [](void* p) { if (p) cudaFree(p); };
     F(h->d_rep_off); F(h->d_rep_stream); F(h->d_atom); F(h->d_rep_sqrtT); F(h->d_dyn); F(h->d_step);
+    F(h->d_rep_sqrtT_f); F(h->d_dynf);
     for (int c = 0; c < 3; c++) {
         F(h->sf[c]); F(h->sl[c]); F(h->esf[c]); F(h->fnf[c]); F(h->detf[c]); F(h->stagf[c]);
         F(h->sd[c]); F(h->esd[c]); F(h->fnd[c]); F(h->detd[c]); F(h->stagd[c]);
@@ -119,10 +120,11 @@ struct TensorTable {
         return b;
     }
     template <typename T>
-    std::vector<T> table() const {   // component-major [nc][ntypes]
-        std::vector<T> t((size_t)nc * list.size());
+    std::vector<T> table() const {   // type-major [ntypes][stride], stride 4 (xx,yy,zz,0) or 12 (9 + 3 zeros)
+        const size_t stride = nc == 9 ? 12 : 4;
+        std::vector<T> t(stride * list.size(), (T)0);
         for (size_t k = 0; k < list.size(); k++)
-            for (int q = 0; q < nc; q++) t[(size_t)q * list.size() + k] = (T)list[k][q];
+            for (int q = 0; q < nc; q++) t[k * stride + q] = (T)list[k][q];
         return t;
     }
 };
@@ -301,7 +303,10 @@ void setup_lr(asd_handle* h, const asd_system& s, bool plain) {
     CK(e);
 }
 
-void set_dyn(asd_handle* h, int idx, double v) { CK(launch_set_scalar(h, h->d_dyn + idx, v)); }
+void set_dyn(asd_handle* h, int idx, double v) {
+    CK(launch_set_scalar(h, h->d_dyn + idx, v));
+    if (idx != DYN_DET_STEP) CK(launch_set_scalar_f(h, h->d_dynf + idx, (float)v));
+}
 
 void scatter_if_needed(asd_handle* h) {
     if (h->lr.mode == ASD_LR_NONE || h->p.precision == ASD_FP64_PLAIN || h->lr_scattered) return;
@@ -439,6 +444,9 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
             mc.k1u = 2.0 * m.k1u / (p.muB * m.mu);
             for (int a = 0; a < 3; a++) mc.k1udir[a] = m.k1u_dir[a];
             mc.sub = m.sublattice;
+            mc.llgpf_f = (float)mc.llgpf; mc.lambda_f = (float)mc.lambda; mc.sigma_f = (float)mc.sigma;
+            mc.k1u_f = (float)mc.k1u;
+            for (int a = 0; a < 3; a++) mc.k1udir_f[a] = (float)mc.k1udir[a];
             h->h_sub_of_mat.push_back(m.sublattice);
             h->nsub = std::max(h->nsub, m.sublattice + 1);
         }
@@ -450,6 +458,11 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         for (int a = 0; a < 3; a++) { sc.k2perpdir[a] = p.k2perpdir[a]; sc.k2pardir[a] = p.k2pardir[a]; }
         for (int a = 0; a < 9; a++) { sc.k4perpdirs[a] = p.k4perpdirs[a]; sc.k4pardirs[a] = p.k4pardirs[a]; }
         sc.seed = p.seed;
+        sc.rdt_f = (float)sc.rdt;
+        sc.k2perp_ff = (float)sc.k2perp_f; sc.k2par_ff = (float)sc.k2par_f;
+        sc.k4perp_ff = (float)sc.k4perp_f; sc.k4par_ff = (float)sc.k4par_f;
+        for (int a = 0; a < 3; a++) { sc.k2perpdir_f[a] = (float)sc.k2perpdir[a]; sc.k2pardir_f[a] = (float)sc.k2pardir[a]; }
+        for (int a = 0; a < 9; a++) { sc.k4perpdirs_f[a] = (float)sc.k4perpdirs[a]; sc.k4pardirs_f[a] = (float)sc.k4pardirs[a]; }
         // per-spin atom table (only when not i % nmat)
         bool need_atom = false;
         std::vector<uint32_t> atom(n);
@@ -469,6 +482,9 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         std::vector<uint32_t> strm(nsys);
         for (uint32_t r = 0; r < nsys; r++) { sq[r] = sqrt(h->h_rep_T[r]); strm[r] = sys[r].stream; }
         h->d_rep_sqrtT = dupload(sq.data(), nsys);
+        std::vector<float> sqf(sq.begin(), sq.end());
+        h->d_rep_sqrtT_f = dupload(sqf.data(), nsys);
+        sc.rep_sqrtT_f = h->d_rep_sqrtT_f;
         h->d_rep_stream = dupload(strm.data(), nsys);
         sc.rep_off = h->d_rep_off; sc.rep_sqrtT = h->d_rep_sqrtT; sc.rep_stream = h->d_rep_stream;
         std::vector<double> dyn(DYN_COUNT, 0.0);
@@ -476,6 +492,9 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         dyn[DYN_STAG_SCALE] = 1.0;
         dyn[DYN_DET_STEP] = -1.0;
         h->d_dyn = dupload(dyn.data(), dyn.size());
+        std::vector<float> dynf(dyn.begin(), dyn.end());
+        h->d_dynf = dupload(dynf.data(), dynf.size());
+        sc.dynf = h->d_dynf;
         h->d_step = dalloc<uint64_t>(1);
         sc.dyn = h->d_dyn; sc.step_base = h->d_step;
         // ---- exchange, concatenated over replicas
@@ -809,6 +828,7 @@ int asd_set_temperature(asd_handle* h, uint32_t replica, double T) {
             if (replica != ASD_ALL_REPLICAS && r != replica) continue;
             h->h_rep_T[r] = T;
             CK(launch_set_scalar(h, h->d_rep_sqrtT + r, sqrt(T)));
+            CK(launch_set_scalar_f(h, h->d_rep_sqrtT_f + r, (float)sqrt(T)));
         }
     } catch (const Fail& f) { return fail(h, f); }
     return ASD_OK;

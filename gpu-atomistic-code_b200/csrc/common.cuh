@@ -20,6 +20,8 @@ struct MatConst {
     double k1udir[3];
     uint32_t sub;
     uint32_t pad;
+    // single-precision copies for the FP32 form (no per-thread conversions)
+    float llgpf_f, lambda_f, sigma_f, k1u_f, k1udir_f[3], pad_f;
 };
 
 // Kernel parameter block shared by all stage kernels (passed by value).
@@ -39,6 +41,12 @@ struct StepConst {
     const uint32_t* rep_stream;
     const double* dyn;         // mutable scalars, see DYN_*
     const uint64_t* step_base; // device step counter
+    // single-precision copies for the FP32 form
+    float rdt_f;
+    float k2perp_ff, k2par_ff, k4perp_ff, k4par_ff;
+    float k2perpdir_f[3], k2pardir_f[3], k4perpdirs_f[9], k4pardirs_f[9];
+    const float* rep_sqrtT_f;  // nrep
+    const float* dynf;         // float copy of the mutable scalars
 };
 
 // Layout of the mutable scalar block (device memory, updated between launches).
@@ -159,10 +167,12 @@ __device__ __forceinline__ void thermal_normals(uint64_t seed, uint32_t stream, 
     out[2] = __dmul_rn(r2, c3);
 }
 
-// Single-precision variant for the FP32 form: the same Philox draw, 23-bit uniforms
-// u = ((x >> 9) + 0.5) 2^-23 (exact in float), and shorter series evaluated with
-// correctly rounded float operations (ln: terms to f^11; sin to psi^11, cos to psi^12),
-// accurate to a few float ulps and reproducible on any IEEE-754 float implementation.
+// Single-precision variant for the FP32 form: the same Philox draw, uniforms
+// u = (float(x) + 0.5) 2^-32 (float(x) rounded to nearest, so small u keep their
+// relative precision and the tail follows the double draw), the sin/cos octant taken
+// exactly from the top 3 bits of x, and shorter series evaluated with correctly rounded
+// float operations (ln: terms to f^11; sin to psi^11, cos to psi^12), accurate to a few
+// float ulps and reproducible on any IEEE-754 float implementation.
 __device__ __forceinline__ float series_logf(float x) {
     int e;
     float m = frexpf(x, &e);
@@ -180,10 +190,8 @@ __device__ __forceinline__ float series_logf(float x) {
 }
 
 __device__ __forceinline__ void series_sincos_2pi_f(uint32_t x, float& sn, float& cs) {
-    const float v = __fmul_rn(__fadd_rn((float)(x >> 9), 0.5f), 0x1p-20f);   // 8u, exact
-    const float qd = floorf(v);
-    const int q = (int)qd;
-    const float r = __fsub_rn(v, qd);
+    const int q = (int)(x >> 29);                                                          // octant
+    const float r = __fmul_rn(__fadd_rn(__uint2float_rn(x & 0x1FFFFFFFu), 0.5f), 0x1p-29f); // in (0, 1]
     const float psi = __fmul_rn((q & 1) ? __fsub_rn(1.0f, r) : r, 0x1.921fb6p-1f);
     const float mp2 = -__fmul_rn(psi, psi);
     float sp = 0x1.ae6456p-26f;               // 1/11!
@@ -216,8 +224,8 @@ __device__ __forceinline__ void thermal_normals_f(uint64_t seed, uint32_t stream
                                                   float out[3]) {
     uint32_t c[4] = {spin, (uint32_t)step, (uint32_t)(step >> 32), stream};
     philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
-    const float u0 = __fmul_rn(__fadd_rn((float)(c[0] >> 9), 0.5f), 0x1p-23f);
-    const float u2 = __fmul_rn(__fadd_rn((float)(c[2] >> 9), 0.5f), 0x1p-23f);
+    const float u0 = __fmul_rn(__fadd_rn(__uint2float_rn(c[0]), 0.5f), 0x1p-32f);   // in (0, 1]
+    const float u2 = __fmul_rn(__fadd_rn(__uint2float_rn(c[2]), 0.5f), 0x1p-32f);
     const float r0 = __fsqrt_rn(__fmul_rn(-2.0f, series_logf(u0)));
     const float r2 = __fsqrt_rn(__fmul_rn(-2.0f, series_logf(u2)));
     float s1, c1, s3, c3;

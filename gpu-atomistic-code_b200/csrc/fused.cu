@@ -40,29 +40,44 @@ struct StageArgs {
     LrArgs lr;
 };
 
+// Anisotropy field (src/cuint.cu:76-137): per-atom K1u plus global K2 / K4 terms, with the
+// constants taken in the kernel's own precision from the parameter block.
+template <typename R>
+struct AnisConst {
+    R k1u, d[3], k2perp, k2perpdir[3], k2par, k2pardir[3], k4perp, k4perpdirs[9], k4par, k4pardirs[9];
+};
+
 template <typename R>
 __device__ __forceinline__ void anis_field(const StepConst& c, const MatConst& mc, const R s[3], R h[3]) {
-    const R d0 = (R)mc.k1udir[0], d1 = (R)mc.k1udir[1], d2 = (R)mc.k1udir[2];
-    const R k1 = (R)mc.k1u * (s[0] * d0 + s[1] * d1 + s[2] * d2);
-    h[0] += k1 * d0; h[1] += k1 * d1; h[2] += k1 * d2;
-    if (c.k2perp_f != 0.0) {
-        const R a0 = (R)c.k2perpdir[0], a1 = (R)c.k2perpdir[1], a2 = (R)c.k2perpdir[2];
-        const R t = (R)c.k2perp_f * (s[0] * a0 + s[1] * a1 + s[2] * a2);
-        h[0] += t * a0; h[1] += t * a1; h[2] += t * a2;
+    const R *d, *k2pd, *k2ad, *k4pd, *k4ad;
+    R k1u, k2perp, k2par, k4perp, k4par;
+    if constexpr (sizeof(R) == 4) {
+        d = mc.k1udir_f; k1u = mc.k1u_f;
+        k2pd = c.k2perpdir_f; k2ad = c.k2pardir_f; k4pd = c.k4perpdirs_f; k4ad = c.k4pardirs_f;
+        k2perp = c.k2perp_ff; k2par = c.k2par_ff; k4perp = c.k4perp_ff; k4par = c.k4par_ff;
+    } else {
+        d = mc.k1udir; k1u = mc.k1u;
+        k2pd = c.k2perpdir; k2ad = c.k2pardir; k4pd = c.k4perpdirs; k4ad = c.k4pardirs;
+        k2perp = c.k2perp_f; k2par = c.k2par_f; k4perp = c.k4perp_f; k4par = c.k4par_f;
     }
-    if (c.k2par_f != 0.0) {
-        const R a0 = (R)c.k2pardir[0], a1 = (R)c.k2pardir[1], a2 = (R)c.k2pardir[2];
-        const R t = (R)c.k2par_f * (s[0] * a0 + s[1] * a1 + s[2] * a2);
-        h[0] += t * a0; h[1] += t * a1; h[2] += t * a2;
+    const R k1 = k1u * (s[0] * d[0] + s[1] * d[1] + s[2] * d[2]);
+    h[0] += k1 * d[0]; h[1] += k1 * d[1]; h[2] += k1 * d[2];
+    if (k2perp != R(0)) {
+        const R t = k2perp * (s[0] * k2pd[0] + s[1] * k2pd[1] + s[2] * k2pd[2]);
+        h[0] += t * k2pd[0]; h[1] += t * k2pd[1]; h[2] += t * k2pd[2];
     }
-    if (c.k4perp_f != 0.0 || c.k4par_f != 0.0) {
+    if (k2par != R(0)) {
+        const R t = k2par * (s[0] * k2ad[0] + s[1] * k2ad[1] + s[2] * k2ad[2]);
+        h[0] += t * k2ad[0]; h[1] += t * k2ad[1]; h[2] += t * k2ad[2];
+    }
+    if (k4perp != R(0) || k4par != R(0)) {
 #pragma unroll
         for (int dir = 0; dir < 3; dir++) {
-            const R p0 = (R)c.k4perpdirs[3 * dir], p1 = (R)c.k4perpdirs[3 * dir + 1], p2 = (R)c.k4perpdirs[3 * dir + 2];
-            const R q0 = (R)c.k4pardirs[3 * dir], q1 = (R)c.k4pardirs[3 * dir + 1], q2 = (R)c.k4pardirs[3 * dir + 2];
-            const R tp = (R)c.k4perp_f * (s[0] * p0 + s[1] * p1 + s[2] * p2);
-            const R tq = (R)c.k4par_f * (s[0] * q0 + s[1] * q1 + s[2] * q2);
-            h[0] += tp * p0 + tq * q0; h[1] += tp * p1 + tq * q1; h[2] += tp * p2 + tq * q2;
+            const R* p = k4pd + 3 * dir;
+            const R* q = k4ad + 3 * dir;
+            const R tp = k4perp * (s[0] * p[0] + s[1] * p[1] + s[2] * p[2]);
+            const R tq = k4par * (s[0] * q[0] + s[1] * q[1] + s[2] * q[2]);
+            h[0] += tp * p[0] + tq * q[0]; h[1] += tp * p[1] + tq * q[1]; h[2] += tp * p[2] + tq * q[2];
         }
     }
 }
@@ -77,7 +92,7 @@ __device__ __forceinline__ void llg_rhs(R llgpf, R lambda, const R s[3], const R
 }
 
 __device__ __forceinline__ void renorm(double v[3]) {
-    const double inv = 1.0 / sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    const double inv = rsqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
     v[0] *= inv; v[1] *= inv; v[2] *= inv;
 }
 
@@ -101,10 +116,10 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* tab = reinterpret_cast<R*>(smem_raw);
     if constexpr (EX == ASD_EXCH_CSR) {
-        if (sell.typed) load_table<R>(table_of<R>(sell), (FULL ? 9u : 3u) * sell.ntypes, tab);
+        if (sell.typed) load_table<R>(table_of<R>(sell), table_stride<FULL>() *sell.ntypes, tab);
     }
     if constexpr (EX == ASD_EXCH_DIA) {
-        if (dia.dtype) load_table<R>(table_of<R>(dia), (FULL ? 9u : 3u) * dia.ntypes, tab);
+        if (dia.dtype) load_table<R>(table_of<R>(dia), table_stride<FULL>() *dia.ntypes, tab);
     }
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
@@ -122,30 +137,35 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
     const uint32_t at = atom_of(c, i);
     const MatConst& mc = c.mat[at];
     const uint32_t r = replica_of(c, i);
-    const double sqrtT = __ldg(c.rep_sqrtT + r);
+    constexpr bool F32 = sizeof(R) == 4;
     R lrn[3] = {R(0), R(0), R(0)};
-    if (sqrtT > 0.0) {
-        const uint32_t stream = __ldg(c.rep_stream + r), local = i - __ldg(c.rep_off + r);
-        if constexpr (sizeof(R) == 4) {
+    if constexpr (F32) {
+        const float sqrtT = __ldg(c.rep_sqrtT_f + r);
+        if (sqrtT > 0.0f) {
             float xi[3];
-            thermal_normals_f(c.seed, stream, local, t, xi);
-            const float tp = (float)(sqrtT * mc.sigma);
+            thermal_normals_f(c.seed, __ldg(c.rep_stream + r), i - __ldg(c.rep_off + r), t, xi);
+            const float tp = sqrtT * mc.sigma_f;
             lrn[0] = xi[0] * tp; lrn[1] = xi[1] * tp; lrn[2] = xi[2] * tp;
-        } else {
+        }
+    } else {
+        const double sqrtT = __ldg(c.rep_sqrtT + r);
+        if (sqrtT > 0.0) {
             double xi[3];
-            thermal_normals(c.seed, stream, local, t, xi);
+            thermal_normals(c.seed, __ldg(c.rep_stream + r), i - __ldg(c.rep_off + r), t, xi);
             const double tp = sqrtT * mc.sigma;
             lrn[0] = xi[0] * tp; lrn[1] = xi[1] * tp; lrn[2] = xi[2] * tp;
         }
     }
     const double* dyn = c.dyn;
+    const R* dynr;
+    if constexpr (F32) dynr = c.dynf; else dynr = c.dyn;
     if (a.stag.p[0]) {
-        const R sc = (R)dyn[DYN_STAG_SCALE];
+        const R sc = dynr[DYN_STAG_SCALE];
         h[0] += sc * a.stag.p[0][i]; h[1] += sc * a.stag.p[1][i]; h[2] += sc * a.stag.p[2][i];
     }
-    h[0] += lrn[0] + (R)dyn[DYN_APPLIED];
-    h[1] += lrn[1] + (R)dyn[DYN_APPLIED + 1];
-    h[2] += lrn[2] + (R)dyn[DYN_APPLIED + 2];
+    h[0] += lrn[0] + dynr[DYN_APPLIED];
+    h[1] += lrn[1] + dynr[DYN_APPLIED + 1];
+    h[2] += lrn[2] + dynr[DYN_APPLIED + 2];
 
     // stage spin at this site
     R sv[3] = {a.src.p[0][i], a.src.p[1][i], a.src.p[2][i]};
@@ -153,59 +173,92 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
     if (kind >= 11 && (c.flags & ASD_FLAG_RK_STAGE_SPIN_MIXED)) { sv[1] = a.base.p[1][i]; sv[2] = a.base.p[2][i]; }
     anis_field<R>(c, mc, sv, h);
     R f[3];
-    llg_rhs<R>((R)mc.llgpf, (R)mc.lambda, sv, h, f);
+    if constexpr (F32) llg_rhs<R>(mc.llgpf_f, mc.lambda_f, sv, h, f);
+    else llg_rhs<R>(mc.llgpf, mc.lambda, sv, h, f);
 
-    // the new S needs the full-precision base; intermediate stage spins use the hi part
     const bool final_spin = kind == 2 || (kind >= 10 && kind - 10 == a.nst - 1);
-    double S[3] = {(double)a.base.p[0][i], (double)a.base.p[1][i], (double)a.base.p[2][i]};
-    if constexpr (COMP) {
-        if (final_spin) { S[0] += (double)a.base_lo.p[0][i]; S[1] += (double)a.base_lo.p[1][i]; S[2] += (double)a.base_lo.p[2][i]; }
-    }
-    const double rdt = c.rdt;
-    double o[3];
-    if (kind == 1) {
-        for (int j = 0; j < 3; j++) { a.fn.p[j][i] = f[j]; o[j] = S[j] + rdt * (double)f[j]; }
-    } else if (kind == 2) {
-        for (int j = 0; j < 3; j++) o[j] = S[j] + 0.5 * rdt * ((double)a.fn.p[j][i] + (double)f[j]);
-        if ((double)t == dyn[DYN_DET_STEP])
-            for (int j = 0; j < 3; j++) a.det.p[j][i] = h[j] - lrn[j];
-    } else {
-        const int st = kind - 10, nst = a.nst;
-        const bool dbl = (c.flags & ASD_FLAG_RK_DOUBLE_RDT) != 0;
-        double k[3];
-        for (int j = 0; j < 3; j++) k[j] = rdt * (double)f[j];
-        if (st < nst - 1) {
-            for (int j = 0; j < 3; j++) a.k[st].p[j][i] = (R)k[j];
+    R out[3];
+    if (!final_spin && F32) {
+        // FP32 form: intermediate stage spins (Heun S', RK stage vectors) only feed field
+        // evaluations, so they are formed and renormalised in single precision
+        const float rdt = c.rdt_f;
+        float o[3];
+        const float S[3] = {(float)a.base.p[0][i], (float)a.base.p[1][i], (float)a.base.p[2][i]};
+        if (kind == 1) {
+            for (int j = 0; j < 3; j++) { a.fn.p[j][i] = f[j]; o[j] = fmaf(rdt, (float)f[j], S[j]); }
+        } else {
+            const int st = kind - 10, nst = a.nst;
+            const bool dbl = (c.flags & ASD_FLAG_RK_DOUBLE_RDT) != 0;
             for (int j = 0; j < 3; j++) {
-                double inc;
+                const float k = rdt * (float)f[j];
+                a.k[st].p[j][i] = (R)k;
+                float inc;
                 if (nst == 4) {
-                    inc = k[j] * (st == 2 ? 1.0 : 0.5);
+                    inc = k * (st == 2 ? 1.0f : 0.5f);
                 } else {
-                    inc = FRK5B[st][st] * k[j];
-                    for (int b = 0; b < st; b++) inc += FRK5B[st][b] * (double)a.k[b].p[j][i];
+                    inc = (float)FRK5B[st][st] * k;
+                    for (int b = 0; b < st; b++) inc = fmaf((float)FRK5B[st][b], (float)a.k[b].p[j][i], inc);
                 }
                 o[j] = S[j] + (dbl ? rdt * inc : inc);
             }
+        }
+        const float inv = rsqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
+        for (int j = 0; j < 3; j++) out[j] = (R)(o[j] * inv);
+        for (int j = 0; j < 3; j++) a.out.p[j][i] = out[j];
+    } else {
+        // new S (and every stage of the FP64 fused form): FP64 accumulation from the
+        // full-precision base, FP64 renormalisation
+        double S[3] = {(double)a.base.p[0][i], (double)a.base.p[1][i], (double)a.base.p[2][i]};
+        if constexpr (COMP) {
+            if (final_spin) { S[0] += (double)a.base_lo.p[0][i]; S[1] += (double)a.base_lo.p[1][i]; S[2] += (double)a.base_lo.p[2][i]; }
+        }
+        const double rdt = c.rdt;
+        double o[3];
+        if (kind == 1) {
+            for (int j = 0; j < 3; j++) { a.fn.p[j][i] = f[j]; o[j] = S[j] + rdt * (double)f[j]; }
+        } else if (kind == 2) {
+            for (int j = 0; j < 3; j++) o[j] = S[j] + 0.5 * rdt * (double)(a.fn.p[j][i] + f[j]);
+            if ((double)t == dyn[DYN_DET_STEP])
+                for (int j = 0; j < 3; j++) a.det.p[j][i] = h[j] - lrn[j];
         } else {
-            const double* C = nst == 4 ? FRK4C : FRK5C;
-            for (int j = 0; j < 3; j++) {
-                double acc = C[st] * k[j];
-                for (int b = 0; b < st; b++) acc += C[b] * (double)a.k[b].p[j][i];
-                o[j] = S[j] + acc;
+            const int st = kind - 10, nst = a.nst;
+            const bool dbl = (c.flags & ASD_FLAG_RK_DOUBLE_RDT) != 0;
+            double k[3];
+            for (int j = 0; j < 3; j++) k[j] = rdt * (double)f[j];
+            if (st < nst - 1) {
+                for (int j = 0; j < 3; j++) a.k[st].p[j][i] = (R)k[j];
+                for (int j = 0; j < 3; j++) {
+                    double inc;
+                    if (nst == 4) {
+                        inc = k[j] * (st == 2 ? 1.0 : 0.5);
+                    } else {
+                        inc = FRK5B[st][st] * k[j];
+                        for (int b = 0; b < st; b++) inc += FRK5B[st][b] * (double)a.k[b].p[j][i];
+                    }
+                    o[j] = S[j] + (dbl ? rdt * inc : inc);
+                }
+            } else {
+                const double* C = nst == 4 ? FRK4C : FRK5C;
+                for (int j = 0; j < 3; j++) {
+                    double acc = C[st] * k[j];
+                    for (int b = 0; b < st; b++) acc += C[b] * (double)a.k[b].p[j][i];
+                    o[j] = S[j] + acc;
+                }
             }
         }
-    }
-    renorm(o);
-    for (int j = 0; j < 3; j++) {
-        const R hi = (R)o[j];
-        a.out.p[j][i] = hi;
-        if constexpr (COMP) { if (final_spin) a.out_lo.p[j][i] = (float)(o[j] - (double)hi); }
+        renorm(o);
+        for (int j = 0; j < 3; j++) {
+            const R hi = (R)o[j];
+            out[j] = hi;
+            a.out.p[j][i] = hi;
+            if constexpr (COMP) { if (final_spin) a.out_lo.p[j][i] = (float)(o[j] - (double)hi); }
+        }
     }
     if (a.lr.mr) {
         const float wv = __ldg(a.lr.w + i);
-        a.lr.mr[midx] = (float)o[0] * wv;
-        a.lr.mr[a.lr.P + midx] = (float)o[1] * wv;
-        a.lr.mr[2 * a.lr.P + midx] = (float)o[2] * wv;
+        a.lr.mr[midx] = (float)out[0] * wv;
+        a.lr.mr[a.lr.P + midx] = (float)out[1] * wv;
+        a.lr.mr[2 * a.lr.P + midx] = (float)out[2] * wv;
     }
 }
 
@@ -250,8 +303,8 @@ cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
     const int B = hd->block;
     const unsigned grid = (hd->n + B - 1) / B;
     size_t smem = 0;
-    if (EX == ASD_EXCH_CSR && hd->sell.typed) smem = sizeof(R) * (FULL ? 9 : 3) * hd->sell.ntypes;
-    if (EX == ASD_EXCH_DIA && hd->dia.dtype) smem = sizeof(R) * (FULL ? 9 : 3) * hd->dia.ntypes;
+    if (EX == ASD_EXCH_CSR && hd->sell.typed) smem = sizeof(R) * table_stride<FULL>() *hd->sell.ntypes;
+    if (EX == ASD_EXCH_DIA && hd->dia.dtype) smem = sizeof(R) * table_stride<FULL>() *hd->dia.ntypes;
     if (hd->timing) cudaEventRecord(hd->kev[0], hd->stream);
     stage_kernel<R, EX, FULL, COMP><<<grid, B, smem, hd->stream>>>(hd->sc, hd->sell, hd->dia, a);
     hd->launches += 1;

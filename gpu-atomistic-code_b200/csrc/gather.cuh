@@ -37,27 +37,52 @@ __device__ __forceinline__ const R* table_of(const DiaDev& m) {
     if constexpr (sizeof(R) == 4) return m.tab_f; else return m.tab_d;
 }
 
+// Table row stride: 4 (xx, yy, zz, 0) for the diagonal form, 12 (9 + 3 zeros) for full tensors.
+template <bool FULL>
+__host__ __device__ constexpr uint32_t table_stride() { return FULL ? 12u : 4u; }
+
+// h += J_t (x, y, z) for tensor id t of the shared-memory table (type-major rows).
+template <typename R, bool FULL>
+__device__ __forceinline__ void accumulate_typed(const R* tab, uint32_t t, R x, R y, R z, R h[3]) {
+    if constexpr (sizeof(R) == 4) {
+        const float4* T = reinterpret_cast<const float4*>(tab) + t * (FULL ? 3 : 1);
+        const float4 a = T[0];
+        if (!FULL) {
+            h[0] = fmaf(a.x, x, h[0]);
+            h[1] = fmaf(a.y, y, h[1]);
+            h[2] = fmaf(a.z, z, h[2]);
+        } else {
+            const float4 b = T[1];
+            const float4 c = T[2];
+            h[0] = fmaf(a.x, x, fmaf(a.y, y, fmaf(a.z, z, h[0])));
+            h[1] = fmaf(a.w, x, fmaf(b.x, y, fmaf(b.y, z, h[1])));
+            h[2] = fmaf(b.z, x, fmaf(b.w, y, fmaf(c.x, z, h[2])));
+        }
+    } else {
+        const R* T = tab + t * table_stride<FULL>();
+        if (!FULL) {
+            h[0] += T[0] * x; h[1] += T[1] * y; h[2] += T[2] * z;
+        } else {
+            h[0] += T[0] * x + T[1] * y + T[2] * z;
+            h[1] += T[3] * x + T[4] * y + T[5] * z;
+            h[2] += T[6] * x + T[7] * y + T[8] * z;
+        }
+    }
+}
+
 // h += sum over the row's entries of J_e S_col(e), SELL-32 layout (one warp per slice).
 template <typename R, bool FULL>
 __device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const CVec3<R>& s, const R* tab, R h[3]) {
     const uint32_t sl = i >> 5, lane = i & 31u;
     const uint32_t p0 = __ldg(m.slice_ptr + sl), p1 = __ldg(m.slice_ptr + sl + 1);
     if (m.typed) {
-        const uint32_t nt = m.ntypes, mask = (1u << m.colbits) - 1u, cb = m.colbits;
+        const uint32_t mask = (1u << m.colbits) - 1u, cb = m.colbits;
 #pragma unroll 4
         for (uint32_t e = p0 + lane; e < p1; e += 32) {
             const uint32_t w = ldcs(m.typed + e);
             const uint32_t j = w & mask, t = w >> cb;
             const R x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
-            if (!FULL) {
-                h[0] += tab[t] * x;
-                h[1] += tab[nt + t] * y;
-                h[2] += tab[2 * nt + t] * z;
-            } else {
-                h[0] += tab[t] * x + tab[nt + t] * y + tab[2 * nt + t] * z;
-                h[1] += tab[3 * nt + t] * x + tab[4 * nt + t] * y + tab[5 * nt + t] * z;
-                h[2] += tab[6 * nt + t] * x + tab[7 * nt + t] * y + tab[8 * nt + t] * z;
-            }
+            accumulate_typed<R, FULL>(tab, t, x, y, z, h);
         }
         return;
     }
@@ -103,22 +128,13 @@ template <typename R, bool FULL>
 __device__ __forceinline__ void gather_dia(const DiaDev& m, uint32_t n, uint32_t i, const CVec3<R>& s, const R* tab,
                                            R h[3]) {
     if (m.dtype) {
-        const uint32_t nt = m.ntypes;
         for (uint32_t d = 0; d < m.ndiag; d++) {
             const int64_t col = (int64_t)i + __ldg(m.off + d);
             if (col < 0 || col >= (int64_t)n) continue;
             const uint32_t t = ldcs(m.dtype + (size_t)d * n + i);
             if (t == 0) continue;
             const R x = __ldg(s.p[0] + col), y = __ldg(s.p[1] + col), z = __ldg(s.p[2] + col);
-            if (!FULL) {
-                h[0] += tab[t] * x;
-                h[1] += tab[nt + t] * y;
-                h[2] += tab[2 * nt + t] * z;
-            } else {
-                h[0] += tab[t] * x + tab[nt + t] * y + tab[2 * nt + t] * z;
-                h[1] += tab[3 * nt + t] * x + tab[4 * nt + t] * y + tab[5 * nt + t] * z;
-                h[2] += tab[6 * nt + t] * x + tab[7 * nt + t] * y + tab[8 * nt + t] * z;
-            }
+            accumulate_typed<R, FULL>(tab, t, x, y, z, h);
         }
         return;
     }

@@ -98,6 +98,7 @@ struct asd_handle {
     // device: replica tables, atoms, mutable scalars
     uint32_t *d_rep_off = nullptr, *d_rep_stream = nullptr, *d_atom = nullptr;
     double *d_rep_sqrtT = nullptr, *d_dyn = nullptr;
+    float *d_rep_sqrtT_f = nullptr, *d_dynf = nullptr;
     uint64_t* d_step = nullptr;
     // FP32 / FP64-fused state, SoA
     float *sf[3] = {nullptr}, *sl[3] = {nullptr}, *esf[3] = {nullptr}, *fnf[3] = {nullptr};
@@ -144,6 +145,7 @@ cudaError_t launch_field_only(asd_handle* h, double* d_out);
 cudaError_t launch_plain_field(asd_handle* h, double* d_out);
 cudaError_t launch_plain_ramp(asd_handle* h, double rv);
 cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v);
+cudaError_t launch_set_scalar_f(asd_handle* h, float* dst, float v);
 cudaError_t launch_magnetisation(asd_handle* h);
 cudaError_t launch_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, double* d_out,
                                    cudaStream_t st);

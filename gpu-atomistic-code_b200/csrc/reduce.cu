@@ -113,10 +113,10 @@ __global__ void field_k(StepConst c, SellDev sell, DiaDev dia, const R* __restri
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* tab = reinterpret_cast<R*>(smem_raw);
     if constexpr (EX == ASD_EXCH_CSR) {
-        if (sell.typed) load_table<R>(table_of<R>(sell), (FULL ? 9u : 3u) * sell.ntypes, tab);
+        if (sell.typed) load_table<R>(table_of<R>(sell), table_stride<FULL>() *sell.ntypes, tab);
     }
     if constexpr (EX == ASD_EXCH_DIA) {
-        if (dia.dtype) load_table<R>(table_of<R>(dia), (FULL ? 9u : 3u) * dia.ntypes, tab);
+        if (dia.dtype) load_table<R>(table_of<R>(dia), table_stride<FULL>() *dia.ntypes, tab);
     }
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;
@@ -153,7 +153,7 @@ cudaError_t field_t(asd_handle* h, double* out) {
     }
     const float inv_p = h->lr.P ? 1.0f / (float)h->lr.P : 0.f;
     const unsigned g = nb(h->n, 256);
-    const size_t cs = sizeof(R) * (h->full ? 9 : 3);
+    const size_t cs = sizeof(R) * (h->full ? table_stride<true>() : table_stride<false>());
     if (h->exch == ASD_EXCH_CSR) {
         const size_t sm = h->sell.typed ? cs * h->sell.ntypes : 0;
         if (h->full) field_k<R, ASD_EXCH_CSR, true><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
@@ -170,11 +170,18 @@ cudaError_t field_t(asd_handle* h, double* out) {
 }
 
 __global__ void set_scalar_k(double* dst, double v) { *dst = v; }
+__global__ void set_scalar_f_k(float* dst, float v) { *dst = v; }
 
 }  // namespace
 
 cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v) {
     set_scalar_k<<<1, 1, 0, h->stream>>>(dst, v);
+    h->launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_set_scalar_f(asd_handle* h, float* dst, float v) {
+    set_scalar_f_k<<<1, 1, 0, h->stream>>>(dst, v);
     h->launches += 1;
     return cudaGetLastError();
 }

@@ -145,8 +145,8 @@ void orc_thermal_normals(uint64_t seed, uint32_t stream, uint32_t spin, uint64_t
     out[2] = r2 * c3;
 }
 
-/* Single-precision variant (the FP32 form's generator): 23-bit uniforms
- * ((x>>9)+0.5)/2^23, ln to f^11, sin to psi^11, cos to psi^12, float fma. */
+/* Single-precision variant (the FP32 form's generator): uniforms (float(x)+0.5)/2^32,
+ * octant from the top 3 bits, ln to f^11, sin to psi^11, cos to psi^12, float fma. */
 static float logf_series(float x) {
     int e;
     float m = frexpf(x, &e);
@@ -164,10 +164,8 @@ static float logf_series(float x) {
 }
 
 static void sincosf_series(uint32_t x, float* sn, float* cs) {
-    const float v = ((float)(x >> 9) + 0.5f) * 0x1p-20f;
-    const float qd = floorf(v);
-    const int q = (int)qd;
-    const float r = v - qd;
+    const int q = (int)(x >> 29);
+    const float r = ((float)(x & 0x1FFFFFFFu) + 0.5f) * 0x1p-29f;
     const float psi = ((q & 1) ? (1.0f - r) : r) * 0x1.921fb6p-1f;
     const float mp2 = -(psi * psi);
     float sp = 0x1.ae6456p-26f;
@@ -201,8 +199,8 @@ void orc_thermal_normals_f(uint64_t seed, uint32_t stream, uint32_t spin, uint64
     uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
     uint32_t x[4];
     orc_philox4x32_10(ctr, key, x);
-    const float u0 = ((float)(x[0] >> 9) + 0.5f) * 0x1p-23f;
-    const float u2 = ((float)(x[2] >> 9) + 0.5f) * 0x1p-23f;
+    const float u0 = ((float)x[0] + 0.5f) * 0x1p-32f;
+    const float u2 = ((float)x[2] + 0.5f) * 0x1p-32f;
     const float r0 = sqrtf(-2.0f * logf_series(u0));
     const float r2 = sqrtf(-2.0f * logf_series(u2));
     float s1, c1, s3, c3;

@@ -50,7 +50,7 @@ def test_thermal_normals_f32_bit_exact(gpu):
         o = O.thermal_normals_f(seed, stream, 2000, step)
         assert np.array_equal(g, o)
         d = O.thermal_normals(seed, stream, 2000, step)
-        assert np.quantile(np.abs(g - d), 0.999) < 1e-5   # same Philox draw, float series
+        assert np.abs(g - d).max() < 1e-5   # same Philox draw, float series
 
 
 @pytest.mark.parametrize("T", [0.0, 300.0])
