@@ -40,6 +40,8 @@ EXPORTED = [
     "asd_set_temperature", "asd_set_applied", "asd_set_site_field", "asd_set_site_field_scale",
     "asd_magnetisation", "asd_num_sublattices", "asd_time_steps", "asd_time_kernels", "asd_kernel_stats",
     "asd_thermal_normals", "asd_build_csr", "asd_csr_to_dia", "asd_build_dipole_nr", "asd_fold_exchange_nr",
+    "asd_set_site_field_pulse", "asd_sample_magnetisation", "asd_magnetisation_stats",
+    "asd_reset_magnetisation_stats", "asd_sq_setup", "asd_sq_sample", "asd_sq_get",
 ]
 
 
@@ -114,6 +116,13 @@ def load_library(path: str = LIB_PATH):
         "asd_magnetisation_noalloc": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p],
                                       C.c_int),
         "asd_thermal_normals_f32": ([C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, C.POINTER(C.c_float)], C.c_int),
+        "asd_set_site_field_pulse": ([P, C.c_double, C.c_double, C.c_double], C.c_int),
+        "asd_sample_magnetisation": ([P], C.c_int),
+        "asd_magnetisation_stats": ([P, dp, C.c_size_t], C.c_int),
+        "asd_reset_magnetisation_stats": ([P], C.c_int),
+        "asd_sq_setup": ([P, C.c_uint32, dp, u32p, u32p, C.c_uint32, u32p, C.c_uint32], C.c_int),
+        "asd_sq_sample": ([P], C.c_int),
+        "asd_sq_get": ([P, dp, C.c_size_t, u32p], C.c_int),
         "asd_build_csr": ([u32p, C.POINTER(C.c_int), C.c_uint32, dp, C.c_uint32, u32p, u32p, i32p, dp, C.c_double,
                            u32p, u32p, dp, u32p], C.c_int),
         "asd_csr_to_dia": ([C.c_uint32, u32p, u32p, dp, C.c_uint32, i32p, dp, u32p], C.c_int),
@@ -325,6 +334,44 @@ class Handle:
 
     def set_site_field_scale(self, rv: float):
         _check(load_library().asd_set_site_field_scale(self.h, rv), self.h)
+
+    def set_site_field_pulse(self, amp: float, t0: float, sigma: float):
+        _check(load_library().asd_set_site_field_pulse(self.h, amp, t0, sigma), self.h)
+
+    def sample_magnetisation(self):
+        _check(load_library().asd_sample_magnetisation(self.h), self.h)
+
+    def magnetisation_stats(self):
+        """[replica, sublattice, (samples, mean |m_s|, variance, previous mean)]."""
+        out = np.empty(self.nrep * self.nsub * 4, dtype=np.float64)
+        _check(load_library().asd_magnetisation_stats(self.h, _p(out, C.c_double), len(out)), self.h)
+        return out.reshape(self.nrep, self.nsub, 4)
+
+    def reset_magnetisation_stats(self):
+        _check(load_library().asd_reset_magnetisation_stats(self.h), self.h)
+
+    def sq_setup(self, mesh, mesh_xyz, kpoints, max_samples: int, qaxis: int = 2, uo=None):
+        """Arm the S(q,t) sampler: spin i sits at mesh_xyz[i] of the lattice mesh; kpoints are
+        mesh indices (nk x 3); uo (nsub x 3) are the per-sublattice signs, 1 by default."""
+        m = np.ascontiguousarray(mesh, dtype=np.uint32).reshape(3)
+        xyz = np.ascontiguousarray(mesh_xyz, dtype=np.uint32).reshape(-1)
+        kp = np.ascontiguousarray(kpoints, dtype=np.uint32).reshape(-1)
+        u = None if uo is None else np.ascontiguousarray(uo, dtype=np.float64).reshape(-1)
+        _check(load_library().asd_sq_setup(self.h, qaxis, _p(u, C.c_double), _p(m, C.c_uint32), _p(xyz, C.c_uint32),
+                                           len(kp) // 3, _p(kp, C.c_uint32), max_samples), self.h)
+        self._sq_nk = len(kp) // 3
+        self._sq_max = max_samples
+
+    def sq_sample(self):
+        _check(load_library().asd_sq_sample(self.h), self.h)
+
+    def sq_series(self):
+        """psi_k(t) as a complex array [samples, nk]."""
+        out = np.empty(self._sq_max * self._sq_nk * 2, dtype=np.float64)
+        ns = C.c_uint32()
+        _check(load_library().asd_sq_get(self.h, _p(out, C.c_double), len(out), C.byref(ns)), self.h)
+        v = out[: ns.value * self._sq_nk * 2].reshape(ns.value, self._sq_nk, 2)
+        return v[..., 0] + 1j * v[..., 1]
 
     def magnetisation(self):
         out = np.empty(self.nrep * self.nsub * 3, dtype=np.float64)

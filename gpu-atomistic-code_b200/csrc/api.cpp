@@ -79,7 +79,9 @@ void free_all(asd_handle* h) {
     if (L.r2c) cufftDestroy(L.r2c);
     if (L.c2r) cufftDestroy(L.c2r);
     if (L.z2z) cufftDestroy(L.z2z);
-    F(h->d_magpart); F(h->d_mag); F(h->d_inv_count); F(h->d_sub_of_atom);
+    F(h->sq.idx); F(h->sq.sub); F(h->sq.uo); F(h->sq.kidx); F(h->sq.grid); F(h->sq.series);
+    if (h->sq.plan) cufftDestroy(h->sq.plan);
+    F(h->d_magpart); F(h->d_mag); F(h->d_inv_count); F(h->d_sub_of_atom); F(h->d_stats);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     if (h->kev[0]) cudaEventDestroy(h->kev[0]);
     if (h->kev[1]) cudaEventDestroy(h->kev[1]);
@@ -451,6 +453,7 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
             h->nsub = std::max(h->nsub, m.sublattice + 1);
         }
         sc.rdt = p.dt * p.gyro;
+        sc.dt = p.dt;
         sc.k2perp_f = 2.0 * p.k2perp / basemm;
         sc.k2par_f = 2.0 * p.k2par / basemm;
         sc.k4perp_f = 2.0 * p.k4perp / basemm;
@@ -491,6 +494,9 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         for (int a = 0; a < 3; a++) dyn[DYN_APPLIED + a] = p.applied[a];
         dyn[DYN_STAG_SCALE] = 1.0;
         dyn[DYN_DET_STEP] = -1.0;
+        dyn[DYN_PULSE_AMP] = 0.0;
+        dyn[DYN_PULSE_T0] = 0.0;
+        dyn[DYN_PULSE_ISIG] = 1.0;
         h->d_dyn = dupload(dyn.data(), dyn.size());
         std::vector<float> dynf(dyn.begin(), dyn.end());
         h->d_dynf = dupload(dynf.data(), dynf.size());
@@ -646,6 +652,7 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         // ---- site fields
         bool any_site = false;
         for (uint32_t r = 0; r < nsys; r++) any_site |= sys[r].site_field != nullptr;
+        h->has_site = any_site;
         if (any_site) {
             std::vector<double> prof(3 * (size_t)n, 0.0);
             for (uint32_t r = 0; r < nsys; r++)
@@ -677,6 +684,7 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
             h->magpart_len = (size_t)nsys * nchunk * h->nsub * 3;
             h->d_magpart = dalloc<double>(h->magpart_len);
             h->d_mag = dalloc<double>((size_t)nsys * h->nsub * 3);
+            h->d_stats = dalloc<double>((size_t)nsys * h->nsub * 4);
             std::vector<double> inv((size_t)nsys * h->nsub, 0.0);
             for (uint32_t r = 0; r < nsys; r++) {
                 std::vector<uint32_t> cnt(h->nsub, 0);
@@ -876,6 +884,8 @@ int asd_set_site_field(asd_handle* h, const double* prof, size_t n_spins) {
         }
         // CsetStagFields resets the ramp: CHstg = CInitHstg
         set_dyn(h, DYN_STAG_SCALE, 1.0);
+        h->stag_rv = 1.0;
+        h->has_site = prof != nullptr;
     } catch (const Fail& f) { return fail(h, f); }
     return ASD_OK;
 }
@@ -887,6 +897,132 @@ int asd_set_site_field_scale(asd_handle* h, double rv) {
         CK(cudaSetDevice(h->device));
         if (h->p.precision == ASD_FP64_PLAIN) CK(launch_plain_ramp(h, rv));
         else set_dyn(h, DYN_STAG_SCALE, rv);
+        h->stag_rv = rv;
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_set_site_field_pulse(asd_handle* h, double amp, double t0, double sigma) {
+    if (!h) return ASD_EINVAL;
+    try {
+        REQUIRE(std::isfinite(amp) && std::isfinite(t0) && std::isfinite(sigma), "non-finite pulse parameter");
+        REQUIRE(amp == 0.0 || sigma > 0.0, "pulse width must be positive");
+        CK(cudaSetDevice(h->device));
+        h->pulse_amp = amp;
+        h->pulse_t0 = t0;
+        h->pulse_sigma = amp == 0.0 ? 1.0 : sigma;
+        if (h->p.precision == ASD_FP64_PLAIN) {
+            if (amp == 0.0) CK(launch_plain_ramp(h, h->stag_rv));   // back to the plain ramp value
+        } else {
+            set_dyn(h, DYN_PULSE_T0, t0);
+            set_dyn(h, DYN_PULSE_ISIG, 1.0 / h->pulse_sigma);
+            set_dyn(h, DYN_PULSE_AMP, amp);
+        }
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_sample_magnetisation(asd_handle* h) {
+    if (!h) return ASD_EINVAL;
+    try {
+        CK(cudaSetDevice(h->device));
+        CK(launch_magnetisation(h));
+        CK(launch_mag_push(h));
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_magnetisation_stats(asd_handle* h, double* out, size_t out_len) {
+    if (!h) return ASD_EINVAL;
+    try {
+        const size_t m = (size_t)h->nrep * h->nsub * 4;
+        REQUIRE(out && out_len >= m, "output must hold nrep*nsub*4 doubles");
+        CK(cudaSetDevice(h->device));
+        CK(cudaMemcpyAsync(out, h->d_stats, m * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (size_t q = 0; q < m; q += 4) {           // M2 -> variance (n-1 normalised), inc/util.h:68-71
+            const double n = out[q];
+            out[q + 2] = n > 1 ? out[q + 2] / (n - 1) : 0.0;
+        }
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_sq_setup(asd_handle* h, uint32_t qaxis, const double* uo, const uint32_t mesh[3], const uint32_t* mesh_xyz,
+                 uint32_t nk, const uint32_t* kpoints, uint32_t max_samples) {
+    if (!h) return ASD_EINVAL;
+    try {
+        REQUIRE(h->nrep == 1, "S(q,t) sampling supports one replica per handle");
+        REQUIRE(qaxis <= 2, "qaxis must be 0, 1 or 2");
+        REQUIRE(mesh && mesh_xyz && kpoints && nk > 0 && max_samples > 0, "mesh, mesh_xyz, kpoints, nk, max_samples");
+        REQUIRE(mesh[0] && mesh[1] && mesh[2], "empty mesh");
+        const size_t P = (size_t)mesh[0] * mesh[1] * mesh[2];
+        REQUIRE(P < (1ull << 31) && (size_t)max_samples * nk < (1ull << 31), "sampler too large");
+        CK(cudaSetDevice(h->device));
+        SqSampler& S = h->sq;
+        auto F = [](void* p) { if (p) cudaFree(p); };
+        F(S.idx); F(S.sub); F(S.uo); F(S.kidx); F(S.grid); F(S.series);
+        if (S.plan) cufftDestroy(S.plan);
+        S = SqSampler{};
+        std::vector<uint32_t> idx(h->n), sub(h->n), kidx(nk);
+        for (uint32_t i = 0; i < h->n; i++) {
+            const uint32_t x = mesh_xyz[3 * i], y = mesh_xyz[3 * i + 1], z = mesh_xyz[3 * i + 2];
+            REQUIRE(x < mesh[0] && y < mesh[1] && z < mesh[2], "mesh_xyz outside the mesh");
+            idx[i] = (uint32_t)(((size_t)x * mesh[1] + y) * mesh[2] + z);
+            sub[i] = h->h_sub_of_mat[h->h_atom.empty() ? i % h->nmat : h->h_atom[i]];
+        }
+        for (uint32_t q = 0; q < nk; q++) {
+            const uint32_t* k = kpoints + 3 * q;
+            REQUIRE(k[0] < mesh[0] && k[1] < mesh[1] && k[2] < mesh[2], "k-point outside the mesh");
+            kidx[q] = (uint32_t)(((size_t)k[0] * mesh[1] + k[1]) * mesh[2] + k[2]);
+        }
+        std::vector<double> u(3 * (size_t)h->nsub, 1.0);
+        if (uo) u.assign(uo, uo + 3 * (size_t)h->nsub);
+        S.idx = dupload(idx.data(), idx.size());
+        S.sub = dupload(sub.data(), sub.size());
+        S.uo = dupload(u.data(), u.size());
+        S.kidx = dupload(kidx.data(), kidx.size());
+        S.grid = dalloc<double2>(P);
+        S.series = dalloc<double2>((size_t)max_samples * nk);
+        int dims[3] = {(int)mesh[0], (int)mesh[1], (int)mesh[2]};
+        CKFFT(cufftPlanMany(&S.plan, 3, dims, nullptr, 1, (int)P, nullptr, 1, (int)P, CUFFT_Z2Z, 1));
+        CKFFT(cufftSetStream(S.plan, h->stream));
+        S.qaxis = qaxis; S.nk = nk; S.max_samples = max_samples; S.P = P; S.on = true;
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_sq_sample(asd_handle* h) {
+    if (!h) return ASD_EINVAL;
+    try {
+        if (!h->sq.on) throw Fail{ASD_ESTATE, "asd_sq_setup has not been called"};
+        if (h->sq.nsamples >= h->sq.max_samples) throw Fail{ASD_ESTATE, "S(q,t) series is full"};
+        CK(cudaSetDevice(h->device));
+        CK(launch_sq_sample(h));
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_sq_get(asd_handle* h, double* out, size_t out_len, uint32_t* nsamples) {
+    if (!h) return ASD_EINVAL;
+    try {
+        if (!h->sq.on) throw Fail{ASD_ESTATE, "asd_sq_setup has not been called"};
+        const size_t m = (size_t)h->sq.nsamples * h->sq.nk * 2;
+        REQUIRE(out && out_len >= m, "output must hold nsamples*nk*2 doubles");
+        CK(cudaSetDevice(h->device));
+        CK(cudaMemcpyAsync(out, h->sq.series, m * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (nsamples) *nsamples = h->sq.nsamples;
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_reset_magnetisation_stats(asd_handle* h) {
+    if (!h) return ASD_EINVAL;
+    try {
+        CK(cudaSetDevice(h->device));
+        CK(cudaMemsetAsync(h->d_stats, 0, (size_t)h->nrep * h->nsub * 4 * sizeof(double), h->stream));
+        CK(cudaStreamSynchronize(h->stream));
     } catch (const Fail& f) { return fail(h, f); }
     return ASD_OK;
 }

@@ -32,6 +32,7 @@ struct StepConst {
     uint32_t flags;
     MatConst mat[ASD_MAX_MAT];
     double rdt;         // dt * gyro (src/llg.cpp:306)
+    double dt;          // [s]
     double k2perp_f, k2perpdir[3], k2par_f, k2pardir[3];   // 2K/basemm (src/cuint.cu:99)
     double k4perp_f, k4perpdirs[9], k4par_f, k4pardirs[9];
     uint64_t seed;
@@ -50,7 +51,29 @@ struct StepConst {
 };
 
 // Layout of the mutable scalar block (device memory, updated between launches).
-enum { DYN_APPLIED = 0, DYN_STAG_SCALE = 3, DYN_DET_STEP = 4, DYN_COUNT = 8 };
+enum {
+    DYN_APPLIED = 0, DYN_STAG_SCALE = 3, DYN_DET_STEP = 4,
+    DYN_PULSE_AMP = 5, DYN_PULSE_T0 = 6, DYN_PULSE_ISIG = 7,   // site-field envelope
+    DYN_COUNT = 8
+};
+
+// Site-field multiplier at step t: rv, times amp exp(-((t dt - t0)/sigma)^2/2) when amp != 0.
+__device__ __forceinline__ float site_scale_f(const float* dynf, const double* dyn, uint64_t t, double dt) {
+    float sc = dynf[DYN_STAG_SCALE];
+    if (dynf[DYN_PULSE_AMP] != 0.0f) {
+        const float x = (float)(((double)t * dt - dyn[DYN_PULSE_T0]) * dyn[DYN_PULSE_ISIG]);
+        sc *= dynf[DYN_PULSE_AMP] * expf(-0.5f * x * x);
+    }
+    return sc;
+}
+__device__ __forceinline__ double site_scale_d(const double* dyn, uint64_t t, double dt) {
+    double sc = dyn[DYN_STAG_SCALE];
+    if (dyn[DYN_PULSE_AMP] != 0.0) {
+        const double x = ((double)t * dt - dyn[DYN_PULSE_T0]) * dyn[DYN_PULSE_ISIG];
+        sc *= dyn[DYN_PULSE_AMP] * exp(-0.5 * x * x);
+    }
+    return sc;
+}
 
 __device__ __forceinline__ uint32_t atom_of(const StepConst& c, uint32_t i) {
     return c.atom ? c.atom[i] : (c.nmat == 1 ? 0u : i % c.nmat);

@@ -160,7 +160,8 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
     const R* dynr;
     if constexpr (F32) dynr = c.dynf; else dynr = c.dyn;
     if (a.stag.p[0]) {
-        const R sc = dynr[DYN_STAG_SCALE];
+        R sc;
+        if constexpr (F32) sc = site_scale_f(c.dynf, dyn, t, c.dt); else sc = site_scale_d(dyn, t, c.dt);
         h[0] += sc * a.stag.p[0][i]; h[1] += sc * a.stag.p[1][i]; h[2] += sc * a.stag.p[2][i];
     }
     h[0] += lrn[0] + dynr[DYN_APPLIED];

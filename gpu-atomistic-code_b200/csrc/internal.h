@@ -72,6 +72,20 @@ struct LongRange {
     cufftHandle z2z = 0;
 };
 
+// In-situ S(q,t) sampler state (lattice mesh, complex FP64 grid, k-point series).
+struct SqSampler {
+    bool on = false;
+    uint32_t qaxis = 2, nk = 0, max_samples = 0, nsamples = 0;
+    size_t P = 0;
+    uint32_t* idx = nullptr;     // per-spin mesh index
+    uint32_t* sub = nullptr;     // per-spin sublattice
+    double* uo = nullptr;        // nsub x 3 signs
+    uint32_t* kidx = nullptr;    // per-k mesh index
+    double2* grid = nullptr;     // [P]
+    double2* series = nullptr;   // [max_samples][nk]
+    cufftHandle plan = 0;
+};
+
 struct KernelTimer {
     std::string name;
     double total_ms = 0.0;
@@ -123,6 +137,12 @@ struct asd_handle {
     uint64_t graph_launches = 0;
     bool lr_scattered = false;
     double nnz_per_row = 0.0;
+    // site-field ramp value and time envelope (host copies; the plain form ramps from the host)
+    double stag_rv = 1.0, pulse_amp = 0.0, pulse_t0 = 0.0, pulse_sigma = 1.0;
+    bool has_site = false;
+    // M(T) running statistics per (replica, sublattice): n, mean, M2, previous mean
+    double* d_stats = nullptr;
+    asd::SqSampler sq;
     // CUDA graph of a chunk of FP32 steps
     cudaGraphExec_t graph = nullptr;
     uint32_t graph_steps = 0;
@@ -146,6 +166,8 @@ cudaError_t launch_plain_field(asd_handle* h, double* d_out);
 cudaError_t launch_plain_ramp(asd_handle* h, double rv);
 cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v);
 cudaError_t launch_set_scalar_f(asd_handle* h, float* dst, float v);
+cudaError_t launch_mag_push(asd_handle* h);
+cudaError_t launch_sq_sample(asd_handle* h);
 cudaError_t launch_magnetisation(asd_handle* h);
 cudaError_t launch_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, double* d_out,
                                    cudaStream_t st);

@@ -343,6 +343,12 @@ cudaError_t launch_plain_step(asd_handle* h, uint64_t t) {
     PlainSpin ps{h->p_sigma, h->p_llgpf, h->p_lambda, h->p_k1u, h->p_k1udir, h->p_hstg};
     const uint32_t upd = h->p.update ? h->p.update : 1;
     const bool dip_refresh = h->lr.mode == ASD_LR_DIPOLE && (t % upd) == 0;
+    if (h->pulse_amp != 0.0 && h->has_site) {
+        // the driver-side rampStag of every step (src/cuda.cu:38-41) with the pulse envelope
+        const double x = ((double)t * h->p.dt - h->pulse_t0) / h->pulse_sigma;
+        const double f = h->pulse_amp * exp(-0.5 * x * x);
+        if ((e = launch_plain_ramp(h, h->stag_rv * f)) != cudaSuccess) return e;
+    }
     if (h->p.integrator == ASD_HEUN) {
         if (dip_refresh && (e = launch_lr_eval_plain(h, h->p_s, h->p_hdemag, true)) != cudaSuccess) return e;
         if ((e = plain_field(h, h->p_s, h->p_ch)) != cudaSuccess) return e;

@@ -169,6 +169,27 @@ cudaError_t field_t(asd_handle* h, double* out) {
     return cudaGetLastError();
 }
 
+// Welford update of |m_s| per (replica, sublattice), the RunningStat::Push of inc/util.h:30-50:
+// st[4q..4q+3] = n, mean, M2, mean before this sample.
+__global__ void mag_push_k(uint32_t m, const double* __restrict__ mag, double* __restrict__ st) {
+    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= m) return;
+    const double x = sqrt(mag[3 * q] * mag[3 * q] + mag[3 * q + 1] * mag[3 * q + 1] + mag[3 * q + 2] * mag[3 * q + 2]);
+    double* s = st + 4 * (size_t)q;
+    const double n = s[0] + 1.0;
+    const double old = s[1];
+    s[3] = old;
+    if (n == 1.0) {
+        s[1] = x;
+        s[2] = 0.0;
+    } else {
+        const double mean = old + (x - old) / n;
+        s[2] = s[2] + (x - old) * (x - mean);
+        s[1] = mean;
+    }
+    s[0] = n;
+}
+
 __global__ void set_scalar_k(double* dst, double v) { *dst = v; }
 __global__ void set_scalar_f_k(float* dst, float v) { *dst = v; }
 
@@ -176,6 +197,13 @@ __global__ void set_scalar_f_k(float* dst, float v) { *dst = v; }
 
 cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v) {
     set_scalar_k<<<1, 1, 0, h->stream>>>(dst, v);
+    h->launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mag_push(asd_handle* h) {
+    const uint32_t m = h->nrep * h->nsub;
+    mag_push_k<<<nb(m, 128), 128, 0, h->stream>>>(m, h->d_mag, h->d_stats);
     h->launches += 1;
     return cudaGetLastError();
 }

@@ -159,6 +159,11 @@ int asd_set_site_field(asd_handle* h, const double* profile, size_t n_spins);
 /* cullg::rampStag(rv) (src/cuda.cu:38-41): site field = rv * profile. */
 int asd_set_site_field_scale(asd_handle* h, double rv);
 
+/* Time envelope of the site field, the in-step form of a driver calling rampStag every step
+ * (src/cuda.cu:38-41, src/ramp_stag.cpp): site field = rv * amp * exp(-(t-t0)^2/(2 sigma^2)) *
+ * profile with t = step*dt [s]; amp = 0 switches the envelope off (site field = rv * profile). */
+int asd_set_site_field_pulse(asd_handle* h, double amp, double t0, double sigma);
+
 /* util::calc_mag method 0 (src/util_mag.cpp:44-65) per replica: out[(r*nsub+s)*3+c], FP64 sums. */
 int asd_magnetisation(asd_handle* h, double* out, size_t out_len);
 /* Sublattice-mean magnetisation of spins that already sit in device memory, without any
@@ -179,6 +184,26 @@ int asd_magnetisation(asd_handle* h, double* out, size_t out_len);
 #define ASD_NOALLOC_MAX_SUBLATTICES 16
 int asd_magnetisation_noalloc(const double* d_spins, uint32_t nspins, const uint32_t* d_sublattice, uint32_t nsub,
                               double* d_out, void* stream);
+/* M(T) statistics kept on the device, the RunningStat of sim::MvT (src/mvt.cpp:258-275,
+ * inc/util.h:22-75): each sample computes every replica's sublattice means and pushes
+ * |m_s| into a Welford accumulator per (replica, sublattice).  Sampling enqueues work on
+ * the handle's stream and returns without a host synchronisation. */
+int asd_sample_magnetisation(asd_handle* h);
+/* out[(r*nsub+s)*4 + k], k = 0: samples, 1: mean |m_s|, 2: variance (n-1 normalised),
+ * 3: the mean before the last sample (MvT's convergence test uses both means). */
+int asd_magnetisation_stats(asd_handle* h, double* out, size_t out_len);
+int asd_reset_magnetisation_stats(asd_handle* h);
+/* In-situ S(q,t) sampling, the spin-map transform of sim::timeseries (src/timeseries.cpp:274-330):
+ * psi(r) = uo_a S_a + i uo_b S_b with (a,b) the axes transverse to qaxis (0: y,z; 1: x,z; 2: x,y),
+ * uo[s*3+c] per sublattice (NULL: all 1), forward 3D FFT on the lattice mesh mesh[3] with each
+ * spin at mesh_xyz (3 per spin), psi_k kept on the device for the nk k-points kpoints (3 mesh
+ * indices each) per sample, up to max_samples samples.  One replica per handle. */
+int asd_sq_setup(asd_handle* h, uint32_t qaxis, const double* uo, const uint32_t mesh[3], const uint32_t* mesh_xyz,
+                 uint32_t nk, const uint32_t* kpoints, uint32_t max_samples);
+/* Record psi_k of the current spins (enqueued on the handle's stream, no host synchronisation). */
+int asd_sq_sample(asd_handle* h);
+/* Copy the recorded series out: out[(sample*nk + k)*2 + {re, im}]; *nsamples = samples recorded. */
+int asd_sq_get(asd_handle* h, double* out, size_t out_len, uint32_t* nsamples);
 /* Number of sublattices (GetNMS) of the handle. */
 int asd_num_sublattices(const asd_handle* h, uint32_t* nsub);
 

@@ -19,6 +19,7 @@ struct orc_ctx {
     double k2perp, k2perpdir[3], k2par, k2pardir[3], k4perp, k4perpdirs[9], k4par, k4pardirs[9], basemm;
     int integrator;
     double rdt, applied[3], stag_scale;
+    double pulse_amp, pulse_t0, pulse_sigma, dt, cur_scale;
     uint32_t nrep, *rep_off, *rep_stream;
     double* rep_T;
     int exch, full;
@@ -544,8 +545,8 @@ static void total_field(const orc_ctx* c, uint32_t i, const double* ch_exch, con
     const double TP = sqrt(c->rep_T[r]) * c->sigma[i];
     const double* xi = c->noise + 3 * (size_t)i;
     lrn[0] = xi[0] * TP; lrn[1] = xi[1] * TP; lrn[2] = xi[2] * TP;
-    const double hs[3] = {c->stag_scale * c->hstag[3 * (size_t)i], c->stag_scale * c->hstag[3 * (size_t)i + 1],
-                          c->stag_scale * c->hstag[3 * (size_t)i + 2]};
+    const double hs[3] = {c->cur_scale * c->hstag[3 * (size_t)i], c->cur_scale * c->hstag[3 * (size_t)i + 1],
+                          c->cur_scale * c->hstag[3 * (size_t)i + 2]};
     if (c->flags & ORC_CPU_SUM_ORDER) {
         /* llgCPU: Hx holds the exchange only, HDemag is separate, H4s = 0. */
         const double* hx = ch_exch + 3 * (size_t)i;
@@ -596,7 +597,26 @@ static void normalise(double v[3]) {
     v[0] /= mods; v[1] /= mods; v[2] /= mods;
 }
 
+/* Site-field multiplier of step t: the ramp value, times the Gaussian envelope
+ * amp exp(-x^2/2), x = (t dt - t0)/sigma, when a pulse is set (a driver calling
+ * rampStag every step, src/cuda.cu:38-41). */
+static void set_step_scale(orc_ctx* c, uint64_t t) {
+    if (c->pulse_amp != 0.0) {
+        const double x = ((double)t * c->dt - c->pulse_t0) / c->pulse_sigma;
+        const double f = c->pulse_amp * exp(-0.5 * x * x);
+        c->cur_scale = c->stag_scale * f;
+    } else {
+        c->cur_scale = c->stag_scale;
+    }
+}
+
+int orc_set_pulse(orc_ctx* c, double amp, double t0, double sigma, double dt) {
+    c->pulse_amp = amp; c->pulse_t0 = t0; c->pulse_sigma = sigma; c->dt = dt;
+    return 0;
+}
+
 static void heun_step(orc_ctx* c, uint64_t t) {
+    set_step_scale(c, t);
     const uint32_t n = c->n;
     double* hsave = NULL;
     if (c->lr == ORC_LR_DIPOLE && t % c->update == 0) {
@@ -675,6 +695,7 @@ static const double RK5_C[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0,
 /* One RK4 / RK5 step with the launch sequence of src/cudaRK4.cu:38-233 and
  * src/cudaRK5.cu (SpMV of the stage spin, then the stage kernel). */
 static void rk_step(orc_ctx* c, uint64_t t) {
+    set_step_scale(c, t);
     const uint32_t n = c->n;
     const int nst = c->integrator == ORC_RK4 ? 4 : 6;
     const int dbl = (c->flags & ORC_RK_DOUBLE_RDT) != 0;

@@ -74,6 +74,8 @@ int orc_set_csr(orc_ctx* c, int full, uint32_t nnz, const uint32_t* xadj, const 
 /* Row-aligned DIA: data[comp][n*N+row] for 9 comps (src/matrix_conv.cpp:28-272). */
 int orc_set_dia(orc_ctx* c, int full, uint32_t ndiag, const int32_t* offsets, const double* val9);
 int orc_set_site_field(orc_ctx* c, const double* hstag, double scale);
+/* Gaussian time envelope of the site field: multiplier amp exp(-((t dt - t0)/sigma)^2 / 2). */
+int orc_set_pulse(orc_ctx* c, double amp, double t0, double sigma, double dt);
 /* Long-range field by direct summation on the periodic padded mesh:
  * H_i = sum_j Nr[s_i][s_j][a][b][(x_i-x_j) mod n] * w_j * S_j[b], with w_j = mu_j for
  * ORC_LR_DIPOLE (src/cufields.cu:355) and 1 for ORC_LR_FFT (src/cufields.cu:381).

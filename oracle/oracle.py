@@ -211,6 +211,16 @@ class Oracle:
         except Exception:
             pass
 
+    def set_pulse(self, amp, t0, sigma, dt):
+        L = olib()
+        L.orc_set_pulse.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double]
+        L.orc_set_pulse(self.c, amp, t0, sigma, dt)
+
+    def set_site_scale(self, rv):
+        hs = a64(np.concatenate([s.site_field for s in self.systems]))
+        self._keep.append(hs)
+        olib().orc_set_site_field(self.c, _ptr(hs, C.c_double), rv)
+
     def set_spins(self, s):
         s = a64(s).reshape(-1)
         olib().orc_set_spins(self.c, _ptr(s, C.c_double))

@@ -267,3 +267,89 @@ def test_errors_are_reported_not_fatal(gpu):
     with pytest.raises(A.AsdError) as e:
         A.Handle(A.RunParams(), s2)
     assert e.value.code == A.ASD_EINVAL
+
+
+def test_site_field_pulse(gpu):
+    """Gaussian-in-time envelope on the site field (the config-4 pulse): plain form bit-exact."""
+    s = LT.sc_ferromagnet(5)
+    s.site_field = np.random.default_rng(5).normal(size=(s.nspins, 3)) * 20.0
+    amp, t0, sig, dt = 0.8, 20e-16, 8e-16, 1e-16
+    S0 = LT.random_spins(s.nspins, 2)
+    o = O.Oracle(s, dt=dt)
+    o.set_site_scale(0.5)
+    o.set_pulse(amp, t0, sig, dt)
+    o.set_spins(S0)
+    o.step(40)
+    for prec, tol in ((A.FP64_PLAIN, 0.0), (A.FP32, 1e-5)):
+        with A.Handle(A.RunParams(precision=prec, dt=dt, flags=A.FLAG_COMPENSATED if prec == A.FP32 else 0), s) as h:
+            h.set_spins(S0)
+            h.set_site_field_scale(0.5)
+            h.set_site_field_pulse(amp, t0, sig)
+            h.step(40)
+            assert maxdiff(h.get_spins(), o.spins()) <= tol, (prec, maxdiff(h.get_spins(), o.spins()))
+
+
+def test_magnetisation_stats_running_welford(gpu):
+    """Device RunningStat of |m_s| (sim::MvT) against a host Welford over the oracle trajectory."""
+    reps = [LT.sc_ferromagnet(4, T=50.0, stream=0), LT.sc_ferromagnet(5, T=150.0, stream=1)]
+    S = np.concatenate([LT.random_spins(r.nspins, 3 + k) for k, r in enumerate(reps)])
+    o = O.Oracle(reps, seed=4)
+    o.set_spins(S)
+    n = np.zeros(2); mean = np.zeros(2); m2 = np.zeros(2); prev = np.zeros(2)
+    with A.Handle(A.RunParams(precision=A.FP64_PLAIN, seed=4), reps) as h:
+        h.set_spins(S)
+        for k in range(25):
+            h.step(2)
+            h.sample_magnetisation()
+            o.step(2)
+            x = np.linalg.norm(o.magnetisation()[:, 0, :], axis=1)
+            n += 1
+            prev = mean.copy()
+            d = x - mean
+            mean = mean + d / n
+            m2 = m2 + d * (x - mean)
+        st = h.magnetisation_stats()[:, 0, :]
+        assert np.array_equal(st[:, 0], n)
+        assert np.allclose(st[:, 1], mean, rtol=1e-12, atol=0)
+        assert np.allclose(st[:, 2], m2 / (n - 1), rtol=1e-9, atol=1e-18)
+        assert np.allclose(st[:, 3], prev, rtol=1e-12, atol=0)
+        h.reset_magnetisation_stats()
+        assert np.all(h.magnetisation_stats() == 0)
+
+
+def _sq_host(S, sub, uo, mesh, xyz, kp, qaxis):
+    a, b = (1, 2) if qaxis == 0 else ((0, 2) if qaxis == 1 else (0, 1))
+    g = np.zeros(mesh, dtype=np.complex128)
+    g[xyz[:, 0], xyz[:, 1], xyz[:, 2]] = S[:, a] * uo[sub, a] + 1j * S[:, b] * uo[sub, b]
+    return np.fft.fftn(g)[kp[:, 0], kp[:, 1], kp[:, 2]]
+
+
+@pytest.mark.parametrize("prec", [A.FP64_PLAIN, A.FP32, A.FP64_FUSED])
+def test_sq_sampler_matches_fftn(gpu, prec):
+    """S(q,t) series: psi_k of psi = uo_a S_a + i uo_b S_b on the mesh, forward transform (FFTW sign)."""
+    rng = np.random.default_rng(11)
+    cases = [(LT.sc_ferromagnet((6, 5, 4), T=200.0), (6, 5, 4), 2, None),
+             (LT.bct2_antiferromagnet(3, T=50.0), (6, 3, 3), 0, np.array([[1.0, 1, 1], [-1, -1, 1]]))]
+    for s, mesh, qaxis, uo in cases:
+        n = s.nspins
+        xyz = np.stack(np.unravel_index(rng.permutation(np.prod(mesh))[:n], mesh), axis=1).astype(np.uint32)
+        kp = np.stack(np.unravel_index(rng.choice(np.prod(mesh), 9, replace=False), mesh), axis=1).astype(np.uint32)
+        atom = np.arange(n) % len(s.materials) if s.atom is None else np.asarray(s.atom)
+        sub = np.array([s.materials[m].sublattice for m in atom])
+        u = np.ones((int(sub.max()) + 1, 3)) if uo is None else uo
+        flags = A.FLAG_COMPENSATED if prec == A.FP32 else 0
+        with A.Handle(A.RunParams(precision=prec, flags=flags), s) as h:
+            h.set_spins(LT.random_spins(n, 4))
+            h.sq_setup(mesh, xyz, kp, max_samples=4, qaxis=qaxis, uo=uo)
+            want = []
+            for _ in range(3):
+                h.step(5)
+                h.sq_sample()
+                want.append(_sq_host(h.get_spins(), sub, u, mesh, xyz, kp, qaxis))
+            got = h.sq_series()
+            assert got.shape == (3, 9)
+            tol = 1e-12 if prec != A.FP32 else 1e-5
+            assert np.abs(got - np.array(want)).max() <= tol * np.sqrt(n)
+            h.sq_sample()
+            with pytest.raises(A.AsdError):
+                h.sq_sample()      # series full
