@@ -42,6 +42,8 @@ EXPORTED = [
     "asd_thermal_normals", "asd_build_csr", "asd_csr_to_dia", "asd_build_dipole_nr", "asd_fold_exchange_nr",
     "asd_set_site_field_pulse", "asd_sample_magnetisation", "asd_magnetisation_stats",
     "asd_reset_magnetisation_stats", "asd_sq_setup", "asd_sq_sample", "asd_sq_get",
+    "asd_sq_spectrum", "asd_tuning", "asd_set_launch_shape",
+    "asd_time_kernels_cold", "asd_time_steps_cold",
 ]
 
 
@@ -123,6 +125,12 @@ def load_library(path: str = LIB_PATH):
         "asd_sq_setup": ([P, C.c_uint32, dp, u32p, u32p, C.c_uint32, u32p, C.c_uint32], C.c_int),
         "asd_sq_sample": ([P], C.c_int),
         "asd_sq_get": ([P, dp, C.c_size_t, u32p], C.c_int),
+        "asd_tuning": ([P, C.c_char_p, C.c_size_t], C.c_int),
+        "asd_time_kernels_cold": ([P, C.c_uint64, C.c_uint64], C.c_int),
+        "asd_time_steps_cold": ([P, C.c_uint64, C.c_uint64, dp, C.POINTER(C.c_uint64)], C.c_int),
+        "asd_set_launch_shape": ([P, C.c_uint32, C.c_uint32], C.c_int),
+        "asd_sq_spectrum": ([P, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                             dp, dp, C.c_size_t, u32p, u32p], C.c_int),
         "asd_build_csr": ([u32p, C.POINTER(C.c_int), C.c_uint32, dp, C.c_uint32, u32p, u32p, i32p, dp, C.c_double,
                            u32p, u32p, dp, u32p], C.c_int),
         "asd_csr_to_dia": ([C.c_uint32, u32p, u32p, dp, C.c_uint32, i32p, dp, u32p], C.c_int),
@@ -373,6 +381,28 @@ class Handle:
         v = out[: ns.value * self._sq_nk * 2].reshape(ns.value, self._sq_nk, 2)
         return v[..., 0] + 1j * v[..., 1]
 
+    def sq_spectrum(self, window=0, alpha=0.54, beta=0.46, width_hz=1.0, sample_dt=1.0, fcut_lo=-np.inf,
+                    fcut_hi=np.inf):
+        """DSF of the recorded series: raw and smoothed one-sided PSD [nk, ns/2] and the peak bins."""
+        ns = self.sq_series().shape[0]
+        half = ns // 2
+        raw = np.empty(self._sq_nk * half)
+        sm = np.empty(self._sq_nk * half)
+        pr = np.empty(self._sq_nk, dtype=np.uint32)
+        ps = np.empty(self._sq_nk, dtype=np.uint32)
+        _check(load_library().asd_sq_spectrum(self.h, window, alpha, beta, width_hz, sample_dt, fcut_lo, fcut_hi,
+                                              _p(raw, C.c_double), _p(sm, C.c_double), len(raw),
+                                              _p(pr, C.c_uint32), _p(ps, C.c_uint32)), self.h)
+        return raw.reshape(self._sq_nk, half), sm.reshape(self._sq_nk, half), pr, ps
+
+    def tuning(self) -> str:
+        buf = C.create_string_buffer(512)
+        _check(load_library().asd_tuning(self.h, buf, len(buf)), self.h)
+        return buf.value.decode()
+
+    def set_launch_shape(self, block: int, staging: bool):
+        _check(load_library().asd_set_launch_shape(self.h, block, int(staging)), self.h)
+
     def magnetisation(self):
         out = np.empty(self.nrep * self.nsub * 3, dtype=np.float64)
         _check(load_library().asd_magnetisation(self.h, _p(out, C.c_double), len(out)), self.h)
@@ -384,9 +414,16 @@ class Handle:
         _check(load_library().asd_time_steps(self.h, n, C.byref(ms), C.byref(l)), self.h)
         return ms.value, l.value
 
-    def time_kernels(self, n: int):
+    def time_steps_cold(self, n: int, flush_bytes: int = 256 << 20):
+        """Device ms summed over n steps, each after an untimed L2 flush; and kernel launches."""
+        ms = C.c_double()
+        l = C.c_uint64()
+        _check(load_library().asd_time_steps_cold(self.h, n, flush_bytes, C.byref(ms), C.byref(l)), self.h)
+        return ms.value, l.value
+
+    def time_kernels(self, n: int, flush_bytes: int = 0):
         lib = load_library()
-        _check(lib.asd_time_kernels(self.h, n), self.h)
+        _check(lib.asd_time_kernels_cold(self.h, n, flush_bytes), self.h)
         name = C.create_string_buffer(128)
         avg, cnt, b = C.c_double(), C.c_uint64(), C.c_double()
         _check(lib.asd_kernel_stats(self.h, name, 128, C.byref(avg), C.byref(cnt), C.byref(b)), self.h)

@@ -66,6 +66,7 @@ void free_all(asd_handle* h) {
         F(h->sd[c]); F(h->esd[c]); F(h->fnd[c]); F(h->detd[c]); F(h->stagd[c]);
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
+    F(h->d_err);
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
     F(h->sell.typed); F(h->sell.tab_f); F(h->sell.tab_d);
     F(h->dia.off); F(h->dia.valf); F(h->dia.vald); F(h->dia.dtype); F(h->dia.tab_f); F(h->dia.tab_d);
@@ -148,6 +149,7 @@ void build_sell(asd_handle* h, const std::vector<uint32_t>& xadj, const std::vec
     h->sell.nslices = ns;
     h->sell.entries = E;
     h->sell.slice_ptr = dupload(sp.data(), sp.size());
+    h->h_slice_ptr = sp;
     auto value = [&](uint32_t k, int q) {
         if (q == 8 && zz_yy) q = 4;
         return val9[9 * (size_t)k + q];
@@ -314,6 +316,62 @@ void scatter_if_needed(asd_handle* h) {
     if (h->lr.mode == ASD_LR_NONE || h->p.precision == ASD_FP64_PLAIN || h->lr_scattered) return;
     CK(launch_lr_scatter_f32(h, h->sf));
     h->lr_scattered = true;
+}
+
+// Largest count of typed words that a block of B threads stages: its B/32 consecutive slices.
+uint32_t stage_capacity(const asd_handle* h, int B) {
+    const std::vector<uint32_t>& sp = h->h_slice_ptr;
+    if (sp.size() < 2) return 0;
+    const uint32_t ns = (uint32_t)sp.size() - 1, spb = (uint32_t)B / 32;
+    uint32_t m = 0;
+    for (uint32_t s0 = 0; s0 < ns; s0 += spb) m = std::max(m, sp[std::min(s0 + spb, ns)] - sp[s0]);
+    return m;
+}
+
+// Shared memory a block may spend on the tensor table plus the staged words (keeps at least
+// two blocks per SM).
+constexpr size_t STAGE_SMEM_MAX = 96 * 1024;
+
+// Launch shape of the fused stage kernel: block size and whether typed SELL words are staged.
+void configure_stage(asd_handle* h, int B, bool stage) {
+    h->block = B;
+    h->sell.stage = 0;
+    h->sell.stage_words = 0;
+    if (!stage || !h->sell.typed || h->exch != ASD_EXCH_CSR) return;
+    const size_t rb = h->p.precision == ASD_FP32 ? 4 : 8;
+    const size_t tab = ((rb * (h->full ? 12 : 4) * h->sell.ntypes) + 15) & ~(size_t)15;
+    const uint32_t w = stage_capacity(h, B);
+    if (w == 0 || tab + 4 * (size_t)w > STAGE_SMEM_MAX) return;
+    h->sell.stage = 1;
+    h->sell.stage_words = w;
+}
+
+// Project autotuner: time the first stage kind of the step (it writes only scratch buffers)
+// for every block size in {64, 128, 256} with and without staging, keep the fastest.
+void autotune(asd_handle* h) {
+    struct Cand { int B; bool stage; };
+    std::vector<Cand> cs;
+    for (int B : {64, 128, 256}) {
+        cs.push_back({B, false});
+        if (h->sell.typed && h->exch == ASD_EXCH_CSR) cs.push_back({B, true});
+    }
+    double best = 1e300;
+    Cand bc{256, true};
+    std::string log;
+    char buf[96];
+    for (const Cand& cd : cs) {
+        configure_stage(h, cd.B, cd.stage);
+        if (cd.stage && !h->sell.stage) continue;
+        float ms = 0.f;
+        CK(time_first_stage(h, 2, 8, &ms));
+        std::snprintf(buf, sizeof buf, "%sB=%d/%s:%.4f", log.empty() ? "" : " ", cd.B, cd.stage ? "stage" : "direct",
+                      (double)ms);
+        log += buf;
+        if (ms < best) { best = ms; bc = cd; }
+    }
+    configure_stage(h, bc.B, bc.stage);
+    std::snprintf(buf, sizeof buf, "block=%d staging=%s; ", h->block, h->sell.stage ? "bulk" : "off");
+    h->tune = std::string(buf) + "ms per stage launch: " + log;
 }
 
 void destroy_graph(asd_handle* h) {
@@ -703,7 +761,16 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         }
         CK(cudaEventCreate(&h->kev[0]));
         CK(cudaEventCreate(&h->kev[1]));
+        h->d_err = dalloc<uint32_t>(1);
+        h->sell.err = h->d_err;
         if (!plain) {
+            if (p.flags & ASD_FLAG_AUTOTUNE) autotune(h);
+            else configure_stage(h, 256, true);
+            if (h->tune.empty()) {
+                char b[64];
+                std::snprintf(b, sizeof b, "block=%d staging=%s (default)", h->block, h->sell.stage ? "bulk" : "off");
+                h->tune = b;
+            }
             const uint32_t upd = p.update;
             uint32_t G = 32;
             if (s0.lr == ASD_LR_DIPOLE) G = upd * std::max<uint32_t>(1, 32 / upd);
@@ -822,7 +889,39 @@ int asd_set_step(asd_handle* h, uint64_t t) {
 
 int asd_sync(asd_handle* h) {
     if (!h) return ASD_EINVAL;
-    try { CK(cudaSetDevice(h->device)); CK(cudaStreamSynchronize(h->stream)); } catch (const Fail& f) { return fail(h, f); }
+    try {
+        CK(cudaSetDevice(h->device));
+        CK(cudaStreamSynchronize(h->stream));
+        uint32_t e = 0;
+        if (h->d_err) CK(cudaMemcpy(&e, h->d_err, sizeof e, cudaMemcpyDeviceToHost));
+        if (e & 1u) {
+            CK(cudaMemset(h->d_err, 0, sizeof(uint32_t)));
+            throw Fail{ASD_ETIMEOUT, "a stage kernel's shared-memory staging wait ran out; those blocks read the "
+                                     "exchange words from global memory instead (results unaffected)"};
+        }
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_set_launch_shape(asd_handle* h, uint32_t block, uint32_t staging) {
+    if (!h) return ASD_EINVAL;
+    try {
+        REQUIRE(block == 64 || block == 128 || block == 256, "block must be 64, 128 or 256");
+        if (h->p.precision == ASD_FP64_PLAIN) return ASD_OK;
+        CK(cudaSetDevice(h->device));
+        CK(cudaStreamSynchronize(h->stream));
+        configure_stage(h, (int)block, staging != 0);
+        char b[64];
+        std::snprintf(b, sizeof b, "block=%d staging=%s (set)", h->block, h->sell.stage ? "bulk" : "off");
+        h->tune = b;
+        if (h->graph_steps) build_graph(h, h->graph_steps);
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_tuning(const asd_handle* h, char* out, size_t out_len) {
+    if (!h || !out || out_len == 0) return ASD_EINVAL;
+    std::snprintf(out, out_len, "%s", h->tune.c_str());
     return ASD_OK;
 }
 
@@ -1017,6 +1116,40 @@ int asd_sq_get(asd_handle* h, double* out, size_t out_len, uint32_t* nsamples) {
     return ASD_OK;
 }
 
+int asd_sq_spectrum(asd_handle* h, uint32_t window, double alpha, double beta, double width_hz, double sample_dt,
+                    double fcut_lo, double fcut_hi, double* raw, double* smooth, size_t len, uint32_t* peak_raw,
+                    uint32_t* peak_smooth) {
+    if (!h) return ASD_EINVAL;
+    double* d = nullptr;
+    uint32_t* dp = nullptr;
+    try {
+        if (!h->sq.on) throw Fail{ASD_ESTATE, "asd_sq_setup has not been called"};
+        const uint32_t ns = h->sq.nsamples, nk = h->sq.nk, half = ns / 2;
+        REQUIRE(ns >= 2, "the spectrum needs at least 2 samples");
+        REQUIRE(window <= 1, "window must be 0 (none) or 1 (generalised Hamming)");
+        REQUIRE(sample_dt > 0.0 && std::isfinite(sample_dt) && std::isfinite(width_hz), "sample_dt, width_hz");
+        const double pw = width_hz * (double)ns * sample_dt + 0.5;
+        REQUIRE(pw >= 1.0 && pw < 4294967296.0, "the Gaussian width rounds to less than one bin");
+        const size_t m = (size_t)nk * half;
+        REQUIRE(!(raw || smooth) || len >= m, "raw/smooth must hold nk*(nsamples/2) doubles");
+        CK(cudaSetDevice(h->device));
+        d = dalloc<double>(2 * m);
+        dp = dalloc<uint32_t>(2 * (size_t)nk);
+        CK(launch_sq_spectrum(h, (int)window, alpha, beta, (uint32_t)pw, sample_dt, fcut_lo, fcut_hi, d, d + m, dp));
+        if (raw) CK(cudaMemcpy(raw, d, m * sizeof(double), cudaMemcpyDeviceToHost));
+        if (smooth) CK(cudaMemcpy(smooth, d + m, m * sizeof(double), cudaMemcpyDeviceToHost));
+        if (peak_raw) CK(cudaMemcpy(peak_raw, dp, nk * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        if (peak_smooth) CK(cudaMemcpy(peak_smooth, dp + nk, nk * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    } catch (const Fail& f) {
+        if (d) cudaFree(d);
+        if (dp) cudaFree(dp);
+        return fail(h, f);
+    }
+    cudaFree(d);
+    cudaFree(dp);
+    return ASD_OK;
+}
+
 int asd_reset_magnetisation_stats(asd_handle* h) {
     if (!h) return ASD_EINVAL;
     try {
@@ -1063,20 +1196,71 @@ int asd_time_steps(asd_handle* h, uint64_t nsteps, double* ms, uint64_t* launche
     return ASD_OK;
 }
 
-int asd_time_kernels(asd_handle* h, uint64_t nsteps) {
+int asd_time_kernels(asd_handle* h, uint64_t nsteps) { return asd_time_kernels_cold(h, nsteps, 0); }
+
+int asd_time_kernels_cold(asd_handle* h, uint64_t nsteps, uint64_t flush_bytes) {
     if (!h) return ASD_EINVAL;
     try {
         CK(cudaSetDevice(h->device));
         CK(cudaStreamSynchronize(h->stream));
         h->ktimer = KernelTimer{};
+        if (flush_bytes) {
+            CK(cudaMalloc(&h->flush_buf, flush_bytes));
+            h->flush_bytes = flush_bytes;
+        }
         h->timing = true;
         const uint32_t G = h->graph_steps;
         h->graph_steps = 0;  // direct launches so each stage kernel is bracketed by events
-        try { run_steps(h, nsteps); } catch (...) { h->timing = false; h->graph_steps = G; throw; }
-        h->graph_steps = G;
-        h->timing = false;
-        CK(cudaStreamSynchronize(h->stream));
+        auto restore = [&]() {
+            h->timing = false;
+            h->graph_steps = G;
+            cudaStreamSynchronize(h->stream);
+            if (h->flush_buf) cudaFree(h->flush_buf);
+            h->flush_buf = nullptr;
+            h->flush_bytes = 0;
+        };
+        try { run_steps(h, nsteps); } catch (...) { restore(); throw; }
+        restore();
+        CK(cudaGetLastError());
     } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_time_steps_cold(asd_handle* h, uint64_t nsteps, uint64_t flush_bytes, double* ms, uint64_t* launches) {
+    if (!h || !ms || flush_bytes == 0) return ASD_EINVAL;
+    void* buf = nullptr;
+    std::vector<cudaEvent_t> ev;
+    try {
+        CK(cudaSetDevice(h->device));
+        CK(cudaStreamSynchronize(h->stream));
+        CK(cudaMalloc(&buf, flush_bytes));
+        ev.assign(2 * nsteps, nullptr);
+        for (auto& e : ev) CK(cudaEventCreate(&e));
+        const uint64_t l0 = h->launches;
+        for (uint64_t q = 0; q < nsteps; q++) {
+            // the flush is enqueued first and runs longer than the host takes to enqueue the
+            // step, so the events bracket device time of the step alone
+            CK(cudaMemsetAsync(buf, (int)(q & 0xFF), flush_bytes, h->stream));
+            CK(cudaEventRecord(ev[2 * q], h->stream));
+            run_steps(h, 1);
+            CK(cudaEventRecord(ev[2 * q + 1], h->stream));
+        }
+        CK(cudaStreamSynchronize(h->stream));
+        double tot = 0.0;
+        for (uint64_t q = 0; q < nsteps; q++) {
+            float f = 0.f;
+            CK(cudaEventElapsedTime(&f, ev[2 * q], ev[2 * q + 1]));
+            tot += f;
+        }
+        *ms = tot;
+        if (launches) *launches = h->launches - l0;
+    } catch (const Fail& f) {
+        for (auto e : ev) if (e) cudaEventDestroy(e);
+        if (buf) cudaFree(buf);
+        return fail(h, f);
+    }
+    for (auto e : ev) cudaEventDestroy(e);
+    cudaFree(buf);
     return ASD_OK;
 }
 

@@ -114,26 +114,37 @@ template <typename R, int EX, bool FULL, bool COMP>
 __global__ void __launch_bounds__(256, MinBlocks<R>::value)
     stage_kernel(const StepConst c, const SellDev sell, const DiaDev dia, const StageArgs<R> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t stage_bar;
     R* tab = reinterpret_cast<R*>(smem_raw);
+    const uint32_t* staged = nullptr;
+    uint32_t wbase = 0;
     if constexpr (EX == ASD_EXCH_CSR) {
-        if (sell.typed) load_table<R>(table_of<R>(sell), table_stride<FULL>() *sell.ntypes, tab);
+        if (sell.typed) {
+            if (sell.stage) {
+                // this block's slices are contiguous in the SELL stream: one bulk copy into
+                // shared memory behind the tensor table, overlapped with the noise draw below
+                const uint32_t tb = (uint32_t)(sizeof(R) * table_stride<FULL>() * sell.ntypes + 15u) & ~15u;
+                const uint32_t spb = blockDim.x >> 5;
+                const uint32_t s0 = blockIdx.x * spb, s1 = min(s0 + spb, sell.nslices);
+                wbase = __ldg(sell.slice_ptr + s0);
+                const uint32_t bytes = (__ldg(sell.slice_ptr + s1) - wbase) * 4u;
+                if (bytes) {
+                    uint32_t* wbuf = reinterpret_cast<uint32_t*>(smem_raw + tb);
+                    if (threadIdx.x == 0) mbar_init(&stage_bar, 1);
+                    __syncthreads();
+                    if (threadIdx.x == 0) bulk_stage(wbuf, sell.typed + wbase, bytes, &stage_bar);
+                    staged = wbuf;
+                }
+            }
+            load_table<R>(table_of<R>(sell), table_stride<FULL>() * sell.ntypes, tab);
+        }
     }
     if constexpr (EX == ASD_EXCH_DIA) {
         if (dia.dtype) load_table<R>(table_of<R>(dia), table_stride<FULL>() *dia.ntypes, tab);
     }
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= c.n) return;
+    if (i >= c.n) return;     // thread 0 of every block has i < n and always waits below
     const uint64_t t = *c.step_base + a.rel;
-    R h[3] = {R(0), R(0), R(0)};
-    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, a.src, tab, h);
-    if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, a.src, tab, h);
-    uint32_t midx = 0;
-    if (a.lr.hr || a.lr.mr) midx = __ldg(a.lr.idx + i);
-    if (a.lr.hr) {
-        h[0] += (R)(__ldg(a.lr.hr + midx) * a.lr.inv_p);
-        h[1] += (R)(__ldg(a.lr.hr + a.lr.P + midx) * a.lr.inv_p);
-        h[2] += (R)(__ldg(a.lr.hr + 2 * a.lr.P + midx) * a.lr.inv_p);
-    }
     const uint32_t at = atom_of(c, i);
     const MatConst& mc = c.mat[at];
     const uint32_t r = replica_of(c, i);
@@ -155,6 +166,23 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
             const double tp = sqrtT * mc.sigma;
             lrn[0] = xi[0] * tp; lrn[1] = xi[1] * tp; lrn[2] = xi[2] * tp;
         }
+    }
+    bool stage_timeout = false;
+    if (staged && !mbar_wait_bounded(&stage_bar, STAGE_WAIT_POLLS)) {
+        // the copy did not land in time: record it and read the words from global memory
+        atomicOr(sell.err, ERR_STAGE_TIMEOUT);
+        staged = nullptr;
+        stage_timeout = true;
+    }
+    R h[3] = {R(0), R(0), R(0)};
+    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, a.src, tab, h, staged, wbase);
+    if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, a.src, tab, h);
+    uint32_t midx = 0;
+    if (a.lr.hr || a.lr.mr) midx = __ldg(a.lr.idx + i);
+    if (a.lr.hr) {
+        h[0] += (R)(__ldg(a.lr.hr + midx) * a.lr.inv_p);
+        h[1] += (R)(__ldg(a.lr.hr + a.lr.P + midx) * a.lr.inv_p);
+        h[2] += (R)(__ldg(a.lr.hr + 2 * a.lr.P + midx) * a.lr.inv_p);
     }
     const double* dyn = c.dyn;
     const R* dynr;
@@ -261,6 +289,8 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
         a.lr.mr[a.lr.P + midx] = (float)out[1] * wv;
         a.lr.mr[2 * a.lr.P + midx] = (float)out[2] * wv;
     }
+    // a block must not retire while its bulk copy may still be writing shared memory
+    if (stage_timeout) mbar_wait_bounded(&stage_bar, STAGE_WAIT_POLLS);
 }
 
 __global__ void advance_k(uint64_t* step, uint32_t n) { *step += n; }
@@ -304,9 +334,24 @@ cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
     const int B = hd->block;
     const unsigned grid = (hd->n + B - 1) / B;
     size_t smem = 0;
-    if (EX == ASD_EXCH_CSR && hd->sell.typed) smem = sizeof(R) * table_stride<FULL>() *hd->sell.ntypes;
+    if (EX == ASD_EXCH_CSR && hd->sell.typed) {
+        smem = sizeof(R) * table_stride<FULL>() * hd->sell.ntypes;
+        if (hd->sell.stage) smem = ((smem + 15) & ~(size_t)15) + 4 * (size_t)hd->sell.stage_words;
+    }
     if (EX == ASD_EXCH_DIA && hd->dia.dtype) smem = sizeof(R) * table_stride<FULL>() *hd->dia.ntypes;
-    if (hd->timing) cudaEventRecord(hd->kev[0], hd->stream);
+    if (smem > 48 * 1024) {
+        static size_t opted = 48 * 1024;   // per instantiation: raise the dynamic shared-memory cap once
+        if (smem > opted) {
+            const cudaError_t e = cudaFuncSetAttribute(stage_kernel<R, EX, FULL, COMP>,
+                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            opted = smem;
+        }
+    }
+    if (hd->timing) {
+        if (hd->flush_buf) cudaMemsetAsync(hd->flush_buf, 0, hd->flush_bytes, hd->stream);
+        cudaEventRecord(hd->kev[0], hd->stream);
+    }
     stage_kernel<R, EX, FULL, COMP><<<grid, B, smem, hd->stream>>>(hd->sc, hd->sell, hd->dia, a);
     hd->launches += 1;
     if (hd->timing) {
@@ -415,6 +460,48 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
 }
 
 }  // namespace
+
+template <typename R>
+cudaError_t time_first_stage_t(asd_handle* h, int warm, int reps, float* ms) {
+    R* const* s; R* const* es; R* const* fn; R* const* det; R* const* stag;
+    state_ptrs<R>(h, &s, &es, &fn, &det, &stag);
+    const bool comp = sizeof(R) == 4 && (h->p.flags & ASD_FLAG_COMPENSATED);
+    StageArgs<R> a{};
+    a.base = c3<R>(s);
+    a.src = c3<R>(s);
+    a.out = v3<R>(es);
+    a.fn = v3<R>(fn);
+    if (stag[0]) a.stag = c3<R>(stag);
+    a.lr.P = h->lr.P; a.lr.idx = h->lr.mesh_idx; a.lr.w = h->lr.w;
+    if (h->p.integrator == ASD_HEUN) {
+        a.kind = 1;
+    } else {
+        a.kind = 10;
+        a.nst = h->p.integrator == ASD_RK4 ? 4 : 6;
+        for (int q = 0; q < 6; q++) {
+            if constexpr (sizeof(R) == 4) a.k[q] = v3<R>(h->kf[q]); else a.k[q] = v3<R>(h->kd[q]);
+        }
+    }
+    auto run = [&]() { return comp ? launch_stage<R, true>(h, a) : launch_stage<R, false>(h, a); };
+    cudaError_t e = cudaSuccess;
+    for (int q = 0; q < warm && e == cudaSuccess; q++) e = run();
+    if (e != cudaSuccess) return e;
+    cudaEventRecord(h->kev[0], h->stream);
+    for (int q = 0; q < reps && e == cudaSuccess; q++) e = run();
+    cudaEventRecord(h->kev[1], h->stream);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaEventSynchronize(h->kev[1])) != cudaSuccess) return e;
+    float t = 0.f;
+    if ((e = cudaEventElapsedTime(&t, h->kev[0], h->kev[1])) != cudaSuccess) return e;
+    *ms = t / (float)reps;
+    h->launches -= (uint64_t)(warm + reps);   // tuning launches are not step launches
+    return cudaSuccess;
+}
+
+cudaError_t time_first_stage(asd_handle* h, int warm, int reps, float* ms) {
+    if (h->p.precision == ASD_FP32) return time_first_stage_t<float>(h, warm, reps, ms);
+    return time_first_stage_t<double>(h, warm, reps, ms);
+}
 
 cudaError_t launch_fused_step(asd_handle* h, uint32_t rel, bool) {
     if (h->p.precision == ASD_FP32) return fused_step_t<float>(h, rel);

@@ -21,6 +21,47 @@ struct CVec3 { const R* p[3]; };
 template <typename T>
 __device__ __forceinline__ T ldcs(const T* p) { return __ldcs(p); }
 
+// ---- bulk (TMA) staging of a block's typed SELL words into shared memory
+// One thread arms an mbarrier with the byte count and issues one cp.async.bulk global->shared
+// copy (16-byte aligned source, destination and size); every thread later waits on the
+// barrier's phase 0 with a bounded number of try_wait polls.
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void bulk_stage(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    uint64_t policy;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for phase 0: false after `limit` polls (each poll may suspend the warp briefly).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t limit) {
+    for (uint32_t it = 0; it < limit; it++)
+        if (mbar_try_wait(bar, 0)) return true;
+    return false;
+}
+constexpr uint32_t STAGE_WAIT_POLLS = 1u << 22;
+constexpr uint32_t ERR_STAGE_TIMEOUT = 1u;
+
 // Copy the tensor table (ncomp x ntypes) into shared memory; all threads of the block take part.
 template <typename R>
 __device__ __forceinline__ void load_table(const R* __restrict__ tab, uint32_t count, R* smem) {
@@ -72,9 +113,22 @@ __device__ __forceinline__ void accumulate_typed(const R* tab, uint32_t t, R x, 
 
 // h += sum over the row's entries of J_e S_col(e), SELL-32 layout (one warp per slice).
 template <typename R, bool FULL>
-__device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const CVec3<R>& s, const R* tab, R h[3]) {
+__device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const CVec3<R>& s, const R* tab, R h[3],
+                                            const uint32_t* staged = nullptr, uint32_t wbase = 0) {
     const uint32_t sl = i >> 5, lane = i & 31u;
     const uint32_t p0 = __ldg(m.slice_ptr + sl), p1 = __ldg(m.slice_ptr + sl + 1);
+    if (m.typed && staged) {
+        // this block's words are in shared memory, indexed from the block's first entry
+        const uint32_t mask = (1u << m.colbits) - 1u, cb = m.colbits;
+#pragma unroll 4
+        for (uint32_t e = p0 - wbase + lane; e < p1 - wbase; e += 32) {
+            const uint32_t w = staged[e];
+            const uint32_t j = w & mask, t = w >> cb;
+            const R x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
+            accumulate_typed<R, FULL>(tab, t, x, y, z, h);
+        }
+        return;
+    }
     if (m.typed) {
         const uint32_t mask = (1u << m.colbits) - 1u, cb = m.colbits;
 #pragma unroll 4

@@ -29,6 +29,10 @@ struct SellDev {
     uint32_t colbits = 0, ntypes = 0;
     float* tab_f = nullptr;
     double* tab_d = nullptr;
+    // bulk staging of each block's typed words in shared memory (stage != 0); stage_words is
+    // the largest block's word count at the launch block size; err collects device error bits
+    uint32_t stage = 0, stage_words = 0;
+    uint32_t* err = nullptr;
 };
 
 // Row-aligned DIA, values component-major val[c][d*N+row], c = 3 (diag) or 9;
@@ -135,6 +139,9 @@ struct asd_handle {
     double* d_inv_count = nullptr;
     uint32_t* d_sub_of_atom = nullptr;
     uint64_t graph_launches = 0;
+    std::vector<uint32_t> h_slice_ptr;   // SELL slice offsets (host copy, for staging capacity)
+    uint32_t* d_err = nullptr;           // device error bits (staging wait timeouts)
+    std::string tune;                    // autotuner result, "B=.. stage=.. (ms ...)"
     bool lr_scattered = false;
     double nnz_per_row = 0.0;
     // site-field ramp value and time envelope (host copies; the plain form ramps from the host)
@@ -149,6 +156,8 @@ struct asd_handle {
     int block = 256;
     // timing of the dominant kernel
     bool timing = false;
+    void* flush_buf = nullptr;           // written before each timed stage launch (cold L2)
+    size_t flush_bytes = 0;
     asd::KernelTimer ktimer;
     cudaEvent_t kev[2] = {nullptr, nullptr};
 };
@@ -167,7 +176,11 @@ cudaError_t launch_plain_ramp(asd_handle* h, double rv);
 cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v);
 cudaError_t launch_set_scalar_f(asd_handle* h, float* dst, float v);
 cudaError_t launch_mag_push(asd_handle* h);
+cudaError_t time_first_stage(asd_handle* h, int warm, int reps, float* ms);
 cudaError_t launch_sq_sample(asd_handle* h);
+cudaError_t launch_sq_spectrum(asd_handle* h, int window, double alpha, double beta, uint32_t pixelwidth,
+                               double sample_dt, double flo, double fhi, double* d_raw, double* d_smooth,
+                               uint32_t* d_peaks);
 cudaError_t launch_magnetisation(asd_handle* h);
 cudaError_t launch_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, double* d_out,
                                    cudaStream_t st);

@@ -204,6 +204,19 @@ int asd_sq_setup(asd_handle* h, uint32_t qaxis, const double* uo, const uint32_t
 int asd_sq_sample(asd_handle* h);
 /* Copy the recorded series out: out[(sample*nk + k)*2 + {re, im}]; *nsamples = samples recorded. */
 int asd_sq_get(asd_handle* h, double* out, size_t out_len, uint32_t* nsamples);
+/* Dynamic structure factor of the recorded series, per k-point, on the device: replaces the
+ * time-series analysis tool fourier_space_analysis/src/timeseries.cpp:142-275.
+ *   window 0: none; 1: generalised Hamming alpha - beta cos(2 pi t / (ns - 1))   (:185-189)
+ *   forward FFT in time, divided by mesh points x ns                             (:143, :124, :198-203)
+ *   one-sided PSD raw[w] = |X(w)|^2 + |X(ns - 1 - w)|^2, w < ns/2                (:225-235)
+ *   smooth = Alvarez-Mazorra recursive Gaussian of raw, 10 passes,
+ *            width round(width_hz * ns * sample_dt) bins                         (:153, :237, :289-325)
+ *   peaks: argmax of smooth (w >= 0) and of raw (w > 1) with fcut_lo < w 2 pi / (ns sample_dt) < fcut_hi (:242-256)
+ * raw and smooth are [nk][ns/2] (either may be NULL); peak_raw / peak_smooth are [nk] bin indices
+ * (0 when no bin qualifies).  ASD_EINVAL when fewer than 2 samples or the width rounds to 0 bins. */
+int asd_sq_spectrum(asd_handle* h, uint32_t window, double alpha, double beta, double width_hz, double sample_dt,
+                    double fcut_lo, double fcut_hi, double* raw, double* smooth, size_t len, uint32_t* peak_raw,
+                    uint32_t* peak_smooth);
 /* Number of sublattices (GetNMS) of the handle. */
 int asd_num_sublattices(const asd_handle* h, uint32_t* nsub);
 
@@ -214,10 +227,23 @@ int asd_time_steps(asd_handle* h, uint64_t nsteps, double* ms, uint64_t* launche
  * launch with CUDA events on the handle's stream; results via asd_kernel_stats.
  * Measurement aid with no reference counterpart. */
 int asd_time_kernels(asd_handle* h, uint64_t nsteps);
+/* As asd_time_kernels, with a device buffer of flush_bytes written before every timed launch so
+ * each launch starts with a cold L2 (flush_bytes > L2 size). */
+int asd_time_kernels_cold(asd_handle* h, uint64_t nsteps, uint64_t flush_bytes);
+/* Device time of nsteps steps, each preceded by an untimed write of flush_bytes (> L2 size) and
+ * bracketed by its own CUDA events; *ms = sum over the steps.  Measurement aid. */
+int asd_time_steps_cold(asd_handle* h, uint64_t nsteps, uint64_t flush_bytes, double* ms, uint64_t* launches);
 /* Per-kernel device time of the fused stage kernel in the last asd_time_kernels:
  * average ms per launch, launch count and algorithmic bytes per launch. */
 int asd_kernel_stats(const asd_handle* h, char* name, size_t name_len, double* avg_ms, uint64_t* count,
                      double* bytes_per_launch);
+/* Launch shape of the fused stage kernel chosen at create (block size, shared-memory staging of
+ * the typed exchange words) and, with ASD_FLAG_AUTOTUNE, the autotuner's timings. */
+int asd_tuning(const asd_handle* h, char* out, size_t out_len);
+/* Set the fused stage kernel's launch shape by hand: block in {64, 128, 256}; staging 1 stages
+ * each block's typed exchange words in shared memory by bulk copy (ignored where the layout
+ * is not typed SELL or the words do not fit).  Results do not depend on the shape. */
+int asd_set_launch_shape(asd_handle* h, uint32_t block, uint32_t staging);
 
 /* The thermal normals the step uses for (seed, stream, step): 3 per spin for spins
  * [0, nspins), computed by the device generator (Philox4x32-10 + Box-Muller). */

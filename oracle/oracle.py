@@ -355,3 +355,66 @@ class RefLLGCPU:
         rc = self.L.refh_run(self.t, k)
         self.t += k
         return rc
+
+
+def sq_psi_k(S, sub, uo, mesh, mesh_xyz, kpoints, qaxis=2):
+    """psi_k of one sample: psi = uo_a S_a + i uo_b S_b on the mesh (a, b transverse to the
+    quantisation axis), forward 3D FFT (FFTW sign), values at the k-points
+    (src/timeseries.cpp:280-314)."""
+    a, b = (1, 2) if qaxis == 0 else ((0, 2) if qaxis == 1 else (0, 1))
+    uo = np.asarray(uo, dtype=np.float64)
+    xyz = np.asarray(mesh_xyz, dtype=np.int64)
+    kp = np.asarray(kpoints, dtype=np.int64)
+    g = np.zeros(tuple(mesh), dtype=np.complex128)
+    g[xyz[:, 0], xyz[:, 1], xyz[:, 2]] = S[:, a] * uo[sub, a] + 1j * (S[:, b] * uo[sub, b])
+    return np.fft.fftn(g)[kp[:, 0], kp[:, 1], kp[:, 2]]
+
+
+def gaussian_iir(x, sigma, nsteps=10):
+    """Recursive Gaussian of Alvarez and Mazorra (SIAM J. Numer. Anal. 31, 590, 1994) as the
+    time-series tool applies it (fourier_space_analysis/src/timeseries.cpp:289-325)."""
+    d = np.array(x, dtype=np.float64)
+    n = len(d)
+    lam = (sigma * sigma) / (2.0 * nsteps)
+    nu = (1.0 + 2.0 * lam - np.sqrt(1.0 + 4.0 * lam)) / (2.0 * lam)
+    bscale = 1.0 / (1.0 - nu)
+    post = (nu / lam) ** nsteps
+    for _ in range(nsteps):
+        d[0] *= bscale
+        for i in range(1, n):
+            d[i] += nu * d[i - 1]
+        d[n - 1] *= bscale
+        for i in range(n - 1, 0, -1):
+            d[i - 1] += nu * d[i]
+    return d * post
+
+
+def sq_spectrum(series, mesh_points, window=0, alpha=0.54, beta=0.46, width_hz=1.0, sample_dt=1.0,
+                fcut_lo=-np.inf, fcut_hi=np.inf):
+    """Per-k-point DSF of a psi_k(t) series [ns, nk] (fourier_space_analysis/src/timeseries.cpp:142-275):
+    optional generalised Hamming window, forward FFT in time divided by mesh_points*ns, one-sided
+    PSD pairing w with ns-1-w, Gaussian smoothing of round(width*ns*dt) bins, peak search inside
+    the frequency cut (raw peak from w > 1).  Returns raw, smooth [nk, ns/2], peak_raw, peak_smooth."""
+    ns, nk = series.shape
+    x = np.array(series, dtype=np.complex128)
+    if window == 1:
+        t = np.arange(ns, dtype=np.float64)
+        x = x * (alpha - beta * np.cos(2.0 * np.pi * t / (ns - 1.0)))[:, None]
+    X = np.fft.fft(x, axis=0) / (float(mesh_points) * ns)
+    half = ns // 2
+    w = np.arange(half)
+    raw = (np.abs(X[w]) ** 2 + np.abs(X[ns - 1 - w]) ** 2).T
+    pw = int(width_hz * ns * sample_dt + 0.5)
+    smooth = np.stack([gaussian_iir(r, float(pw)) for r in raw])
+    f = w * 2.0 * np.pi / (ns * sample_dt)
+    inside = (f > fcut_lo) & (f < fcut_hi)
+    pr = np.zeros(nk, dtype=np.uint32)
+    ps = np.zeros(nk, dtype=np.uint32)
+    for k in range(nk):
+        mr = ms = 0.0
+        for i in range(half):
+            if smooth[k, i] > ms and inside[i]:
+                ms, ps[k] = smooth[k, i], i
+            if raw[k, i] > mr and i > 1 and inside[i]:
+                mr, pr[k] = raw[k, i], i
+    return raw, smooth, pr, ps

@@ -317,13 +317,6 @@ def test_magnetisation_stats_running_welford(gpu):
         assert np.all(h.magnetisation_stats() == 0)
 
 
-def _sq_host(S, sub, uo, mesh, xyz, kp, qaxis):
-    a, b = (1, 2) if qaxis == 0 else ((0, 2) if qaxis == 1 else (0, 1))
-    g = np.zeros(mesh, dtype=np.complex128)
-    g[xyz[:, 0], xyz[:, 1], xyz[:, 2]] = S[:, a] * uo[sub, a] + 1j * S[:, b] * uo[sub, b]
-    return np.fft.fftn(g)[kp[:, 0], kp[:, 1], kp[:, 2]]
-
-
 @pytest.mark.parametrize("prec", [A.FP64_PLAIN, A.FP32, A.FP64_FUSED])
 def test_sq_sampler_matches_fftn(gpu, prec):
     """S(q,t) series: psi_k of psi = uo_a S_a + i uo_b S_b on the mesh, forward transform (FFTW sign)."""
@@ -345,7 +338,7 @@ def test_sq_sampler_matches_fftn(gpu, prec):
             for _ in range(3):
                 h.step(5)
                 h.sq_sample()
-                want.append(_sq_host(h.get_spins(), sub, u, mesh, xyz, kp, qaxis))
+                want.append(O.sq_psi_k(h.get_spins(), sub, u, mesh, xyz, kp, qaxis))
             got = h.sq_series()
             assert got.shape == (3, 9)
             tol = 1e-12 if prec != A.FP32 else 1e-5
@@ -353,3 +346,75 @@ def test_sq_sampler_matches_fftn(gpu, prec):
             h.sq_sample()
             with pytest.raises(A.AsdError):
                 h.sq_sample()      # series full
+
+
+def test_dsf_peaks_fp32_match_fp64_oracle(gpu):
+    """Spin-wave film (J1+J2 DIA, RK4, Gaussian-in-time x sinc-in-space pulse): the DSF computed on
+    the device equals the time-series restatement applied to the device series, the FP64 plain
+    series equals the oracle trajectory's, and the FP32 run finds the same peak bins."""
+    s = LT.film_dia(16, 16, 4, dipole=False)
+    n, dt, every, ns = s.nspins, 5e-16, 10, 256
+    mesh, xyz = (16, 16, 4), LT.sc_mesh_xyz((16, 16, 4))
+    kp = np.array([[2, 0, 0], [4, 0, 0], [6, 0, 0], [3, 3, 0], [0, 5, 1]], dtype=np.uint32)
+    sub = np.zeros(n, dtype=np.int64)
+    uo = np.ones((1, 3))
+    S0 = np.tile([0.0, 0.0, 1.0], (n, 1))
+    amp, t0, sig = 0.1, 20 * dt, 5 * dt
+    sdt = every * dt
+    spec = dict(window=0, width_hz=1.0 / (ns * sdt), sample_dt=sdt, fcut_lo=1e12, fcut_hi=1e15)
+    o = O.Oracle(s, integrator=A.RK4, dt=dt)
+    o.set_pulse(amp, t0, sig, dt)
+    o.set_spins(S0)
+    want = []
+    for _ in range(ns):
+        o.step(every)
+        want.append(O.sq_psi_k(o.spins(), sub, uo, mesh, xyz, kp))
+    want = np.array(want)
+    _, _, pr_o, ps_o = O.sq_spectrum(want, np.prod(mesh), **spec)
+    for prec in (A.FP64_PLAIN, A.FP32):
+        flags = A.FLAG_COMPENSATED if prec == A.FP32 else 0
+        with A.Handle(A.RunParams(integrator=A.RK4, precision=prec, dt=dt, flags=flags), s) as h:
+            h.set_spins(S0)
+            h.set_site_field_pulse(amp, t0, sig)
+            h.sq_setup(mesh, xyz, kp, max_samples=ns)
+            for _ in range(ns):
+                h.step(every)
+                h.sq_sample()
+            got = h.sq_series()
+            raw, sm, pr, ps = h.sq_spectrum(**spec)
+        r2, s2, pr2, ps2 = O.sq_spectrum(got, np.prod(mesh), **spec)
+        np.testing.assert_allclose(raw, r2, rtol=1e-9, atol=1e-300)
+        np.testing.assert_allclose(sm, s2, rtol=1e-9, atol=1e-300)
+        assert np.array_equal(pr, pr2) and np.array_equal(ps, ps2)
+        if prec == A.FP64_PLAIN:
+            assert np.abs(got - want).max() <= 1e-9 * np.sqrt(n)
+        assert np.array_equal(ps, ps_o), (prec, ps, ps_o)
+        assert np.array_equal(pr, pr_o), (prec, pr, pr_o)
+
+
+@pytest.mark.parametrize("prec", [A.FP32, A.FP64_FUSED])
+def test_launch_shapes_and_staging_bit_identical(gpu, prec):
+    """Every block size, with and without bulk staging of the typed SELL words, and the
+    autotuner's choice give bit-identical spins (each thread's arithmetic does not depend on
+    the shape); no staging wait runs out."""
+    s = LT.bct2_antiferromagnet(6, T=300.0)
+    S0 = LT.random_spins(s.nspins, 8)
+    flags = A.FLAG_COMPENSATED if prec == A.FP32 else 0
+    outs = []
+    for shape in [(256, True), (256, False), (128, True), (64, True), (64, False), None]:
+        f = flags | (A.FLAG_AUTOTUNE if shape is None else 0)
+        with A.Handle(A.RunParams(precision=prec, flags=f, seed=3), s) as h:
+            if shape is not None:
+                h.set_launch_shape(*shape)
+                assert ("staging=bulk" in h.tuning()) == shape[1], h.tuning()
+            else:
+                assert "ms per stage launch" in h.tuning(), h.tuning()
+            h.set_spins(S0)
+            h.step(70)
+            h.sync()
+            outs.append(h.get_spins())
+    for o in outs[1:]:
+        assert np.array_equal(o, outs[0])
+    g, o, _, _ = pair(s, 70, prec, flags=flags, seed=3, spins=S0)
+    assert np.array_equal(g, outs[0])
+    assert maxdiff(g, o) <= (1e-5 if prec == A.FP32 else 1e-10)

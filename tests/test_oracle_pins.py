@@ -2,6 +2,8 @@
 reference's own llgCPU compiled from source (tests/golden/make_golden.py),
 Philox known-answer vectors, and analytic single-spin dynamics."""
 import math
+import os
+import subprocess
 
 import numpy as np
 import pytest
@@ -130,3 +132,53 @@ def test_float_normals_statistics_and_closeness():
     assert d.max() < 2e-6 * max(1.0, np.abs(xd).max())
     v = xf.reshape(-1).astype(np.float64)
     assert abs(v.mean()) < 0.02 and abs(v.var() - 1.0) < 0.03
+
+
+TS_BIN = os.path.join(os.path.dirname(O.__file__), "_ref", "ref_timeseries")
+
+
+def _run_ref_timeseries(tmp, series, mesh, sample_dt, width, flo, fhi, hamm=None):
+    """Write the reference's k-series and info files, run its analysis tool, read kx*ky*kz*.dat."""
+    ns, nk = series.shape
+    kp = [(k, 0, 0) for k in range(nk)]
+    with open(os.path.join(tmp, "kvec.dat"), "w") as f:
+        for t in range(ns):
+            f.write(f"{t * sample_dt:.17g}\t" + "".join(f"{z.real:.17g}\t{z.imag:.17g}\t" for z in series[t]) + "\n")
+    with open(os.path.join(tmp, "info.in"), "w") as f:
+        f.write(f"file: kvec.dat\nsamples: {ns}\ndt: {sample_dt:.17g}\ndim: {mesh[0]} {mesh[1]} {mesh[2]}\n")
+        f.write(f"kdim: {mesh[0]} {mesh[1]} {mesh[2]}\nnk: {nk}\n")
+        for i, (a, b, c) in enumerate(kp):
+            f.write(f"k {i} : {a} {b} {c} x 0 x 0 0 0\n")
+    args = [TS_BIN, "info.in", repr(width), repr(flo), repr(fhi)]
+    if hamm is not None:
+        args += ["hamm", repr(hamm[0]), repr(hamm[1])]
+    subprocess.run(args, cwd=tmp, check=True, capture_output=True, timeout=120)
+    return [np.loadtxt(os.path.join(tmp, f"kx{a}ky{b}kz{c}.dat")) for a, b, c in kp]
+
+
+@pytest.mark.skipif(not os.path.exists(TS_BIN), reason="reference time-series tool not built")
+@pytest.mark.parametrize("hamm", [None, (0.54, 0.46)])
+def test_sq_spectrum_restatement_reproduces_reference_tool(tmp_path, hamm):
+    """oracle.sq_spectrum == fourier_space_analysis/src/timeseries.cpp run on the same series
+    (window, normalisation, w / ns-1-w pairing, recursive Gaussian, peak search); the tool prints
+    6 significant digits."""
+    rng = np.random.default_rng(9)
+    ns, nk, sdt, mesh = 256, 3, 2e-14, (8, 4, 2)
+    t = np.arange(ns) * sdt
+    freqs = np.array([3.0e12, 7.5e12, 1.2e13])          # rad/s
+    series = (np.exp(-1j * np.outer(t, freqs)) * np.array([5.0, 2.0, 1.0])
+              + 0.3 * (rng.normal(size=(ns, nk)) + 1j * rng.normal(size=(ns, nk))))
+    width, flo, fhi = 4.0e11, 1.0e11, 1.5e14
+    out = _run_ref_timeseries(str(tmp_path), series, mesh, sdt, width, flo, fhi, hamm)
+    win = 0 if hamm is None else 1
+    # the tool reads alpha from argv[5] (the word "hamm", so 0) and beta from argv[6]
+    # (fourier_space_analysis/src/timeseries.cpp:80-81): its window is -hamm[0] cos(2 pi t/(ns-1))
+    a, b = (0.54, 0.46) if hamm is None else (0.0, hamm[0])
+    raw, sm, pr, ps = O.sq_spectrum(series, np.prod(mesh), win, a, b, width, sdt, flo, fhi)
+    for k in range(nk):
+        ref = out[k]
+        assert ref.shape == (ns // 2, 5)
+        np.testing.assert_allclose(ref[:, 0], np.arange(ns // 2) * 2 * np.pi / (ns * sdt), rtol=1e-5)
+        np.testing.assert_allclose(ref[:, 1], raw[k], rtol=2e-5, atol=1e-30)
+        np.testing.assert_allclose(ref[:, 2], sm[k], rtol=2e-5, atol=1e-30)
+        assert ref[pr[k], 3] == 1.0 and ref[ps[k], 4] == 1.0
