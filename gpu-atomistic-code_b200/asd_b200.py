@@ -43,13 +43,20 @@ EXPORTED = [
     "asd_set_site_field_pulse", "asd_sample_magnetisation", "asd_magnetisation_stats",
     "asd_reset_magnetisation_stats", "asd_sq_setup", "asd_sq_sample", "asd_sq_get",
     "asd_sq_spectrum", "asd_tuning", "asd_set_launch_shape",
-    "asd_time_kernels_cold", "asd_time_steps_cold",
+    "asd_time_kernels_cold", "asd_time_steps_cold", "asd_read_ucf", "asd_read_exch", "asd_read_csr_exch",
+    "asd_write_csr_exch",
 ]
 
 
 class Material(C.Structure):
     _fields_ = [("mu", C.c_double), ("lambda_", C.c_double), ("gamma", C.c_double), ("k1u", C.c_double),
                 ("k1u_dir", C.c_double * 3), ("sublattice", C.c_uint32)]
+
+
+class UcfAtom(C.Structure):
+    _fields_ = [("sublattice", C.c_uint32), ("xred", C.c_double * 3), ("mesh_point", C.c_int32 * 3),
+                ("mu", C.c_double), ("damping", C.c_double), ("gamma", C.c_double), ("element", C.c_char * 16),
+                ("init_spin", C.c_double * 3), ("k1u", C.c_double), ("k1u_dir", C.c_double * 3)]
 
 
 class Params(C.Structure):
@@ -126,6 +133,13 @@ def load_library(path: str = LIB_PATH):
         "asd_sq_sample": ([P], C.c_int),
         "asd_sq_get": ([P, dp, C.c_size_t, u32p], C.c_int),
         "asd_tuning": ([P, C.c_char_p, C.c_size_t], C.c_int),
+        "asd_read_ucf": ([C.c_char_p, C.c_int, u32p, u32p, C.POINTER(UcfAtom), C.c_uint32, C.c_char_p, C.c_size_t],
+                         C.c_int),
+        "asd_read_exch": ([C.c_char_p, C.c_uint32, u32p, u32p, u32p, i32p, dp, C.c_uint32, C.c_char_p, C.c_size_t],
+                          C.c_int),
+        "asd_read_csr_exch": ([C.c_char_p, C.c_uint32, u32p, u32p, u32p, dp, C.c_uint32, C.c_char_p, C.c_size_t],
+                              C.c_int),
+        "asd_write_csr_exch": ([C.c_char_p, C.c_uint32, u32p, u32p, dp], C.c_int),
         "asd_time_kernels_cold": ([P, C.c_uint64, C.c_uint64], C.c_int),
         "asd_time_steps_cold": ([P, C.c_uint64, C.c_uint64, dp, C.POINTER(C.c_uint64)], C.c_int),
         "asd_set_launch_shape": ([P, C.c_uint32, C.c_uint32], C.c_int),
@@ -428,6 +442,65 @@ class Handle:
         avg, cnt, b = C.c_double(), C.c_uint64(), C.c_double()
         _check(lib.asd_kernel_stats(self.h, name, 128, C.byref(avg), C.byref(cnt), C.byref(b)), self.h)
         return {"name": name.value.decode(), "avg_ms": avg.value, "count": cnt.value, "bytes": b.value}
+
+
+def _read_check(rc: int, err):
+    if rc != ASD_OK:
+        raise AsdError(rc, err.value.decode(errors="replace"))
+
+
+def read_ucf(path: str, mesh_points: bool = False):
+    """Unit-cell file -> (nms, list of per-atom dicts) (geom::readGlobalGeom's .ucf block)."""
+    lib = load_library()
+    err = C.create_string_buffer(256)
+    nms, nauc = C.c_uint32(), C.c_uint32()
+    _read_check(lib.asd_read_ucf(path.encode(), int(mesh_points), C.byref(nms), C.byref(nauc), None, 0, err, 256), err)
+    atoms = (UcfAtom * nauc.value)()
+    _read_check(lib.asd_read_ucf(path.encode(), int(mesh_points), C.byref(nms), C.byref(nauc), atoms, nauc.value,
+                                 err, 256), err)
+    out = [{"sublattice": a.sublattice, "xred": tuple(a.xred), "mesh_point": tuple(a.mesh_point), "mu": a.mu,
+            "damping": a.damping, "gamma": a.gamma, "element": a.element.decode(), "init_spin": tuple(a.init_spin),
+            "k1u": a.k1u, "k1u_dir": tuple(a.k1u_dir)} for a in atoms]
+    return nms.value, out
+
+
+def read_exch(path: str, nms: int):
+    """Exchange file (libconfig syntax) -> bonds (s1, s2, cell offset (3,), J 3x3 [J]) in file order."""
+    lib = load_library()
+    err = C.create_string_buffer(256)
+    nb = C.c_uint32()
+    _read_check(lib.asd_read_exch(path.encode(), nms, C.byref(nb), None, None, None, None, 0, err, 256), err)
+    m = max(nb.value, 1)
+    s1 = np.zeros(m, dtype=np.uint32)
+    s2 = np.zeros(m, dtype=np.uint32)
+    v = np.zeros((m, 3), dtype=np.int32)
+    J = np.zeros((m, 9))
+    _read_check(lib.asd_read_exch(path.encode(), nms, C.byref(nb), _p(s1, C.c_uint32), _p(s2, C.c_uint32),
+                                  _p(v, C.c_int32), _p(J, C.c_double), m, err, 256), err)
+    k = nb.value
+    return s1[:k], s2[:k], v[:k], J[:k].reshape(k, 3, 3)
+
+
+def read_csr_exch(path: str, nspins: int):
+    """csr_exch_mat.dat -> xadj, adjncy, val9 (nnz x 9, diagonal filled)."""
+    lib = load_library()
+    err = C.create_string_buffer(256)
+    nnz = C.c_uint32()
+    _read_check(lib.asd_read_csr_exch(path.encode(), nspins, C.byref(nnz), None, None, None, 0, err, 256), err)
+    xadj = np.zeros(nspins + 1, dtype=np.uint32)
+    adj = np.zeros(nnz.value, dtype=np.uint32)
+    val = np.zeros((nnz.value, 9))
+    _read_check(lib.asd_read_csr_exch(path.encode(), nspins, C.byref(nnz), _p(xadj, C.c_uint32), _p(adj, C.c_uint32),
+                                      _p(val, C.c_double), nnz.value, err, 256), err)
+    return xadj, adj, val
+
+
+def write_csr_exch(path: str, xadj, adjncy, val9):
+    x = np.ascontiguousarray(xadj, dtype=np.uint32)
+    a = np.ascontiguousarray(adjncy, dtype=np.uint32)
+    v = np.ascontiguousarray(val9, dtype=np.float64)
+    _check(load_library().asd_write_csr_exch(path.encode(), len(x) - 1, _p(x, C.c_uint32), _p(a, C.c_uint32),
+                                             _p(v, C.c_double)))
 
 
 def thermal_normals(seed: int, stream: int, step: int, nspins: int) -> np.ndarray:

@@ -236,3 +236,23 @@ def replica_batch(nrep=96, edges=(16, 24, 32, 48, 64), seed=4, Tmax=None, Tc=Non
 def pulse_amplitude(t_s, amp=0.1, t0=2e-13, sigma=5e-14):
     """Gaussian-in-time envelope of the site-field pulse [T]."""
     return amp * math.exp(-0.5 * ((t_s - t0) / sigma) ** 2)
+
+
+def from_reference_inputs(ucf_path, exch_path, dim, pbc=(1, 1, 1), full=True, T=0.0, mesh_points=False):
+    """A SpinSystem from the reference's own input files: the unit-cell file (.ucf) and the
+    exchange file (.exch, unitcell method), on dim[0] x dim[1] x dim[2] cells.  Species and atoms
+    coincide as in the unitcell exchange method (src/exch_unitcell.cpp:296-401).  Returns the
+    system and the per-atom records (initial spins, positions)."""
+    nms, atoms = A.read_ucf(ucf_path, mesh_points)
+    if nms != len(atoms):
+        raise ValueError("the unitcell exchange method pairs species with unit-cell atoms: nms must equal nauc")
+    s1, s2, vec, J = A.read_exch(exch_path, nms)
+    mus = [a["mu"] for a in atoms]
+    xadj, adj, val = build_csr(dim, pbc, mus, s1, s2, vec, J.reshape(-1, 9))
+    mats = [A.MaterialSpec(mu=a["mu"], lam=a["damping"], gamma=a["gamma"], k1u=a["k1u"], k1u_dir=a["k1u_dir"],
+                           sublattice=a["sublattice"]) for a in atoms]
+    n = int(np.prod(dim)) * len(atoms)
+    s = A.SpinSystem(nspins=n, materials=mats, full=full, temperature=T, exch=A.EXCH_CSR, xadj=xadj, adjncy=adj,
+                     csr_val=val)
+    s.meta = {"dim": tuple(dim), "nnz": len(adj), "kind": "reference-inputs"}
+    return s, atoms

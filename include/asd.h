@@ -272,6 +272,40 @@ int asd_build_dipole_nr(const uint32_t dim[3], const uint32_t nk[3], const doubl
 int asd_fold_exchange_nr(const uint32_t mesh[3], uint32_t nshell, const int32_t* shell_vec,
                          const double* J9, double mu_muB, double* nr, uint32_t* count);
 
+/* ---- input files of the reference (no libconfig needed); messages go to err[err_len] ---- */
+/* One atom of a unit-cell (.ucf) file. */
+typedef struct asd_ucf_atom {
+    uint32_t sublattice;       /* magnetic species */
+    double xred[3];            /* reduced coordinates */
+    int32_t mesh_point[3];     /* position on the unit cell's k-mesh (only when mesh_points) */
+    double mu, damping, gamma; /* [muB], Gilbert damping, relative to 1.76e11 */
+    char element[16];
+    double init_spin[3];
+    double k1u;                /* [J] */
+    double k1u_dir[3];
+} asd_ucf_atom;
+/* .ucf reader, geom::readGlobalGeom (src/geom_glob.cpp:190-295): "nms nauc", then per atom
+ * "sl x y z [mx my mz] mu damping gamma element sx sy sz K1U dx dy dz" (mesh point present when
+ * the k-mesh is set, mesh_points != 0), with the reference's checks on mu, gamma, the K1U axis
+ * and per-species moments (src/unitcell.h:131-218).  atoms == NULL: counts only. */
+int asd_read_ucf(const char* path, int mesh_points, uint32_t* nms, uint32_t* nauc, asd_ucf_atom* atoms,
+                 uint32_t cap, char* err, size_t err_len);
+/* .exch reader for the unitcell method, exch::get_exch_unitcell
+ * (src/exch_determine_exchange_matrix.cpp:27-144): groups exchange_<s1>_<s2> with
+ * Num_Interactions, units and UnitCell<i> / J<i>_<row> arrays.  Bonds come out in file order
+ * per (s1, s2): species, cell offset rounded half away from zero (src/exch_unitcell.cpp:303-327),
+ * J in joules, 3x3 row-major.  bond arrays NULL: *nbonds only.  Feeds asd_build_csr. */
+int asd_read_exch(const char* path, uint32_t nms, uint32_t* nbonds, uint32_t* bond_s1, uint32_t* bond_s2,
+                  int32_t* bond_vec, double* bond_J, uint32_t cap, char* err, size_t err_len);
+/* csr_exch_mat.dat reader (src/exch.cpp:63-133): "N", "nnz", xadj[N+1], then per entry
+ * "col xx yy zz" [T]; val9 is nnz x 9 with only the diagonal filled.  xadj NULL: *nnz only. */
+int asd_read_csr_exch(const char* path, uint32_t nspins, uint32_t* nnz, uint32_t* xadj, uint32_t* adjncy,
+                      double* val9, uint32_t cap, char* err, size_t err_len);
+/* csr_exch_mat.dat writer in the layout src/exch_unitcell.cpp:36-63 writes (diagonal
+ * components; 17 significant digits where the reference prints 6). */
+int asd_write_csr_exch(const char* path, uint32_t nspins, const uint32_t* xadj, const uint32_t* adjncy,
+                       const double* val9);
+
 #ifdef __cplusplus
 }
 #endif

@@ -418,3 +418,67 @@ def sq_spectrum(series, mesh_points, window=0, alpha=0.54, beta=0.46, width_hz=1
             if raw[k, i] > mr and i > 1 and inside[i]:
                 mr, pr[k] = raw[k, i], i
     return raw, smooth, pr, ps
+
+
+REF_BUILDERS_SO = os.path.join(HERE, "_ref", "libref_builders.so")
+
+
+def _ref_builders():
+    if not os.path.exists(REF_BUILDERS_SO):
+        build()
+    L = C.CDLL(REF_BUILDERS_SO, mode=os.RTLD_LOCAL)
+    L.refb_exchunitcell.argtypes = [u32p, C.POINTER(C.c_int), C.c_uint, dp, u32p, C.c_uint, dp, dp, C.c_int,
+                                    u32p, u32p, u32p, dp, C.c_uint]
+    L.refb_csr_to_dia.argtypes = [C.c_uint, u32p, u32p, dp, C.c_int, u32p, i32p, dp, C.c_uint]
+    return L
+
+
+def ref_exchunitcell(dim, pbc, mus, bonds, offdiag=True):
+    """The reference's exch::exchunitcell (src/exch_unitcell.cpp:265-489) on bonds given as
+    (atom s1, atom s2, cell offset, 3x3 J [J]) in shell order per (s1, s2).  Returns xadj,
+    adjncy, val9 (J/(mu muB), nnz x 9; only xx, yy, zz unless offdiag)."""
+    L = _ref_builders()
+    nauc = len(mus)
+    per = {}
+    for s1, s2, v, Jm in bonds:
+        per.setdefault((s1, s2), []).append((v, np.asarray(Jm, dtype=np.float64).reshape(9)))
+    maxsh = max([len(x) for x in per.values()] + [1])
+    shells = np.zeros(nauc * nauc, dtype=np.uint32)
+    vec = np.zeros((nauc * nauc * maxsh, 3))
+    Jt = np.zeros((nauc * nauc * maxsh, 9))
+    for (s1, s2), lst in per.items():
+        shells[s1 * nauc + s2] = len(lst)
+        for k, (v, Jm) in enumerate(lst):
+            vec[(s1 * nauc + s2) * maxsh + k] = v
+            Jt[(s1 * nauc + s2) * maxsh + k] = Jm
+    d = au32(dim)
+    p = np.ascontiguousarray(pbc, dtype=np.int32)
+    m = a64(mus)
+    nnz = C.c_uint()
+    args = [_ptr(d, C.c_uint32), p.ctypes.data_as(C.POINTER(C.c_int)), nauc, _ptr(m, C.c_double),
+            _ptr(shells, C.c_uint32), maxsh, _ptr(vec, C.c_double), _ptr(Jt, C.c_double), int(offdiag)]
+    L.refb_exchunitcell(*args, C.byref(nnz), None, None, None, 0)
+    n = int(np.prod(dim)) * nauc
+    xadj = np.zeros(n + 1, dtype=np.uint32)
+    adj = np.zeros(max(nnz.value, 1), dtype=np.uint32)
+    val = np.zeros((max(nnz.value, 1), 9))
+    rc = L.refb_exchunitcell(*args, C.byref(nnz), _ptr(xadj, C.c_uint32), _ptr(adj, C.c_uint32),
+                             _ptr(val, C.c_double), len(adj))
+    assert rc == 0
+    return xadj, adj[: nnz.value], val[: nnz.value]
+
+
+def ref_csr_to_dia(n, xadj, adjncy, val9, offdiag=True):
+    """The reference's matconv::csr_to_dia_diag / _offdiag (src/matrix_conv.cpp:28-272).
+    Returns offsets and data [9, ndiag*n] (row-aligned, component-major)."""
+    L = _ref_builders()
+    x, a, v = au32(xadj), au32(adjncy), a64(val9)
+    nd = C.c_uint()
+    L.refb_csr_to_dia(n, _ptr(x, C.c_uint32), _ptr(a, C.c_uint32), _ptr(v, C.c_double), int(offdiag), C.byref(nd),
+                      None, None, 0)
+    off = np.zeros(nd.value, dtype=np.int32)
+    data = np.zeros(9 * nd.value * n)
+    rc = L.refb_csr_to_dia(n, _ptr(x, C.c_uint32), _ptr(a, C.c_uint32), _ptr(v, C.c_double), int(offdiag),
+                           C.byref(nd), _ptr(off, C.c_int32), _ptr(data, C.c_double), nd.value)
+    assert rc == 0
+    return off, data.reshape(9, nd.value * n)

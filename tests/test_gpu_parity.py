@@ -352,10 +352,13 @@ def test_dsf_peaks_fp32_match_fp64_oracle(gpu):
     """Spin-wave film (J1+J2 DIA, RK4, Gaussian-in-time x sinc-in-space pulse): the DSF computed on
     the device equals the time-series restatement applied to the device series, the FP64 plain
     series equals the oracle trajectory's, and the FP32 run finds the same peak bins."""
-    s = LT.film_dia(16, 16, 4, dipole=False)
-    n, dt, every, ns = s.nspins, 5e-16, 10, 256
-    mesh, xyz = (16, 16, 4), LT.sc_mesh_xyz((16, 16, 4))
-    kp = np.array([[2, 0, 0], [4, 0, 0], [6, 0, 0], [3, 3, 0], [0, 5, 1]], dtype=np.uint32)
+    # the sinc profile varies along x only, so the pulse excites the (k, 0, 0) magnons; the
+    # peak bins rise with k (the dispersion) and are separated from their neighbours by far
+    # more than the FP32 error
+    s = LT.film_dia(16, 16, 2, dipole=False, pulse_width_sites=2.0)
+    n, dt, every, ns = s.nspins, 5e-16, 20, 512
+    mesh, xyz = (16, 16, 2), LT.sc_mesh_xyz((16, 16, 2))
+    kp = np.array([[k, 0, 0] for k in range(1, 9)], dtype=np.uint32)
     sub = np.zeros(n, dtype=np.int64)
     uo = np.ones((1, 3))
     S0 = np.tile([0.0, 0.0, 1.0], (n, 1))
@@ -390,6 +393,7 @@ def test_dsf_peaks_fp32_match_fp64_oracle(gpu):
             assert np.abs(got - want).max() <= 1e-9 * np.sqrt(n)
         assert np.array_equal(ps, ps_o), (prec, ps, ps_o)
         assert np.array_equal(pr, pr_o), (prec, pr, pr_o)
+    assert np.all(np.diff(ps_o.astype(int)) >= 0) and ps_o[-1] > ps_o[0]
 
 
 @pytest.mark.parametrize("prec", [A.FP32, A.FP64_FUSED])
