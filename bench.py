@@ -223,6 +223,9 @@ def run_ours(args):
     flags = A.FLAG_COMPENSATED | A.FLAG_AUTOTUNE | (A.FLAG_STREAMED_EXCHANGE if streamed else 0)
     p32 = A.RunParams(precision=A.FP32, seed=1 + rank, flags=flags, **kw)
     h = A.Handle(p32, systems)
+    if args.launch_shape:
+        blk, stg = (int(x) for x in args.launch_shape.split(","))
+        h.set_launch_shape(blk, stg)
     h.set_spins(S0)
     h.step(args.warmup)
     h.sync()
@@ -264,6 +267,8 @@ def run_ours(args):
     # applied field (H2D) + step + magnetisation read-back (D2H), download spins
     nsub_out = h.nrep * h.nsub * 3
     he = A.Handle(p32, systems)
+    if args.launch_shape:
+        he.set_launch_shape(blk, stg)
     he.step(1)
     he.sync()
     barrier()
@@ -355,6 +360,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=1500)
     ap.add_argument("--err-steps", type=int, default=100)
+    ap.add_argument("--launch-shape", default="",
+                    help="block,staging for the fused stage kernel instead of the autotuner's choice "
+                         "(staging 0 none, 1 words, 2 words+spins)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

@@ -44,7 +44,7 @@ EXPORTED = [
     "asd_reset_magnetisation_stats", "asd_sq_setup", "asd_sq_sample", "asd_sq_get",
     "asd_sq_spectrum", "asd_tuning", "asd_set_launch_shape",
     "asd_time_kernels_cold", "asd_time_steps_cold", "asd_read_ucf", "asd_read_exch", "asd_read_csr_exch",
-    "asd_write_csr_exch",
+    "asd_write_csr_exch", "asd_plan_spin_spans",
 ]
 
 
@@ -140,6 +140,8 @@ def load_library(path: str = LIB_PATH):
         "asd_read_csr_exch": ([C.c_char_p, C.c_uint32, u32p, u32p, u32p, dp, C.c_uint32, C.c_char_p, C.c_size_t],
                               C.c_int),
         "asd_write_csr_exch": ([C.c_char_p, C.c_uint32, u32p, u32p, dp], C.c_int),
+        "asd_plan_spin_spans": ([C.c_uint32, C.c_uint32, u32p, u32p, C.c_uint32, C.c_uint32, C.c_uint32, u32p, u32p,
+                                 C.c_uint32, u32p, u32p, u32p], C.c_int),
         "asd_time_kernels_cold": ([P, C.c_uint64, C.c_uint64], C.c_int),
         "asd_time_steps_cold": ([P, C.c_uint64, C.c_uint64, dp, C.POINTER(C.c_uint64)], C.c_int),
         "asd_set_launch_shape": ([P, C.c_uint32, C.c_uint32], C.c_int),
@@ -414,7 +416,8 @@ class Handle:
         _check(load_library().asd_tuning(self.h, buf, len(buf)), self.h)
         return buf.value.decode()
 
-    def set_launch_shape(self, block: int, staging: bool):
+    def set_launch_shape(self, block: int, staging: int):
+        """staging 0: none, 1: typed words, 2: typed words and neighbour spins."""
         _check(load_library().asd_set_launch_shape(self.h, block, int(staging)), self.h)
 
     def magnetisation(self):

@@ -67,6 +67,7 @@ void free_all(asd_handle* h) {
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
     F(h->d_err);
+    F(h->sell.lwords); F(h->sell.span_ptr); F(h->sell.spans);
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
     F(h->sell.typed); F(h->sell.tab_f); F(h->sell.tab_d);
     F(h->dia.off); F(h->dia.valf); F(h->dia.vald); F(h->dia.dtype); F(h->dia.tab_f); F(h->dia.tab_d);
@@ -181,6 +182,7 @@ void build_sell(asd_handle* h, const std::vector<uint32_t>& xadj, const std::vec
                     }
             }
             h->sell.typed = dupload(w.data(), w.size());
+            h->h_words = std::move(w);
             h->sell.colbits = 32 - tb;
             h->sell.ntypes = tt.size();
             if (h->p.precision == ASD_FP32) {
@@ -329,48 +331,90 @@ uint32_t stage_capacity(const asd_handle* h, int B) {
 }
 
 // Shared memory a block may spend on the tensor table plus the staged words (keeps at least
-// two blocks per SM).
+// two blocks per SM), and on staged neighbour spins on top of that.
 constexpr size_t STAGE_SMEM_MAX = 96 * 1024;
 
-// Launch shape of the fused stage kernel: block size and whether typed SELL words are staged.
-void configure_stage(asd_handle* h, int B, bool stage) {
+void free_spin_stage(asd_handle* h) {
+    SellDev& m = h->sell;
+    if (m.lwords) cudaFree(m.lwords);
+    if (m.span_ptr) cudaFree(m.span_ptr);
+    if (m.spans) cudaFree(m.spans);
+    m.lwords = nullptr; m.span_ptr = nullptr; m.spans = nullptr;
+    m.spin_slots = 0; m.spin_block = 0;
+}
+
+// Neighbour-spin spans and local words for blocks of B rows (asd_plan_spin_spans); returns
+// false when no block can stage.
+bool build_spin_stage(asd_handle* h, int B) {
+    free_spin_stage(h);
+    const std::vector<uint32_t>& sp = h->h_slice_ptr;
+    const std::vector<uint32_t>& w = h->h_words;
+    if (sp.size() < 2 || w.empty()) return false;
+    const uint32_t rb = h->p.precision == ASD_FP32 ? 4 : 8;
+    const uint32_t ns = (uint32_t)sp.size() - 1, spb = (uint32_t)B / 32;
+    const uint32_t nblk = (ns + spb - 1) / spb;
+    std::vector<uint32_t> ptr(nblk + 1);
+    uint32_t nspans = 0, slots = 0;
+    if (asd_plan_spin_spans(h->n, ns, sp.data(), w.data(), h->sell.colbits, rb, (uint32_t)B, ptr.data(), nullptr, 0,
+                            nullptr, &nspans, &slots) != ASD_OK || nspans == 0)
+        return false;
+    std::vector<uint32_t> spans(4 * (size_t)nspans), lw(w.size());
+    if (asd_plan_spin_spans(h->n, ns, sp.data(), w.data(), h->sell.colbits, rb, (uint32_t)B, ptr.data(), spans.data(),
+                            nspans, lw.data(), &nspans, &slots) != ASD_OK)
+        return false;
+    SellDev& m = h->sell;
+    m.lwords = dupload(lw.data(), lw.size());
+    m.span_ptr = dupload(ptr.data(), ptr.size());
+    m.spans = reinterpret_cast<uint4*>(dupload(spans.data(), spans.size()));
+    m.spin_slots = slots;
+    m.spin_block = (uint32_t)B;
+    return true;
+}
+
+// Launch shape of the fused stage kernel: block size and the staging mode of typed SELL
+// words (0 none, 1 words, 2 words and neighbour spins).
+void configure_stage(asd_handle* h, int B, int mode) {
     h->block = B;
     h->sell.stage = 0;
     h->sell.stage_words = 0;
-    if (!stage || !h->sell.typed || h->exch != ASD_EXCH_CSR) return;
+    if (mode == 0 || !h->sell.typed || h->exch != ASD_EXCH_CSR) return;
     const size_t rb = h->p.precision == ASD_FP32 ? 4 : 8;
     const size_t tab = ((rb * (h->full ? 12 : 4) * h->sell.ntypes) + 15) & ~(size_t)15;
     const uint32_t w = stage_capacity(h, B);
     if (w == 0 || tab + 4 * (size_t)w > STAGE_SMEM_MAX) return;
     h->sell.stage = 1;
     h->sell.stage_words = w;
+    if (mode == 2) {
+        if (h->sell.spin_block != (uint32_t)B && !build_spin_stage(h, B)) return;
+        if (h->sell.spin_block == (uint32_t)B) h->sell.stage = 2;
+    }
 }
 
 // Project autotuner: time the first stage kind of the step (it writes only scratch buffers)
 // for every block size in {64, 128, 256} with and without staging, keep the fastest.
 void autotune(asd_handle* h) {
-    struct Cand { int B; bool stage; };
+    struct Cand { int B; int mode; };
+    static const char* names[3] = {"direct", "words", "words+spins"};
     std::vector<Cand> cs;
     for (int B : {64, 128, 256}) {
-        cs.push_back({B, false});
-        if (h->sell.typed && h->exch == ASD_EXCH_CSR) cs.push_back({B, true});
+        cs.push_back({B, 0});
+        if (h->sell.typed && h->exch == ASD_EXCH_CSR) { cs.push_back({B, 1}); cs.push_back({B, 2}); }
     }
     double best = 1e300;
-    Cand bc{256, true};
+    Cand bc{256, 1};
     std::string log;
     char buf[96];
     for (const Cand& cd : cs) {
-        configure_stage(h, cd.B, cd.stage);
-        if (cd.stage && !h->sell.stage) continue;
+        configure_stage(h, cd.B, cd.mode);
+        if ((int)h->sell.stage != cd.mode) continue;
         float ms = 0.f;
         CK(time_first_stage(h, 2, 8, &ms));
-        std::snprintf(buf, sizeof buf, "%sB=%d/%s:%.4f", log.empty() ? "" : " ", cd.B, cd.stage ? "stage" : "direct",
-                      (double)ms);
+        std::snprintf(buf, sizeof buf, "%sB=%d/%s:%.4f", log.empty() ? "" : " ", cd.B, names[cd.mode], (double)ms);
         log += buf;
         if (ms < best) { best = ms; bc = cd; }
     }
-    configure_stage(h, bc.B, bc.stage);
-    std::snprintf(buf, sizeof buf, "block=%d staging=%s; ", h->block, h->sell.stage ? "bulk" : "off");
+    configure_stage(h, bc.B, bc.mode);
+    std::snprintf(buf, sizeof buf, "block=%d staging=%s; ", h->block, names[h->sell.stage]);
     h->tune = std::string(buf) + "ms per stage launch: " + log;
 }
 
@@ -645,14 +689,18 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         } else {
             const size_t bytes = p.precision == ASD_FP32 ? 4 : 8;
             for (int c = 0; c < 3; c++) {
+                // gather sources carry SPIN_PAD zeroed elements so 16-byte-aligned span copies
+                // of neighbour spins stay inside the allocation
                 if (bytes == 4) {
-                    h->sf[c] = dalloc<float>(n); h->esf[c] = dalloc<float>(n); h->fnf[c] = dalloc<float>(n);
+                    h->sf[c] = dalloc<float>(n + SPIN_PAD); h->esf[c] = dalloc<float>(n + SPIN_PAD);
+                    h->fnf[c] = dalloc<float>(n + SPIN_PAD);
                     h->detf[c] = dalloc<float>(n);
                     if (p.flags & ASD_FLAG_COMPENSATED) h->sl[c] = dalloc<float>(n);
                     if (p.integrator != ASD_HEUN)
                         for (int q = 0; q < (p.integrator == ASD_RK4 ? 3 : 5); q++) h->kf[q][c] = dalloc<float>(n);
                 } else {
-                    h->sd[c] = dalloc<double>(n); h->esd[c] = dalloc<double>(n); h->fnd[c] = dalloc<double>(n);
+                    h->sd[c] = dalloc<double>(n + SPIN_PAD); h->esd[c] = dalloc<double>(n + SPIN_PAD);
+                    h->fnd[c] = dalloc<double>(n + SPIN_PAD);
                     h->detd[c] = dalloc<double>(n);
                     if (p.integrator != ASD_HEUN)
                         for (int q = 0; q < (p.integrator == ASD_RK4 ? 3 : 5); q++) h->kd[q][c] = dalloc<double>(n);
@@ -765,10 +813,11 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         h->sell.err = h->d_err;
         if (!plain) {
             if (p.flags & ASD_FLAG_AUTOTUNE) autotune(h);
-            else configure_stage(h, 256, true);
+            else configure_stage(h, 256, 1);
             if (h->tune.empty()) {
+                static const char* names[3] = {"direct", "words", "words+spins"};
                 char b[64];
-                std::snprintf(b, sizeof b, "block=%d staging=%s (default)", h->block, h->sell.stage ? "bulk" : "off");
+                std::snprintf(b, sizeof b, "block=%d staging=%s (default)", h->block, names[h->sell.stage]);
                 h->tune = b;
             }
             const uint32_t upd = p.update;
@@ -907,12 +956,14 @@ int asd_set_launch_shape(asd_handle* h, uint32_t block, uint32_t staging) {
     if (!h) return ASD_EINVAL;
     try {
         REQUIRE(block == 64 || block == 128 || block == 256, "block must be 64, 128 or 256");
+        REQUIRE(staging <= 2, "staging must be 0, 1 or 2");
         if (h->p.precision == ASD_FP64_PLAIN) return ASD_OK;
         CK(cudaSetDevice(h->device));
         CK(cudaStreamSynchronize(h->stream));
-        configure_stage(h, (int)block, staging != 0);
+        configure_stage(h, (int)block, (int)staging);
+        static const char* names[3] = {"direct", "words", "words+spins"};
         char b[64];
-        std::snprintf(b, sizeof b, "block=%d staging=%s (set)", h->block, h->sell.stage ? "bulk" : "off");
+        std::snprintf(b, sizeof b, "block=%d staging=%s (set)", h->block, names[h->sell.stage]);
         h->tune = b;
         if (h->graph_steps) build_graph(h, h->graph_steps);
     } catch (const Fail& f) { return fail(h, f); }

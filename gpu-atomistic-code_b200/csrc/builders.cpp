@@ -1,6 +1,7 @@
 // Set-up builders (host, FP64): bond list -> CSR, CSR -> row-aligned DIA,
 // point-dipole interaction matrix on the padded mesh, exchange fold.
 #include "../../include/asd.h"
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -167,3 +168,90 @@ int asd_fold_exchange_nr(const uint32_t mesh[3], uint32_t nshell, const int32_t*
 }
 
 }  // extern "C"
+
+// ---- neighbour-spin staging plan of the fused stage kernel
+namespace {
+constexpr uint32_t SPIN_SMEM_MAX = 64 * 1024;   // bytes of staged spins (3 components) per block
+constexpr uint32_t SPANS_MAX = 24;               // spans per block (one bulk copy per span and component)
+constexpr uint32_t SPAN_GAP = 32;                // columns closer than this share one span
+constexpr uint32_t SPIN_PAD_ELEMS = 8;           // zeroed elements after each spin array in the library
+}  // namespace
+
+int asd_plan_spin_spans(uint32_t n, uint32_t nslices, const uint32_t* slice_ptr, const uint32_t* words,
+                        uint32_t colbits, uint32_t elem_bytes, uint32_t block, uint32_t* span_ptr, uint32_t* spans,
+                        uint32_t spans_cap, uint32_t* local_words, uint32_t* nspans_out, uint32_t* slots_out) {
+    if (!slice_ptr || !words || !span_ptr || !nspans_out || !slots_out || n == 0 || nslices == 0) return ASD_EINVAL;
+    if ((elem_bytes != 4 && elem_bytes != 8) || block < 32 || block % 32 || colbits == 0 || colbits > 32)
+        return ASD_EINVAL;
+    if ((uint64_t)nslices * 32 < n || (uint64_t)nslices * 32 >= (uint64_t)n + 32) return ASD_EINVAL;
+    const bool fill = spans != nullptr;
+    if (fill && !local_words) return ASD_EINVAL;
+    const uint32_t align = 16 / elem_bytes;
+    const uint32_t slots_cap = (SPIN_SMEM_MAX / (3 * elem_bytes)) & ~(align - 1);
+    const uint32_t mask = colbits >= 32 ? 0xFFFFFFFFu : (1u << colbits) - 1u;
+    if (slots_cap > mask) return ASD_ENOTSUP;
+    const uint32_t spb = block / 32, nblk = (nslices + spb - 1) / spb;
+    const uint64_t limit = (uint64_t)n + SPIN_PAD_ELEMS;
+    std::vector<uint32_t> cols;
+    std::vector<uint32_t> bs;   // (start, len) pairs of the current block
+    uint32_t total_spans = 0, slots_max = 0;
+    span_ptr[0] = 0;
+    for (uint32_t b = 0; b < nblk; b++) {
+        const uint32_t e0 = slice_ptr[b * spb], e1 = slice_ptr[std::min((b + 1) * spb, nslices)];
+        if (e1 < e0) return ASD_EINVAL;
+        cols.clear();
+        for (uint32_t e = e0; e < e1; e++) {
+            const uint32_t c = words[e] & mask;
+            if (c >= n) return ASD_EINVAL;
+            cols.push_back(c);
+        }
+        std::sort(cols.begin(), cols.end());
+        cols.erase(std::unique(cols.begin(), cols.end()), cols.end());
+        bs.clear();
+        uint32_t total = 0;
+        bool fits = !cols.empty();
+        for (size_t q = 0; q < cols.size() && fits;) {
+            uint32_t hi = cols[q];
+            size_t r = q + 1;
+            while (r < cols.size() && cols[r] - hi <= SPAN_GAP) hi = cols[r++];
+            const uint32_t a0 = cols[q] & ~(align - 1);
+            // hi <= n-1, so the aligned end is at most n+align-1 < n+SPIN_PAD_ELEMS; checked all the same
+            const uint64_t a1 = ((uint64_t)hi + align) & ~(uint64_t)(align - 1);
+            if (a1 > limit) { fits = false; break; }
+            if (!bs.empty() && a0 < bs[bs.size() - 2] + bs.back()) {      // aligned spans touch: merge
+                const uint32_t end = std::max<uint32_t>(bs[bs.size() - 2] + bs.back(), (uint32_t)a1);
+                total += end - (bs[bs.size() - 2] + bs.back());
+                bs.back() = end - bs[bs.size() - 2];
+            } else {
+                bs.push_back(a0);
+                bs.push_back((uint32_t)(a1 - a0));
+                total += (uint32_t)(a1 - a0);
+            }
+            if (bs.size() / 2 > SPANS_MAX || total > slots_cap) fits = false;
+            q = r;
+        }
+        const uint32_t nb = fits ? (uint32_t)(bs.size() / 2) : 0;
+        if (fill) {
+            if (total_spans + nb > spans_cap) return ASD_EINVAL;
+            uint32_t off = 0;
+            for (uint32_t k = 0; k < nb; k++) {
+                uint32_t* t = spans + 4 * (size_t)(total_spans + k);
+                t[0] = bs[2 * k]; t[1] = bs[2 * k + 1]; t[2] = off; t[3] = 0;
+                off += bs[2 * k + 1];
+            }
+            for (uint32_t e = e0; e < e1; e++) {
+                if (!nb) { local_words[e] = words[e]; continue; }
+                const uint32_t c = words[e] & mask;
+                uint32_t k = 0, o = 0;
+                while (!(c >= bs[2 * k] && c < bs[2 * k] + bs[2 * k + 1])) { o += bs[2 * k + 1]; k++; }
+                local_words[e] = (o + (c - bs[2 * k])) | (words[e] & ~mask);
+            }
+        }
+        if (nb) slots_max = std::max(slots_max, total);
+        total_spans += nb;
+        span_ptr[b + 1] = total_spans;
+    }
+    *nspans_out = total_spans;
+    *slots_out = (slots_max + align - 1) & ~(align - 1);
+    return ASD_OK;
+}

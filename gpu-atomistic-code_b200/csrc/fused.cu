@@ -117,23 +117,49 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
     __shared__ __align__(8) uint64_t stage_bar;
     R* tab = reinterpret_cast<R*>(smem_raw);
     const uint32_t* staged = nullptr;
+    const R* sspin = nullptr;
     uint32_t wbase = 0;
     if constexpr (EX == ASD_EXCH_CSR) {
         if (sell.typed) {
             if (sell.stage) {
                 // this block's slices are contiguous in the SELL stream: one bulk copy into
-                // shared memory behind the tensor table, overlapped with the noise draw below
+                // shared memory behind the tensor table; with stage 2 also one copy per
+                // (neighbour-spin span, component); all overlap the noise draw below
                 const uint32_t tb = (uint32_t)(sizeof(R) * table_stride<FULL>() * sell.ntypes + 15u) & ~15u;
                 const uint32_t spb = blockDim.x >> 5;
                 const uint32_t s0 = blockIdx.x * spb, s1 = min(s0 + spb, sell.nslices);
                 wbase = __ldg(sell.slice_ptr + s0);
                 const uint32_t bytes = (__ldg(sell.slice_ptr + s1) - wbase) * 4u;
+                uint32_t sp0 = 0, nsp = 0;
+                if (sell.stage == 2) {
+                    sp0 = __ldg(sell.span_ptr + blockIdx.x);
+                    nsp = __ldg(sell.span_ptr + blockIdx.x + 1) - sp0;
+                }
                 if (bytes) {
                     uint32_t* wbuf = reinterpret_cast<uint32_t*>(smem_raw + tb);
+                    R* sbuf = reinterpret_cast<R*>(smem_raw + tb + 4u * sell.stage_words);
                     if (threadIdx.x == 0) mbar_init(&stage_bar, 1);
                     __syncthreads();
-                    if (threadIdx.x == 0) bulk_stage(wbuf, sell.typed + wbase, bytes, &stage_bar);
+                    if (threadIdx.x < 32) {
+                        if (threadIdx.x == 0) {
+                            uint32_t tx = bytes;
+                            for (uint32_t q = 0; q < nsp; q++) tx += 3u * sell.spans[sp0 + q].y * (uint32_t)sizeof(R);
+                            mbar_arrive_expect_tx(&stage_bar, tx);
+                        }
+                        __syncwarp();
+                        for (uint32_t k = threadIdx.x; k < 1 + 3 * nsp; k += 32) {
+                            if (k == 0) {
+                                bulk_copy_stream(wbuf, (nsp ? sell.lwords : sell.typed) + wbase, bytes, &stage_bar);
+                            } else {
+                                const uint4 sp = sell.spans[sp0 + (k - 1) / 3];
+                                const uint32_t c = (k - 1) % 3;
+                                bulk_copy(sbuf + c * sell.spin_slots + sp.z, a.src.p[c] + sp.x,
+                                          sp.y * (uint32_t)sizeof(R), &stage_bar);
+                            }
+                        }
+                    }
                     staged = wbuf;
+                    if (nsp) sspin = sbuf;
                 }
             }
             load_table<R>(table_of<R>(sell), table_stride<FULL>() * sell.ntypes, tab);
@@ -171,11 +197,12 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
     if (staged && !mbar_wait_bounded(&stage_bar, STAGE_WAIT_POLLS)) {
         // the copy did not land in time: record it and read the words from global memory
         atomicOr(sell.err, ERR_STAGE_TIMEOUT);
-        staged = nullptr;
+        staged = nullptr;      // the global words carry global columns
+        sspin = nullptr;
         stage_timeout = true;
     }
     R h[3] = {R(0), R(0), R(0)};
-    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, a.src, tab, h, staged, wbase);
+    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, a.src, tab, h, staged, wbase, sspin);
     if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, a.src, tab, h);
     uint32_t midx = 0;
     if (a.lr.hr || a.lr.mr) midx = __ldg(a.lr.idx + i);
@@ -337,6 +364,7 @@ cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
     if (EX == ASD_EXCH_CSR && hd->sell.typed) {
         smem = sizeof(R) * table_stride<FULL>() * hd->sell.ntypes;
         if (hd->sell.stage) smem = ((smem + 15) & ~(size_t)15) + 4 * (size_t)hd->sell.stage_words;
+        if (hd->sell.stage == 2) smem += 3 * sizeof(R) * (size_t)hd->sell.spin_slots;
     }
     if (EX == ASD_EXCH_DIA && hd->dia.dtype) smem = sizeof(R) * table_stride<FULL>() *hd->dia.ntypes;
     if (smem > 48 * 1024) {

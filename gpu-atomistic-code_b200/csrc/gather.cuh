@@ -32,15 +32,28 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-__device__ __forceinline__ void bulk_stage(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+// The one arrival of the barrier's phase, announcing the bytes all copies will deliver.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// Streamed data (read once per launch): evict-first in L2.
+__device__ __forceinline__ void bulk_copy_stream(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
     uint64_t policy;
     asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(policy));
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
     asm volatile(
         "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
             smem_addr(dst)),
         "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
         : "memory");
+}
+
+// Reused data (neighbour spins other blocks read too): default L2 policy.
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
@@ -114,9 +127,21 @@ __device__ __forceinline__ void accumulate_typed(const R* tab, uint32_t t, R x, 
 // h += sum over the row's entries of J_e S_col(e), SELL-32 layout (one warp per slice).
 template <typename R, bool FULL>
 __device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const CVec3<R>& s, const R* tab, R h[3],
-                                            const uint32_t* staged = nullptr, uint32_t wbase = 0) {
+                                            const uint32_t* staged = nullptr, uint32_t wbase = 0,
+                                            const R* sspin = nullptr) {
     const uint32_t sl = i >> 5, lane = i & 31u;
     const uint32_t p0 = __ldg(m.slice_ptr + sl), p1 = __ldg(m.slice_ptr + sl + 1);
+    if (m.typed && staged && sspin) {
+        // words carry block-local slots into the staged neighbour spins [3][spin_slots]
+        const uint32_t mask = (1u << m.colbits) - 1u, cb = m.colbits, ns = m.spin_slots;
+#pragma unroll 4
+        for (uint32_t e = p0 - wbase + lane; e < p1 - wbase; e += 32) {
+            const uint32_t w = staged[e];
+            const uint32_t j = w & mask, t = w >> cb;
+            accumulate_typed<R, FULL>(tab, t, sspin[j], sspin[ns + j], sspin[2 * ns + j], h);
+        }
+        return;
+    }
     if (m.typed && staged) {
         // this block's words are in shared memory, indexed from the block's first entry
         const uint32_t mask = (1u << m.colbits) - 1u, cb = m.colbits;

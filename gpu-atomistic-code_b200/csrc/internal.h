@@ -29,11 +29,21 @@ struct SellDev {
     uint32_t colbits = 0, ntypes = 0;
     float* tab_f = nullptr;
     double* tab_d = nullptr;
-    // bulk staging of each block's typed words in shared memory (stage != 0); stage_words is
-    // the largest block's word count at the launch block size; err collects device error bits
+    // bulk staging in shared memory at the launch block size: stage 1 copies each block's typed
+    // words, stage 2 also the neighbour spins its rows read (spin_block = block size the local
+    // words were built for); stage_words / spin_slots size the buffers; err collects device
+    // error bits
     uint32_t stage = 0, stage_words = 0;
     uint32_t* err = nullptr;
+    // neighbour-spin staging: per block, spans [start, start+len) of the spin arrays land at
+    // slot offset off in shared memory ([3][spin_slots] components); lwords are the typed words
+    // with the column replaced by the slot (blocks without spans keep global columns)
+    uint32_t* lwords = nullptr;
+    uint32_t* span_ptr = nullptr;
+    uint4* spans = nullptr;          // (start, len, off, 0) in elements
+    uint32_t spin_slots = 0, spin_block = 0;
 };
+constexpr uint32_t SPIN_PAD = 8;     // zeroed elements after every gather-source spin array
 
 // Row-aligned DIA, values component-major val[c][d*N+row], c = 3 (diag) or 9;
 // typed layout: one id byte per (diagonal, row), table [ncomp][ntypes].
@@ -140,6 +150,7 @@ struct asd_handle {
     uint32_t* d_sub_of_atom = nullptr;
     uint64_t graph_launches = 0;
     std::vector<uint32_t> h_slice_ptr;   // SELL slice offsets (host copy, for staging capacity)
+    std::vector<uint32_t> h_words;       // typed SELL words (host copy, for the local words)
     uint32_t* d_err = nullptr;           // device error bits (staging wait timeouts)
     std::string tune;                    // autotuner result, "B=.. stage=.. (ms ...)"
     bool lr_scattered = false;

@@ -241,8 +241,9 @@ int asd_kernel_stats(const asd_handle* h, char* name, size_t name_len, double* a
  * the typed exchange words) and, with ASD_FLAG_AUTOTUNE, the autotuner's timings. */
 int asd_tuning(const asd_handle* h, char* out, size_t out_len);
 /* Set the fused stage kernel's launch shape by hand: block in {64, 128, 256}; staging 1 stages
- * each block's typed exchange words in shared memory by bulk copy (ignored where the layout
- * is not typed SELL or the words do not fit).  Results do not depend on the shape. */
+ * each block's typed exchange words in shared memory by bulk copy, staging 2 also the spans of
+ * neighbour spins its rows read (each falls back to the lower mode where the layout is not
+ * typed SELL or the data do not fit).  Results do not depend on the shape. */
 int asd_set_launch_shape(asd_handle* h, uint32_t block, uint32_t staging);
 
 /* The thermal normals the step uses for (seed, stream, step): 3 per spin for spins
@@ -271,6 +272,18 @@ int asd_build_dipole_nr(const uint32_t dim[3], const uint32_t nk[3], const doubl
 /* exch::fft (src/exch_intmat.cpp:28-163): fold shell tensors into nr (+=); returns images in *count. */
 int asd_fold_exchange_nr(const uint32_t mesh[3], uint32_t nshell, const int32_t* shell_vec,
                          const double* J9, double mu_muB, double* nr, uint32_t* count);
+
+/* Neighbour-spin staging plan of the fused stage kernel (host only, no device needed).  For
+ * SELL-32 slices (nslices, slice_ptr[nslices+1]) of typed words (column in the low colbits bits)
+ * and blocks of `block` rows: each block's distinct columns are merged into spans (gaps of at
+ * most 32 joined), widened to 16-byte boundaries of elem_bytes-sized elements and given
+ * consecutive shared-memory slots.  A block whose spans exceed 24 or 64 KB of 3-component spins
+ * gets none and keeps global columns.  Outputs span_ptr[nblocks+1], spans[4*k] = (start, len,
+ * slot offset, 0), local_words[E] (column replaced by the slot), *nspans and *slots (largest
+ * block's slots).  spans == NULL: counts only (span_ptr still filled). */
+int asd_plan_spin_spans(uint32_t n, uint32_t nslices, const uint32_t* slice_ptr, const uint32_t* words,
+                        uint32_t colbits, uint32_t elem_bytes, uint32_t block, uint32_t* span_ptr, uint32_t* spans,
+                        uint32_t spans_cap, uint32_t* local_words, uint32_t* nspans, uint32_t* slots);
 
 /* ---- input files of the reference (no libconfig needed); messages go to err[err_len] ---- */
 /* One atom of a unit-cell (.ucf) file. */
