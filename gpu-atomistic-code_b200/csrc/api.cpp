@@ -70,6 +70,7 @@ void free_all(asd_handle* h) {
     F(h->sell.lwords); F(h->sell.span_ptr); F(h->sell.spans);
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
     F(h->sell.typed); F(h->sell.tab_f); F(h->sell.tab_d);
+    F(h->dia.tile_ptr); F(h->dia.tile_diag);
     F(h->dia.off); F(h->dia.valf); F(h->dia.vald); F(h->dia.dtype); F(h->dia.tab_f); F(h->dia.tab_d);
     F(h->p_s); F(h->p_es); F(h->p_fn); F(h->p_ch); F(h->p_hdemag); F(h->p_rand); F(h->p_det); F(h->p_hstg); F(h->p_hinit);
     for (int q = 0; q < 6; q++) F(h->p_k[q]);
@@ -713,6 +714,29 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
                 const size_t m = (size_t)s0.ndiag * n;
                 const int nc = h->full ? 9 : 3;
                 const int qmap3[3] = {0, 4, zz_yy ? 4 : 8};
+                {
+                    // active diagonals of every 32-row tile: a periodic lattice has many distinct
+                    // offsets, each row only a few nonzero ones
+                    const uint32_t nt = (n + 31) / 32;
+                    std::vector<uint32_t> tp(nt + 1, 0), td;
+                    const double* comp[9];
+                    for (int q = 0; q < nc; q++) comp[q] = dia_comp(h->full ? q : qmap3[q]);
+                    for (uint32_t w = 0; w < nt; w++) {
+                        const uint32_t r0 = 32 * w, r1 = std::min(n, r0 + 32);
+                        for (uint32_t d = 0; d < s0.ndiag; d++) {
+                            bool any = false;
+                            for (uint32_t r = r0; r < r1 && !any; r++) {
+                                const int64_t col = (int64_t)r + doff[d];
+                                if (col < 0 || col >= (int64_t)n) continue;
+                                for (int q = 0; q < nc && !any; q++) any = comp[q][(size_t)d * n + r] != 0.0;
+                            }
+                            if (any) td.push_back(d);
+                        }
+                        tp[w + 1] = (uint32_t)td.size();
+                    }
+                    h->dia.tile_ptr = dupload(tp.data(), tp.size());
+                    h->dia.tile_diag = dupload(td.data(), std::max<size_t>(td.size(), 1));
+                }
                 bool typed = false;
                 if (!(p.flags & ASD_FLAG_STREAMED_EXCHANGE)) {
                     // typed DIA: one id byte per (diagonal, row) into the distinct tensors

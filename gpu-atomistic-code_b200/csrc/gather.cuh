@@ -206,8 +206,11 @@ __device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const 
 template <typename R, bool FULL>
 __device__ __forceinline__ void gather_dia(const DiaDev& m, uint32_t n, uint32_t i, const CVec3<R>& s, const R* tab,
                                            R h[3]) {
+    // the warp walks its tile's active diagonals (warp-uniform list)
+    const uint32_t k0 = __ldg(m.tile_ptr + (i >> 5)), k1 = __ldg(m.tile_ptr + (i >> 5) + 1);
     if (m.dtype) {
-        for (uint32_t d = 0; d < m.ndiag; d++) {
+        for (uint32_t k = k0; k < k1; k++) {
+            const uint32_t d = __ldg(m.tile_diag + k);
             const int64_t col = (int64_t)i + __ldg(m.off + d);
             if (col < 0 || col >= (int64_t)n) continue;
             const uint32_t t = ldcs(m.dtype + (size_t)d * n + i);
@@ -220,7 +223,8 @@ __device__ __forceinline__ void gather_dia(const DiaDev& m, uint32_t n, uint32_t
     const size_t ND = (size_t)m.ndiag * n;
     const R* v;
     if constexpr (sizeof(R) == 4) v = m.valf; else v = m.vald;
-    for (uint32_t d = 0; d < m.ndiag; d++) {
+    for (uint32_t k = k0; k < k1; k++) {
+        const uint32_t d = __ldg(m.tile_diag + k);
         const int64_t col = (int64_t)i + __ldg(m.off + d);
         if (col < 0 || col >= (int64_t)n) continue;
         const size_t a = (size_t)d * n + i;

@@ -56,6 +56,10 @@ struct DiaDev {
     uint32_t ntypes = 0;
     float* tab_f = nullptr;
     double* tab_d = nullptr;
+    // per warp tile (32 rows): the diagonals with a nonzero entry in the tile's rows,
+    // tile_diag[tile_ptr[w] .. tile_ptr[w+1]) in ascending order
+    uint32_t* tile_ptr = nullptr;
+    uint32_t* tile_diag = nullptr;
 };
 
 // Reference-structured CSR / DIA for the FP64 plain form (separate component arrays).
