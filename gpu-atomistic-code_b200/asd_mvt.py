@@ -8,18 +8,21 @@ statistics on the device (asd_sample_magnetisation), and the host reads the stat
 every `check_every` samples to test convergence.
 
     python asd_mvt.py [--replicas 96] [--equil 20000] [--average 20000] [--update 100]
+    torchrun --nproc-per-node N asd_mvt.py ...   (temperatures split over N GPUs, rows gathered to rank 0)
 """
 from __future__ import annotations
 
 import argparse
 import json
 import math
+import os
 import time
 
 import numpy as np
 
 import asd_b200 as A
 import asd_lattice as LT
+import asd_replicas as R
 
 
 def run_mvt(reps, equil, average, update=100, convmean=1e-4, convvar=1e-4, precision=A.FP32, seed=1,
@@ -59,18 +62,36 @@ def main():
     ap.add_argument("--seed", type=int, default=4)
     args = ap.parse_args()
     reps, L, Ts = LT.replica_batch(args.replicas, seed=args.seed, Tmax=args.tmax)
+    # under torchrun each rank (one GPU) runs its share of the temperatures
+    dist = None
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = tdist
+    rank = dist.get_rank() if dist else 0
+    mine = R.shard([r.nspins for r in reps], rank, world)
     t0 = time.time()
-    mean, sem, cnt, steps = run_mvt(reps, args.equil, args.average, args.update, convmean=0.0, convvar=0.0)
-    wall = time.time() - t0
-    rows = [{"edge": int(l), "T_K": float(t), "m": float(mean[r, 0]), "sem": float(sem[r, 0]), "samples": int(cnt[r, 0])}
-            for r, (l, t) in enumerate(zip(L, Ts))]
+    mean, sem, cnt, steps = run_mvt([reps[g] for g in mine], args.equil, args.average, args.update, convmean=0.0,
+                                    convvar=0.0)
+    wall = R.allmax(time.time() - t0, dist)
+    part = [{"edge": int(L[g]), "T_K": float(Ts[g]), "m": float(mean[k, 0]), "sem": float(sem[k, 0]),
+             "samples": int(cnt[k, 0])} for k, g in enumerate(mine)]
+    rows = R.gather_rows(part, mine, dist, len(reps))
+    if dist:
+        dist.destroy_process_group()
+    if rows is None:
+        return
     # temperature where <|m|> of the largest replicas crosses 0.5 (a finite-size Tc estimate)
     big = [row for row in rows if row["edge"] == max(L)]
     tc = None
     for a, b in zip(big, big[1:]):
         if a["m"] >= 0.5 > b["m"]:
             tc = a["T_K"] + (a["m"] - 0.5) * (b["T_K"] - a["T_K"]) / (a["m"] - b["m"])
-    print(json.dumps({"steps": steps, "wall_s": wall, "nspins": int(sum(r.nspins for r in reps)),
+    print(json.dumps({"steps": steps, "wall_s": wall, "ranks": world, "nspins": int(sum(r.nspins for r in reps)),
                       "tc_half_m_K": tc, "rows": rows}))
 
 
