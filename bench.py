@@ -220,7 +220,8 @@ def run_ours(args):
     systems, kw, cfg = make_workload(args.workload[: -len("_streamed")] if streamed else args.workload)
     n = sum(s.nspins for s in systems)
     S0 = LT.random_spins(n, 0)
-    flags = A.FLAG_COMPENSATED | A.FLAG_AUTOTUNE | (A.FLAG_STREAMED_EXCHANGE if streamed else 0)
+    flags = A.FLAG_COMPENSATED | (0 if args.launch_shape else A.FLAG_AUTOTUNE) | \
+        (A.FLAG_STREAMED_EXCHANGE if streamed else 0)
     p32 = A.RunParams(precision=A.FP32, seed=1 + rank, flags=flags, **kw)
     h = A.Handle(p32, systems)
     if args.launch_shape:

@@ -64,6 +64,7 @@ void free_all(asd_handle* h) {
     for (int c = 0; c < 3; c++) {
         F(h->sf[c]); F(h->sl[c]); F(h->esf[c]); F(h->fnf[c]); F(h->detf[c]); F(h->stagf[c]);
         F(h->sd[c]); F(h->esd[c]); F(h->fnd[c]); F(h->detd[c]); F(h->stagd[c]);
+        F(h->nzf[c]); F(h->nzd[c]);
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
     F(h->d_err);
@@ -695,6 +696,7 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
                 if (bytes == 4) {
                     h->sf[c] = dalloc<float>(n + SPIN_PAD); h->esf[c] = dalloc<float>(n + SPIN_PAD);
                     h->fnf[c] = dalloc<float>(n + SPIN_PAD);
+                    h->nzf[c] = dalloc<float>(n);
                     h->detf[c] = dalloc<float>(n);
                     if (p.flags & ASD_FLAG_COMPENSATED) h->sl[c] = dalloc<float>(n);
                     if (p.integrator != ASD_HEUN)
@@ -702,6 +704,7 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
                 } else {
                     h->sd[c] = dalloc<double>(n + SPIN_PAD); h->esd[c] = dalloc<double>(n + SPIN_PAD);
                     h->fnd[c] = dalloc<double>(n + SPIN_PAD);
+                    h->nzd[c] = dalloc<double>(n);
                     h->detd[c] = dalloc<double>(n);
                     if (p.integrator != ASD_HEUN)
                         for (int q = 0; q < (p.integrator == ASD_RK4 ? 3 : 5); q++) h->kd[q][c] = dalloc<double>(n);

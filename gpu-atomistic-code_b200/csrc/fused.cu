@@ -34,6 +34,8 @@ struct StageArgs {
     Vec3<R> det;         // det field (stage 2, at the det step)
     CVec3<R> stag;       // site-field profile or nullptrs
     Vec3<R> k[6];        // RK stage increments
+    Vec3<R> nz;          // sigma sqrt(T) xi of this step: the first stage writes it, later stages read it
+    int nz_mode;         // 0: draw only, 1: draw and store in nz, 2: load from nz
     int kind;            // 1: Heun predictor, 2: Heun corrector, 10+st: RK stage st
     int nst;             // RK stages
     uint32_t rel;        // step offset inside a graph chunk
@@ -175,23 +177,26 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
     const MatConst& mc = c.mat[at];
     const uint32_t r = replica_of(c, i);
     constexpr bool F32 = sizeof(R) == 4;
+    // one thermal draw per spin and step serves every stage (src/cuint.cu:72): the first stage
+    // draws it, later stages of the step load what the first stored
     R lrn[3] = {R(0), R(0), R(0)};
-    if constexpr (F32) {
-        const float sqrtT = __ldg(c.rep_sqrtT_f + r);
-        if (sqrtT > 0.0f) {
+    bool hot;
+    if constexpr (F32) hot = __ldg(c.rep_sqrtT_f + r) > 0.0f; else hot = __ldg(c.rep_sqrtT + r) > 0.0;
+    if (hot && a.nz_mode == 2) {
+        lrn[0] = a.nz.p[0][i]; lrn[1] = a.nz.p[1][i]; lrn[2] = a.nz.p[2][i];
+    } else if (hot) {
+        if constexpr (F32) {
             float xi[3];
             thermal_normals_f(c.seed, __ldg(c.rep_stream + r), i - __ldg(c.rep_off + r), t, xi);
-            const float tp = sqrtT * mc.sigma_f;
+            const float tp = __ldg(c.rep_sqrtT_f + r) * mc.sigma_f;
             lrn[0] = xi[0] * tp; lrn[1] = xi[1] * tp; lrn[2] = xi[2] * tp;
-        }
-    } else {
-        const double sqrtT = __ldg(c.rep_sqrtT + r);
-        if (sqrtT > 0.0) {
+        } else {
             double xi[3];
             thermal_normals(c.seed, __ldg(c.rep_stream + r), i - __ldg(c.rep_off + r), t, xi);
-            const double tp = sqrtT * mc.sigma;
+            const double tp = __ldg(c.rep_sqrtT + r) * mc.sigma;
             lrn[0] = xi[0] * tp; lrn[1] = xi[1] * tp; lrn[2] = xi[2] * tp;
         }
+        if (a.nz_mode == 1) { a.nz.p[0][i] = lrn[0]; a.nz.p[1][i] = lrn[1]; a.nz.p[2][i] = lrn[2]; }
     }
     bool stage_timeout = false;
     if (staged && !mbar_wait_bounded(&stage_bar, STAGE_WAIT_POLLS)) {
@@ -353,7 +358,10 @@ double stage_bytes(const asd_handle* h, const StageArgs<R>& a, bool comp) {
     if (a.stag.p[0]) st += 3 * vb;
     if (a.lr.hr) st += 12;
     if (a.lr.mr) st += 12;
-    return n * (m + st);
+    double hot = 0.0;                                    // spins with T > 0: the step's draw is
+    for (uint32_t r = 0; r < h->nrep; r++)               // stored by the first stage, loaded by the rest
+        if (h->h_rep_T[r] > 0.0) hot += h->h_rep_off[r + 1] - h->h_rep_off[r];
+    return n * (m + st) + (a.nz_mode ? hot * 3 * vb : 0.0);
 }
 
 template <typename R, int EX, bool FULL, bool COMP>
@@ -426,6 +434,7 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
     if (comp) a.base_lo = CVec3<float>{{h->sl[0], h->sl[1], h->sl[2]}};
     if (stag[0]) a.stag = c3<R>(stag);
     a.rel = rel;
+    if constexpr (sizeof(R) == 4) a.nz = v3<R>(h->nzf); else a.nz = v3<R>(h->nzd);
     const uint64_t t = h->step + rel;
     const uint32_t upd = h->p.update ? h->p.update : 1;
     LongRange& L = h->lr;
@@ -435,7 +444,7 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
     auto run = [&](const StageArgs<R>& aa) { return comp ? launch_stage<R, true>(h, aa) : launch_stage<R, false>(h, aa); };
     if (h->p.integrator == ASD_HEUN) {
         // predictor
-        a.src = c3<R>(s); a.out = v3<R>(es); a.fn = v3<R>(fn); a.kind = 1;
+        a.src = c3<R>(s); a.out = v3<R>(es); a.fn = v3<R>(fn); a.kind = 1; a.nz_mode = 1;
         a.lr = none;
         if (L.mode == ASD_LR_FFT) {
             if ((e = launch_lr_eval_f32(h)) != cudaSuccess) return e;   // field of S (scattered before)
@@ -446,7 +455,7 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
         }
         if ((e = run(a)) != cudaSuccess) return e;
         // corrector
-        a.src = c3<R>(es); a.out = v3<R>(s); a.kind = 2; a.det = v3<R>(det);
+        a.src = c3<R>(es); a.out = v3<R>(s); a.kind = 2; a.det = v3<R>(det); a.nz_mode = 2;
         if (comp) a.out_lo = Vec3<float>{{h->sl[0], h->sl[1], h->sl[2]}};
         a.lr = none;
         if (L.mode == ASD_LR_FFT) {
@@ -464,6 +473,7 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
     if (L.mode == ASD_LR_DIPOLE && t % upd == 0 && (e = launch_lr_eval_f32(h)) != cudaSuccess) return e;
     for (int st = 0; st < nst; st++) {
         a.kind = 10 + st;
+        a.nz_mode = st == 0 ? 1 : 2;
         a.src = st == 0 ? c3<R>(s) : c3<R>(pp[(st - 1) & 1]);
         for (int q = 0; q < 6; q++) {
             if constexpr (sizeof(R) == 4) a.k[q] = v3<R>(h->kf[q]); else a.k[q] = v3<R>(h->kd[q]);
@@ -501,6 +511,8 @@ cudaError_t time_first_stage_t(asd_handle* h, int warm, int reps, float* ms) {
     a.fn = v3<R>(fn);
     if (stag[0]) a.stag = c3<R>(stag);
     a.lr.P = h->lr.P; a.lr.idx = h->lr.mesh_idx; a.lr.w = h->lr.w;
+    if constexpr (sizeof(R) == 4) a.nz = v3<R>(h->nzf); else a.nz = v3<R>(h->nzd);
+    a.nz_mode = 1;
     if (h->p.integrator == ASD_HEUN) {
         a.kind = 1;
     } else {

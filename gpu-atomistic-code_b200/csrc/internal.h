@@ -137,6 +137,8 @@ struct asd_handle {
     float *kf[6][3] = {{nullptr}};
     float *detf[3] = {nullptr}, *stagf[3] = {nullptr};
     double *sd[3] = {nullptr}, *esd[3] = {nullptr}, *fnd[3] = {nullptr}, *kd[6][3] = {{nullptr}};
+    float* nzf[3] = {nullptr};           // this step's thermal field sigma sqrt(T) xi (fused forms)
+    double* nzd[3] = {nullptr};
     double *detd[3] = {nullptr}, *stagd[3] = {nullptr};
     asd::SellDev sell;
     asd::DiaDev dia;
