@@ -132,6 +132,16 @@ __device__ __forceinline__ double series_log(double x) {
     return __fma_rn((double)e, 0x1.62e42fefa39efp-1, lnm);
 }
 
+// (sin, cos) of the angle from those of its reduced argument in octant q, without branches:
+// q in {1,2,5,6} swaps the pair, q in {4..7} negates sin, q in {2..5} negates cos.
+template <typename T>
+__device__ __forceinline__ void octant_select(int q, T s, T c, T& sn, T& cs) {
+    const bool swap = ((q + 1) >> 1) & 1;
+    const T a = swap ? c : s, b = swap ? s : c;
+    sn = (q >> 2) & 1 ? -a : a;
+    cs = ((q + 2) >> 2) & 1 ? -b : b;
+}
+
 // sin, cos of 2 pi (x+0.5)/2^32: exact octant reduction, Taylor series on [0, pi/4].
 __device__ __forceinline__ void series_sincos_2pi(uint32_t x, double& sn, double& cs) {
     const double v = __dmul_rn(__dadd_rn((double)x, 0.5), 0x1p-29);
@@ -162,16 +172,7 @@ __device__ __forceinline__ void series_sincos_2pi(uint32_t x, double& sn, double
     cp = __fma_rn(cp, mp2, 0x1.5555555555555p-5);  // 1/4!
     cp = __fma_rn(cp, mp2, 0x1.0000000000000p-1);  // 1/2!
     const double c = __fma_rn(cp, mp2, 1.0);
-    switch (q) {
-    case 0: sn = s;  cs = c;  break;
-    case 1: sn = c;  cs = s;  break;
-    case 2: sn = c;  cs = -s; break;
-    case 3: sn = s;  cs = -c; break;
-    case 4: sn = -s; cs = -c; break;
-    case 5: sn = -c; cs = -s; break;
-    case 6: sn = -c; cs = s;  break;
-    default: sn = -s; cs = c; break;
-    }
+    octant_select(q, s, c, sn, cs);
 }
 
 __device__ __forceinline__ void thermal_normals(uint64_t seed, uint32_t stream, uint32_t spin, uint64_t step,
@@ -231,16 +232,7 @@ __device__ __forceinline__ void series_sincos_2pi_f(uint32_t x, float& sn, float
     cp = __fmaf_rn(cp, mp2, 0x1.555556p-5f);  // 1/4!
     cp = __fmaf_rn(cp, mp2, 0x1.000000p-1f);  // 1/2!
     const float c = __fmaf_rn(cp, mp2, 1.0f);
-    switch (q) {
-    case 0: sn = s;  cs = c;  break;
-    case 1: sn = c;  cs = s;  break;
-    case 2: sn = c;  cs = -s; break;
-    case 3: sn = s;  cs = -c; break;
-    case 4: sn = -s; cs = -c; break;
-    case 5: sn = -c; cs = -s; break;
-    case 6: sn = -c; cs = s;  break;
-    default: sn = -s; cs = c; break;
-    }
+    octant_select(q, s, c, sn, cs);
 }
 
 __device__ __forceinline__ void thermal_normals_f(uint64_t seed, uint32_t stream, uint32_t spin, uint64_t step,

@@ -35,6 +35,8 @@ struct StageArgs {
     CVec3<R> stag;       // site-field profile or nullptrs
     Vec3<R> k[6];        // RK stage increments
     Vec3<R> nz;          // sigma sqrt(T) xi of this step: the first stage writes it, later stages read it
+    const void* pf[24];  // per-spin arrays this stage reads at its own rows: prefetched into L2
+    uint32_t npf;        // at the start of each block
     int nz_mode;         // 0: draw only, 1: draw and store in nz, 2: load from nz
     int kind;            // 1: Heun predictor, 2: Heun corrector, 10+st: RK stage st
     int nst;             // RK stages
@@ -112,12 +114,25 @@ __constant__ double FRK4C[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
 template <typename R>
 struct MinBlocks { static constexpr int value = sizeof(R) == 4 ? 5 : 1; };
 
-template <typename R, int EX, bool FULL, bool COMP>
+// K: the stage kind at compile time (1 Heun predictor, 2 Heun corrector, 3 RK stage before the
+// last, 4 last RK stage); a.kind still carries the RK stage index.
+template <typename R, int EX, bool FULL, bool COMP, int K>
 __global__ void __launch_bounds__(256, MinBlocks<R>::value)
     stage_kernel(const StepConst c, const SellDev sell, const DiaDev dia, const StageArgs<R> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t stage_bar;
     R* tab = reinterpret_cast<R*>(smem_raw);
+    if (threadIdx.x == 0 && a.npf) {
+        // the block's rows of every per-spin input: one bulk L2 prefetch each, so the loads
+        // after the exchange gather find them in L2; sizes stop at the last row (whole
+        // 16-byte units), so no prefetch reaches past an array
+        const uint32_t r0 = blockIdx.x * blockDim.x;
+        const uint32_t rows = min(blockDim.x, c.n - r0);
+        const uint32_t bytes = (rows * (uint32_t)sizeof(R)) & ~15u;
+        if (bytes)
+            for (uint32_t q = 0; q < a.npf; q++)
+                bulk_prefetch_l2(static_cast<const char*>(a.pf[q]) + (size_t)r0 * sizeof(R), bytes);
+    }
     const uint32_t* staged = nullptr;
     const R* sspin = nullptr;
     uint32_t wbase = 0;
@@ -231,21 +246,23 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
     // stage spin at this site
     R sv[3] = {a.src.p[0][i], a.src.p[1][i], a.src.p[2][i]};
     const int kind = a.kind;
-    if (kind >= 11 && (c.flags & ASD_FLAG_RK_STAGE_SPIN_MIXED)) { sv[1] = a.base.p[1][i]; sv[2] = a.base.p[2][i]; }
+    if constexpr (K >= 3) {
+        if (kind >= 11 && (c.flags & ASD_FLAG_RK_STAGE_SPIN_MIXED)) { sv[1] = a.base.p[1][i]; sv[2] = a.base.p[2][i]; }
+    }
     anis_field<R>(c, mc, sv, h);
     R f[3];
     if constexpr (F32) llg_rhs<R>(mc.llgpf_f, mc.lambda_f, sv, h, f);
     else llg_rhs<R>(mc.llgpf, mc.lambda, sv, h, f);
 
-    const bool final_spin = kind == 2 || (kind >= 10 && kind - 10 == a.nst - 1);
+    constexpr bool final_spin = K == 2 || K == 4;
     R out[3];
-    if (!final_spin && F32) {
+    if constexpr (!final_spin && F32) {
         // FP32 form: intermediate stage spins (Heun S', RK stage vectors) only feed field
         // evaluations, so they are formed and renormalised in single precision
         const float rdt = c.rdt_f;
         float o[3];
         const float S[3] = {(float)a.base.p[0][i], (float)a.base.p[1][i], (float)a.base.p[2][i]};
-        if (kind == 1) {
+        if constexpr (K == 1) {
             for (int j = 0; j < 3; j++) { a.fn.p[j][i] = f[j]; o[j] = fmaf(rdt, (float)f[j], S[j]); }
         } else {
             const int st = kind - 10, nst = a.nst;
@@ -270,14 +287,14 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
         // new S (and every stage of the FP64 fused form): FP64 accumulation from the
         // full-precision base, FP64 renormalisation
         double S[3] = {(double)a.base.p[0][i], (double)a.base.p[1][i], (double)a.base.p[2][i]};
-        if constexpr (COMP) {
-            if (final_spin) { S[0] += (double)a.base_lo.p[0][i]; S[1] += (double)a.base_lo.p[1][i]; S[2] += (double)a.base_lo.p[2][i]; }
+        if constexpr (COMP && final_spin) {
+            S[0] += (double)a.base_lo.p[0][i]; S[1] += (double)a.base_lo.p[1][i]; S[2] += (double)a.base_lo.p[2][i];
         }
         const double rdt = c.rdt;
         double o[3];
-        if (kind == 1) {
+        if constexpr (K == 1) {
             for (int j = 0; j < 3; j++) { a.fn.p[j][i] = f[j]; o[j] = S[j] + rdt * (double)f[j]; }
-        } else if (kind == 2) {
+        } else if constexpr (K == 2) {
             for (int j = 0; j < 3; j++) o[j] = S[j] + 0.5 * rdt * (double)(a.fn.p[j][i] + f[j]);
             if ((double)t == dyn[DYN_DET_STEP])
                 for (int j = 0; j < 3; j++) a.det.p[j][i] = h[j] - lrn[j];
@@ -286,7 +303,7 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
             const bool dbl = (c.flags & ASD_FLAG_RK_DOUBLE_RDT) != 0;
             double k[3];
             for (int j = 0; j < 3; j++) k[j] = rdt * (double)f[j];
-            if (st < nst - 1) {
+            if constexpr (K == 3) {
                 for (int j = 0; j < 3; j++) a.k[st].p[j][i] = (R)k[j];
                 for (int j = 0; j < 3; j++) {
                     double inc;
@@ -312,7 +329,7 @@ __global__ void __launch_bounds__(256, MinBlocks<R>::value)
             const R hi = (R)o[j];
             out[j] = hi;
             a.out.p[j][i] = hi;
-            if constexpr (COMP) { if (final_spin) a.out_lo.p[j][i] = (float)(o[j] - (double)hi); }
+            if constexpr (COMP && final_spin) a.out_lo.p[j][i] = (float)(o[j] - (double)hi);
         }
     }
     if (a.lr.mr) {
@@ -364,8 +381,8 @@ double stage_bytes(const asd_handle* h, const StageArgs<R>& a, bool comp) {
     return n * (m + st) + (a.nz_mode ? hot * 3 * vb : 0.0);
 }
 
-template <typename R, int EX, bool FULL, bool COMP>
-cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
+template <typename R, int EX, bool FULL, bool COMP, int K>
+cudaError_t launch_stage_k(asd_handle* hd, const StageArgs<R>& a) {
     const int B = hd->block;
     const unsigned grid = (hd->n + B - 1) / B;
     size_t smem = 0;
@@ -378,7 +395,7 @@ cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
     if (smem > 48 * 1024) {
         static size_t opted = 48 * 1024;   // per instantiation: raise the dynamic shared-memory cap once
         if (smem > opted) {
-            const cudaError_t e = cudaFuncSetAttribute(stage_kernel<R, EX, FULL, COMP>,
+            const cudaError_t e = cudaFuncSetAttribute(stage_kernel<R, EX, FULL, COMP, K>,
                                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
             opted = smem;
@@ -388,7 +405,7 @@ cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
         if (hd->flush_buf) cudaMemsetAsync(hd->flush_buf, 0, hd->flush_bytes, hd->stream);
         cudaEventRecord(hd->kev[0], hd->stream);
     }
-    stage_kernel<R, EX, FULL, COMP><<<grid, B, smem, hd->stream>>>(hd->sc, hd->sell, hd->dia, a);
+    stage_kernel<R, EX, FULL, COMP, K><<<grid, B, smem, hd->stream>>>(hd->sc, hd->sell, hd->dia, a);
     hd->launches += 1;
     if (hd->timing) {
         cudaEventRecord(hd->kev[1], hd->stream);
@@ -408,6 +425,14 @@ cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
     return cudaGetLastError();
 }
 
+template <typename R, int EX, bool FULL, bool COMP>
+cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
+    if (a.kind == 1) return launch_stage_k<R, EX, FULL, COMP, 1>(hd, a);
+    if (a.kind == 2) return launch_stage_k<R, EX, FULL, COMP, 2>(hd, a);
+    if (a.kind - 10 == a.nst - 1) return launch_stage_k<R, EX, FULL, COMP, 4>(hd, a);
+    return launch_stage_k<R, EX, FULL, COMP, 3>(hd, a);
+}
+
 template <typename R, bool COMP>
 cudaError_t launch_stage(asd_handle* hd, const StageArgs<R>& a) {
     if (hd->exch == ASD_EXCH_CSR) {
@@ -422,6 +447,28 @@ template <typename R>
 void state_ptrs(asd_handle* h, R* const** s, R* const** es, R* const** fn, R* const** det, R* const** stag) {
     if constexpr (sizeof(R) == 4) { *s = h->sf; *es = h->esf; *fn = h->fnf; *det = h->detf; *stag = h->stagf; }
     else { *s = h->sd; *es = h->esd; *fn = h->fnd; *det = h->detd; *stag = h->stagd; }
+}
+
+// Per-spin arrays a stage reads at its own rows, for the kernel's L2 prefetch: base S, the stage
+// spin if it differs, the lo part (last stage, compensated), f_n (Heun corrector), the carried
+// thermal field, the site-field profile, earlier RK increments.
+template <typename R>
+void set_prefetch(StageArgs<R>& a, bool comp) {
+    const bool last = a.kind == 2 || (a.kind >= 10 && a.kind - 10 == a.nst - 1);
+    uint32_t k = 0;
+    auto add3 = [&](const void* p0, const void* p1, const void* p2) {
+        if (!p0 || k + 3 > 24) return;
+        a.pf[k++] = p0; a.pf[k++] = p1; a.pf[k++] = p2;
+    };
+    add3(a.base.p[0], a.base.p[1], a.base.p[2]);
+    if (a.src.p[0] != a.base.p[0]) add3(a.src.p[0], a.src.p[1], a.src.p[2]);
+    if (comp && last) add3(a.base_lo.p[0], a.base_lo.p[1], a.base_lo.p[2]);
+    if (a.kind == 2) add3(a.fn.p[0], a.fn.p[1], a.fn.p[2]);
+    if (a.nz_mode == 2) add3(a.nz.p[0], a.nz.p[1], a.nz.p[2]);
+    add3(a.stag.p[0], a.stag.p[1], a.stag.p[2]);
+    if (a.kind >= 10)
+        for (int b = 0; b < a.kind - 10; b++) add3(a.k[b].p[0], a.k[b].p[1], a.k[b].p[2]);
+    a.npf = k;
 }
 
 template <typename R>
@@ -441,7 +488,12 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
     LrArgs none{};
     none.P = L.P; none.idx = L.mesh_idx; none.w = L.w; none.inv_p = L.P ? 1.0f / (float)L.P : 0.f;
     cudaError_t e;
-    auto run = [&](const StageArgs<R>& aa) { return comp ? launch_stage<R, true>(h, aa) : launch_stage<R, false>(h, aa); };
+    auto run = [&](const StageArgs<R>& a0) {
+        StageArgs<R> aa = a0;
+        set_prefetch(aa, comp);
+        if constexpr (sizeof(R) == 4) return comp ? launch_stage<R, true>(h, aa) : launch_stage<R, false>(h, aa);
+        else return launch_stage<R, false>(h, aa);
+    };
     if (h->p.integrator == ASD_HEUN) {
         // predictor
         a.src = c3<R>(s); a.out = v3<R>(es); a.fn = v3<R>(fn); a.kind = 1; a.nz_mode = 1;
@@ -522,7 +574,11 @@ cudaError_t time_first_stage_t(asd_handle* h, int warm, int reps, float* ms) {
             if constexpr (sizeof(R) == 4) a.k[q] = v3<R>(h->kf[q]); else a.k[q] = v3<R>(h->kd[q]);
         }
     }
-    auto run = [&]() { return comp ? launch_stage<R, true>(h, a) : launch_stage<R, false>(h, a); };
+    set_prefetch(a, comp);
+    auto run = [&]() {
+        if constexpr (sizeof(R) == 4) return comp ? launch_stage<R, true>(h, a) : launch_stage<R, false>(h, a);
+        else return launch_stage<R, false>(h, a);
+    };
     cudaError_t e = cudaSuccess;
     for (int q = 0; q < warm && e == cudaSuccess; q++) e = run();
     if (e != cudaSuccess) return e;
