@@ -287,6 +287,30 @@ void setup_lr(asd_handle* h, const asd_system& s, bool plain) {
                 nrs[pr[0] * L.P + c] = m;
                 nrs[pr[1] * L.P + c] = m;
             }
+    if (!plain) {
+        // On an even mesh axis the plane at index m/2 holds the aliased displacement +-m/2; when
+        // the spins span fewer than m/2 mesh points along that axis no two spins are that far
+        // apart, so the plane never reaches a spin and is cleared.  N_r is then exactly even
+        // (N(-r) = N(r)), its transform real, and the convolution takes the 6-component real form.
+        uint32_t lo[3] = {~0u, ~0u, ~0u}, hi[3] = {0, 0, 0};
+        for (uint32_t i = 0; i < h->n; i++)
+            for (int a = 0; a < 3; a++) {
+                lo[a] = std::min(lo[a], s.mesh_xyz[3 * i + a]);
+                hi[a] = std::max(hi[a], s.mesh_xyz[3 * i + a]);
+            }
+        for (int a = 0; a < 3; a++) {
+            const uint32_t m = L.mesh[a];
+            if (m % 2 || h->n == 0 || hi[a] - lo[a] >= m / 2) continue;
+            for (uint32_t x = 0; x < L.mesh[0]; x++)
+                for (uint32_t y = 0; y < L.mesh[1]; y++)
+                    for (uint32_t z = 0; z < L.mesh[2]; z++) {
+                        const uint32_t v[3] = {x, y, z};
+                        if (v[a] != m / 2) continue;
+                        const size_t c = ((size_t)x * L.mesh[1] + y) * L.mesh[2] + z;
+                        for (int q = 0; q < 9; q++) nrs[q * L.P + c] = 0.0;
+                    }
+        }
+    }
     double* d_nr = dupload(plain ? s.nr : nrs.data(), 9 * L.P);
     int dims[3] = {(int)L.mesh[0], (int)L.mesh[1], (int)L.mesh[2]};
     cudaError_t e;
