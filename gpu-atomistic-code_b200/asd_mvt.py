@@ -52,6 +52,29 @@ def run_mvt(reps, equil, average, update=100, convmean=1e-4, convvar=1e-4, preci
     return mean, sem, st[..., 0], steps
 
 
+def compare(args):
+    """M(T) of the FP32 form against the FP64 plain form on the same replicas and seeds: at finite
+    T the trajectories decorrelate, so the check is statistical, per replica
+    z = (m32 - m64) / sqrt(sem32^2 + sem64^2), with the share of |z| < 2 reported."""
+    edges = tuple(int(e) for e in args.edges.split(","))
+    reps, L, Ts = LT.replica_batch(args.replicas, edges=edges, seed=args.seed, Tmax=args.tmax)
+    out = {}
+    for name, prec in (("fp32", A.FP32), ("fp64_plain", A.FP64_PLAIN)):
+        t0 = time.time()
+        mean, sem, cnt, steps = run_mvt(reps, args.equil, args.average, args.update, convmean=0.0, convvar=0.0,
+                                        precision=prec, seed=args.seed)
+        out[name] = (mean[:, 0], sem[:, 0], time.time() - t0)
+    m32, s32, w32 = out["fp32"]
+    m64, s64, w64 = out["fp64_plain"]
+    z = (m32 - m64) / np.sqrt(np.maximum(s32 ** 2 + s64 ** 2, 1e-300))
+    hot = Ts > 0
+    rows = [{"edge": int(l), "T_K": float(t), "m_fp32": float(a), "sem_fp32": float(b), "m_fp64": float(c),
+             "sem_fp64": float(d), "z": float(e)} for l, t, a, b, c, d, e in zip(L, Ts, m32, s32, m64, s64, z)]
+    print(json.dumps({"steps": steps, "wall_s_fp32": w32, "wall_s_fp64_plain": w64,
+                      "within_2sigma": float(np.mean(np.abs(z[hot]) < 2.0)), "max_abs_z": float(np.abs(z[hot]).max()),
+                      "rows": rows}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--replicas", type=int, default=96)
@@ -60,7 +83,13 @@ def main():
     ap.add_argument("--update", type=int, default=100)
     ap.add_argument("--tmax", type=float, default=None, help="highest temperature (default 1.2 x 104 K)")
     ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--edges", default="16,24,32,48,64", help="replica edge lengths to draw from")
+    ap.add_argument("--compare-fp64", action="store_true",
+                    help="also run the FP64 plain form and report (m32 - m64) / sqrt(sem32^2 + sem64^2)")
     args = ap.parse_args()
+    if args.compare_fp64:
+        compare(args)
+        return
     reps, L, Ts = LT.replica_batch(args.replicas, seed=args.seed, Tmax=args.tmax)
     # under torchrun each rank (one GPU) runs its share of the temperatures
     dist = None

@@ -83,6 +83,8 @@ void free_all(asd_handle* h) {
     if (L.r2c) cufftDestroy(L.r2c);
     if (L.c2r) cufftDestroy(L.c2r);
     if (L.z2z) cufftDestroy(L.z2z);
+    if (L.c2c) cufftDestroy(L.c2c);
+    F(L.k1); F(L.k2);
     F(h->sq.idx); F(h->sq.sub); F(h->sq.uo); F(h->sq.kidx); F(h->sq.grid); F(h->sq.series);
     if (h->sq.plan) cufftDestroy(h->sq.plan);
     F(h->d_magpart); F(h->d_mag); F(h->d_inv_count); F(h->d_sub_of_atom); F(h->d_stats);
@@ -287,17 +289,17 @@ void setup_lr(asd_handle* h, const asd_system& s, bool plain) {
                 nrs[pr[0] * L.P + c] = m;
                 nrs[pr[1] * L.P + c] = m;
             }
+    uint32_t lo[3] = {~0u, ~0u, ~0u}, hi[3] = {0, 0, 0};    // bounding box of the spins on the mesh
+    for (uint32_t i = 0; i < h->n; i++)
+        for (int a = 0; a < 3; a++) {
+            lo[a] = std::min(lo[a], s.mesh_xyz[3 * i + a]);
+            hi[a] = std::max(hi[a], s.mesh_xyz[3 * i + a]);
+        }
     if (!plain) {
         // On an even mesh axis the plane at index m/2 holds the aliased displacement +-m/2; when
         // the spins span fewer than m/2 mesh points along that axis no two spins are that far
         // apart, so the plane never reaches a spin and is cleared.  N_r is then exactly even
         // (N(-r) = N(r)), its transform real, and the convolution takes the 6-component real form.
-        uint32_t lo[3] = {~0u, ~0u, ~0u}, hi[3] = {0, 0, 0};
-        for (uint32_t i = 0; i < h->n; i++)
-            for (int a = 0; a < 3; a++) {
-                lo[a] = std::min(lo[a], s.mesh_xyz[3 * i + a]);
-                hi[a] = std::max(hi[a], s.mesh_xyz[3 * i + a]);
-            }
         for (int a = 0; a < 3; a++) {
             const uint32_t m = L.mesh[a];
             if (m % 2 || h->n == 0 || hi[a] - lo[a] >= m / 2) continue;
@@ -324,12 +326,27 @@ void setup_lr(asd_handle* h, const asd_system& s, bool plain) {
         e = build_nk_plain(h, d_nr);
     } else {
         L.r = dalloc<float>(6 * L.P);   // [0,3P): M_r, [3P,6P): H_r
-        L.k = dalloc<float2>(3 * L.Pk);
-        CKFFT(cufftPlanMany(&L.r2c, 3, dims, nullptr, 1, (int)L.P, nullptr, 1, (int)L.Pk, CUFFT_R2C, 3));
-        CKFFT(cufftPlanMany(&L.c2r, 3, dims, nullptr, 1, (int)L.Pk, nullptr, 1, (int)L.P, CUFFT_C2R, 3));
-        CKFFT(cufftSetStream(L.r2c, h->stream));
-        CKFFT(cufftSetStream(L.c2r, h->stream));
+        const uint32_t mz = L.mesh[2];
+        // pruned transform when the last axis is a power of two: z transforms only for the rows
+        // of the spins' box, 2D transforms of the (x, y) planes by cuFFT
+        L.pruned = (mz >= 4 && mz <= 4096 && (mz & (mz - 1)) == 0 && h->n > 0) ? 1 : 0;
+        if (L.pruned) {
+            for (int a = 0; a < 3; a++) { L.box0[a] = lo[a]; L.box1[a] = hi[a]; }
+            L.k1 = dalloc<float2>(3 * L.Pk);
+            L.k2 = dalloc<float2>(3 * L.Pk);
+            int d2[2] = {(int)L.mesh[0], (int)L.mesh[1]};
+            const int plane = (int)(L.mesh[0] * L.mesh[1]);
+            CKFFT(cufftPlanMany(&L.c2c, 2, d2, nullptr, 1, plane, nullptr, 1, plane, CUFFT_C2C, 3 * (int)(mz / 2 + 1)));
+            CKFFT(cufftSetStream(L.c2c, h->stream));
+        } else {
+            L.k = dalloc<float2>(3 * L.Pk);
+            CKFFT(cufftPlanMany(&L.r2c, 3, dims, nullptr, 1, (int)L.P, nullptr, 1, (int)L.Pk, CUFFT_R2C, 3));
+            CKFFT(cufftPlanMany(&L.c2r, 3, dims, nullptr, 1, (int)L.Pk, nullptr, 1, (int)L.P, CUFFT_C2R, 3));
+            CKFFT(cufftSetStream(L.r2c, h->stream));
+            CKFFT(cufftSetStream(L.c2r, h->stream));
+        }
         e = build_nk_f32(h, d_nr);
+        if (e == cudaSuccess && L.pruned) e = permute_nk_pruned(h);
     }
     cudaFree(d_nr);
     CK(e);

@@ -12,6 +12,7 @@
 // stored in FP32: 6 real components when N_r is symmetric and even (point
 // dipole + symmetric exchange), else 9 complex.
 #include "internal.h"
+#include <algorithm>
 #include <cstdio>
 
 namespace asd {
@@ -99,7 +100,167 @@ __global__ void real_to_cplx(size_t m, const double* __restrict__ r, double2* __
     z[i] = make_double2(r[i], 0.0);
 }
 
+// ---- pruned transform along z: M = mesh[2] = 2N real points per row, N complex points
+// z_n = x_2n + i x_2n+1 per row, radix-2 decimation in time in shared memory.
+struct ZPass {
+    uint32_t m0, m1, mz, N, logN, Kz, TY;
+    uint32_t bx0, by0, by1, bz0, bz1;   // box: x from bx0 (grid y), y in [by0, by1], z in [bz0, bz1]
+    size_t P, Pk;                       // padded real points; spectrum points Kz*m0*m1
+};
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// In-place radix-2 FFT of TY rows of N points (stride ld) already in bit-reversed order;
+// tw[j] = exp(-2 pi i j / N), conjugated for the inverse.
+__device__ __forceinline__ void smem_fft(float2* s, uint32_t ld, const float2* tw, const ZPass& A, bool inv) {
+    const uint32_t half_n = A.N / 2;
+    for (uint32_t len = 2, lg = 1; len <= A.N; len <<= 1, lg++) {
+        const uint32_t half = len >> 1, step = A.N >> lg;
+        for (uint32_t b = threadIdx.x; b < A.TY * half_n; b += blockDim.x) {
+            const uint32_t r = b / half_n, q = b % half_n;
+            const uint32_t g = q / half, j = q % half;
+            const uint32_t i0 = r * ld + g * len + j, i1 = i0 + half;
+            float2 w = tw[j * step];
+            if (inv) w.y = -w.y;
+            const float2 u = s[i0], v = cmul(s[i1], w);
+            s[i0] = make_float2(u.x + v.x, u.y + v.y);
+            s[i1] = make_float2(u.x - v.x, u.y - v.y);
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ void load_twiddles(float2* tw, uint32_t N) {
+    for (uint32_t j = threadIdx.x; j < N / 2; j += blockDim.x) {
+        float sn, cs;
+        sincospif(-2.0f * (float)j / (float)N, &sn, &cs);
+        tw[j] = make_float2(cs, sn);
+    }
+}
+
+// M_r rows (c, x, y in the box) -> half spectrum k1[c][kz][x][y], kz = 0..N.
+// grid: (y tiles of TY rows, box rows in x, 3 components).
+__global__ void zpass_r2c(const float* __restrict__ mr, float2* __restrict__ k1, const ZPass A) {
+    extern __shared__ float2 zs[];
+    const uint32_t ld = A.N + 1;
+    float2* tw = zs + A.TY * ld;
+    const uint32_t c = blockIdx.z, x = A.bx0 + blockIdx.y, y0 = A.by0 + blockIdx.x * A.TY;
+    load_twiddles(tw, A.N);
+    const float2* row0 = reinterpret_cast<const float2*>(mr + (size_t)c * A.P);
+    for (uint32_t e = threadIdx.x; e < A.TY * A.N; e += blockDim.x) {
+        const uint32_t r = e / A.N, n = e % A.N, y = y0 + r;
+        float2 v = make_float2(0.f, 0.f);
+        if (y <= A.by1 && 2 * n + 1 >= A.bz0 && 2 * n <= A.bz1)
+            v = row0[(((size_t)x * A.m1 + y) * A.mz) / 2 + n];
+        zs[r * ld + (__brev(n) >> (32 - A.logN))] = v;
+    }
+    __syncthreads();
+    smem_fft(zs, ld, tw, A, false);
+    // X_k = E_k + w^k O_k, E = (Z_k + conj Z_{N-k}) / 2, O = -i (Z_k - conj Z_{N-k}) / 2, w = e^{-i pi / N}
+    for (uint32_t e = threadIdx.x; e < (A.N + 1) * A.TY; e += blockDim.x) {
+        const uint32_t k = e / A.TY, r = e % A.TY, y = y0 + r;
+        if (y > A.by1) continue;
+        const float2 zk = zs[r * ld + (k & (A.N - 1))], zm = zs[r * ld + ((A.N - k) & (A.N - 1))];
+        const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
+        const float2 O = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
+        float sn, cs;
+        sincospif(-(float)k / (float)A.N, &sn, &cs);
+        const float2 wo = cmul(make_float2(cs, sn), O);
+        k1[(((size_t)c * A.Kz + k) * A.m0 + x) * A.m1 + y] = make_float2(E.x + wo.x, E.y + wo.y);
+    }
+}
+
+// Spectrum k2[c][kz][x][y] of the box rows -> H_r rows, unnormalised like cuFFT's C2R.
+__global__ void zpass_c2r(const float2* __restrict__ k2, float* __restrict__ hr, const ZPass A) {
+    extern __shared__ float2 zs[];
+    const uint32_t ldx = A.N + 2, ld = A.N + 1;
+    float2* xs = zs;                         // [TY][N+1] spectrum rows
+    float2* s = zs + A.TY * ldx;             // [TY][N] complex rows for the inverse FFT
+    float2* tw = s + A.TY * ld;
+    const uint32_t c = blockIdx.z, x = A.bx0 + blockIdx.y, y0 = A.by0 + blockIdx.x * A.TY;
+    load_twiddles(tw, A.N);
+    for (uint32_t e = threadIdx.x; e < (A.N + 1) * A.TY; e += blockDim.x) {
+        const uint32_t k = e / A.TY, r = e % A.TY, y = y0 + r;
+        xs[r * ldx + k] = y <= A.by1 ? k2[(((size_t)c * A.Kz + k) * A.m0 + x) * A.m1 + y] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    // Z_k = (X_k + conj X_{N-k}) + i e^{+i pi k / N} (X_k - conj X_{N-k}), k < N, bit-reversed
+    for (uint32_t e = threadIdx.x; e < A.TY * A.N; e += blockDim.x) {
+        const uint32_t r = e / A.N, k = e % A.N;
+        const float2 xk = xs[r * ldx + k], xm = xs[r * ldx + (A.N - k)];
+        const float2 sp = make_float2(xk.x + xm.x, xk.y - xm.y);
+        const float2 df = make_float2(xk.x - xm.x, xk.y + xm.y);
+        float sn, cs;
+        sincospif((float)k / (float)A.N, &sn, &cs);
+        const float2 t = cmul(make_float2(cs, sn), df);
+        s[r * ld + (__brev(k) >> (32 - A.logN))] = make_float2(sp.x - t.y, sp.y + t.x);
+    }
+    __syncthreads();
+    smem_fft(s, ld, tw, A, true);
+    float2* out0 = reinterpret_cast<float2*>(hr + (size_t)c * A.P);
+    for (uint32_t e = threadIdx.x; e < A.TY * A.N; e += blockDim.x) {
+        const uint32_t r = e / A.N, n = e % A.N, y = y0 + r;
+        if (y > A.by1 || 2 * n + 1 < A.bz0 || 2 * n > A.bz1) continue;
+        out0[(((size_t)x * A.m1 + y) * A.mz) / 2 + n] = s[r * ld + n];
+    }
+}
+
+// [comp][x][y][kz] -> [comp][kz][x][y] for the pruned spectrum layout.
+template <typename T>
+__global__ void permute_nk(size_t Pk, uint32_t ncomp, uint32_t m0, uint32_t m1, uint32_t Kz, const T* __restrict__ in,
+                           T* __restrict__ out) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Pk * ncomp) return;
+    const size_t q = e / Pk, i = e % Pk;
+    const uint32_t kz = (uint32_t)(i % Kz);
+    const size_t xy = i / Kz;                       // x * m1 + y
+    out[q * Pk + (size_t)kz * m0 * m1 + xy] = in[e];
+}
+
+ZPass zpass_args(const LongRange& L) {
+    ZPass A{};
+    A.m0 = L.mesh[0]; A.m1 = L.mesh[1]; A.mz = L.mesh[2]; A.N = A.mz / 2;
+    A.logN = 0;
+    while ((1u << A.logN) < A.N) A.logN++;
+    A.Kz = A.N + 1;
+    A.TY = A.N >= 2048 ? 1 : std::min<uint32_t>(32, 2048 / A.N);
+    A.bx0 = L.box0[0]; A.by0 = L.box0[1]; A.by1 = L.box1[1]; A.bz0 = L.box0[2]; A.bz1 = L.box1[2];
+    A.P = L.P; A.Pk = (size_t)A.Kz * A.m0 * A.m1;
+    return A;
+}
+
 }  // namespace
+
+// Pruned-transform sizes: shared memory of the two z-pass kernels.
+size_t zpass_smem(const LongRange& L, bool inverse) {
+    const ZPass A = zpass_args(L);
+    if (!inverse) return sizeof(float2) * ((size_t)A.TY * (A.N + 1) + A.N / 2);
+    return sizeof(float2) * ((size_t)A.TY * (A.N + 2) + (size_t)A.TY * (A.N + 1) + A.N / 2);
+}
+
+cudaError_t permute_nk_pruned(asd_handle* h) {
+    LongRange& L = h->lr;
+    const ZPass A = zpass_args(L);
+    cudaError_t e;
+    if (L.ncomp == 6 && L.nk_real) {
+        float* t = nullptr;
+        if ((e = cudaMalloc(&t, sizeof(float) * 6 * A.Pk)) != cudaSuccess) return e;
+        permute_nk<float><<<nb(6 * A.Pk, 256), 256, 0, h->stream>>>(A.Pk, 6, A.m0, A.m1, A.Kz, L.nkr, t);
+        cudaStreamSynchronize(h->stream);
+        cudaFree(L.nkr);
+        L.nkr = t;
+    } else {
+        float2* t = nullptr;
+        if ((e = cudaMalloc(&t, sizeof(float2) * 9 * A.Pk)) != cudaSuccess) return e;
+        permute_nk<float2><<<nb(9 * A.Pk, 256), 256, 0, h->stream>>>(A.Pk, 9, A.m0, A.m1, A.Kz, L.nkc, t);
+        cudaStreamSynchronize(h->stream);
+        cudaFree(L.nkc);
+        L.nkc = t;
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t launch_lr_scatter_f32(asd_handle* h, const float* const s[3]) {
     LongRange& L = h->lr;
@@ -111,6 +272,20 @@ cudaError_t launch_lr_scatter_f32(asd_handle* h, const float* const s[3]) {
 // M_r -> (R2C) -> N_k . M_k -> (C2R) -> H_r
 cudaError_t launch_lr_eval_f32(asd_handle* h) {
     LongRange& L = h->lr;
+    if (L.pruned) {
+        const ZPass A = zpass_args(L);
+        const dim3 grid((A.by1 - A.by0 + A.TY) / A.TY, L.box1[0] - L.box0[0] + 1, 3);
+        zpass_r2c<<<grid, 256, zpass_smem(L, false), h->stream>>>(L.r, L.k1, A);
+        if (cufftExecC2C(L.c2c, (cufftComplex*)L.k1, (cufftComplex*)L.k2, CUFFT_FORWARD) != CUFFT_SUCCESS)
+            return cudaErrorUnknown;
+        if (L.ncomp == 6 && L.nk_real) kconv6r<<<nb(A.Pk, 256), 256, 0, h->stream>>>(A.Pk, L.nkr, L.k2);
+        else kconv9c<<<nb(A.Pk, 256), 256, 0, h->stream>>>(A.Pk, L.nkc, L.k2);
+        if (cufftExecC2C(L.c2c, (cufftComplex*)L.k2, (cufftComplex*)L.k2, CUFFT_INVERSE) != CUFFT_SUCCESS)
+            return cudaErrorUnknown;
+        zpass_c2r<<<grid, 256, zpass_smem(L, true), h->stream>>>(L.k2, L.r + 3 * L.P, A);
+        h->launches += 3;
+        return cudaGetLastError();
+    }
     if (cufftExecR2C(L.r2c, (cufftReal*)L.r, (cufftComplex*)L.k) != CUFFT_SUCCESS) return cudaErrorUnknown;
     if (L.ncomp == 6 && L.nk_real) kconv6r<<<nb(L.Pk, 256), 256, 0, h->stream>>>(L.Pk, L.nkr, L.k);
     else kconv9c<<<nb(L.Pk, 256), 256, 0, h->stream>>>(L.Pk, L.nkc, L.k);

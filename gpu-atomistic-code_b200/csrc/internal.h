@@ -85,6 +85,14 @@ struct LongRange {
     float* nkr = nullptr;          // [ncomp][Pk] real N_k
     float2* nkc = nullptr;         // [ncomp][Pk] complex N_k
     cufftHandle r2c = 0, c2r = 0;
+    // pruned transform (power-of-two last mesh axis): own real FFT along z for the rows of the
+    // spins' bounding box box0..box1 (inclusive), then 2D C2C over the (x, y) planes; spectra
+    // in the transposed layout [c][kz][x][y]; k1 stays zero outside the box rows
+    int pruned = 0;
+    uint32_t box0[3] = {0, 0, 0}, box1[3] = {0, 0, 0};
+    float2* k1 = nullptr;
+    float2* k2 = nullptr;
+    cufftHandle c2c = 0;
     // FP64 plain: complex padded arrays [3][P] and full complex N_k [9][P]
     double2 *zr = nullptr, *zk = nullptr, *zh = nullptr, *znk = nullptr;
     cufftHandle z2z = 0;
@@ -206,5 +214,6 @@ cudaError_t launch_thermal_normals_f(uint64_t seed, uint32_t stream, uint64_t st
 cudaError_t launch_convert_spins_in(asd_handle* h, const double* d_aos);
 cudaError_t launch_convert_out(asd_handle* h, int what, double* d_aos);
 cudaError_t build_nk_f32(asd_handle* h, const double* d_nr);
+cudaError_t permute_nk_pruned(asd_handle* h);
 cudaError_t build_nk_plain(asd_handle* h, const double* d_nr);
 }  // namespace asd

@@ -144,8 +144,11 @@ def test_fp32_finite_temperature_close(gpu):
     assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
 
 
-def test_dipole_csr_plain_and_fp32(gpu):
-    s = LT.sc_ferromagnet(6, pbc=(0, 0, 0), dipole=True)
+# mesh 2L per axis: L = 6 takes the full 3D transform (last axis 12), (8, 6, 4) and (5, 7, 8)
+# the pruned one (last axis 8 / 16; odd box extents in x and y)
+@pytest.mark.parametrize("L", [6, (8, 6, 4), (5, 7, 8)])
+def test_dipole_csr_plain_and_fp32(gpu, L):
+    s = LT.sc_ferromagnet(L, pbc=(0, 0, 0), dipole=True)
     g, o, _, _ = pair(s, 40, A.FP64_PLAIN, update=1)
     assert maxdiff(g, o) <= 1e-10, maxdiff(g, o)
     g, o, _, _ = pair(s, 40, A.FP32, update=1, flags=A.FLAG_COMPENSATED)
@@ -154,8 +157,9 @@ def test_dipole_csr_plain_and_fp32(gpu):
     assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
 
 
-def test_fft_exchange_mode_plain_and_fp32(gpu):
-    s = LT.sc_fft(6)
+@pytest.mark.parametrize("L", [6, (8, 6, 4), (5, 7, 8)])
+def test_fft_exchange_mode_plain_and_fp32(gpu, L):
+    s = LT.sc_fft(L)
     g, o, _, _ = pair(s, 40, A.FP64_PLAIN)
     assert maxdiff(g, o) <= 1e-10, maxdiff(g, o)
     g, o, _, _ = pair(s, 40, A.FP32, flags=A.FLAG_COMPENSATED)
