@@ -44,7 +44,7 @@ EXPORTED = [
     "asd_reset_magnetisation_stats", "asd_sq_setup", "asd_sq_sample", "asd_sq_get",
     "asd_sq_spectrum", "asd_tuning", "asd_set_launch_shape",
     "asd_time_kernels_cold", "asd_time_steps_cold", "asd_read_ucf", "asd_read_exch", "asd_read_csr_exch",
-    "asd_write_csr_exch", "asd_plan_spin_spans",
+    "asd_write_csr_exch", "asd_plan_spin_spans", "asd_set_device_layout",
 ]
 
 
@@ -145,6 +145,7 @@ def load_library(path: str = LIB_PATH):
         "asd_time_kernels_cold": ([P, C.c_uint64, C.c_uint64], C.c_int),
         "asd_time_steps_cold": ([P, C.c_uint64, C.c_uint64, dp, C.POINTER(C.c_uint64)], C.c_int),
         "asd_set_launch_shape": ([P, C.c_uint32, C.c_uint32], C.c_int),
+        "asd_set_device_layout": ([P, C.c_uint32], C.c_int),
         "asd_sq_spectrum": ([P, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                              dp, dp, C.c_size_t, u32p, u32p], C.c_int),
         "asd_build_csr": ([u32p, C.POINTER(C.c_int), C.c_uint32, dp, C.c_uint32, u32p, u32p, i32p, dp, C.c_double,
@@ -415,6 +416,10 @@ class Handle:
         buf = C.create_string_buffer(512)
         _check(load_library().asd_tuning(self.h, buf, len(buf)), self.h)
         return buf.value.decode()
+
+    def set_device_layout(self, layout: int):
+        """EXCH_DIA or EXCH_CSR (SELL-32) for a DIA matrix."""
+        _check(load_library().asd_set_device_layout(self.h, layout), self.h)
 
     def set_launch_shape(self, block: int, staging: int):
         """staging 0: none, 1: typed words, 2: typed words and neighbour spins."""

@@ -420,7 +420,7 @@ void configure_stage(asd_handle* h, int B, int mode) {
     h->block = B;
     h->sell.stage = 0;
     h->sell.stage_words = 0;
-    if (mode == 0 || !h->sell.typed || h->exch != ASD_EXCH_CSR) return;
+    if (mode == 0 || !h->sell.typed || h->dexch != ASD_EXCH_CSR) return;
     const size_t rb = h->p.precision == ASD_FP32 ? 4 : 8;
     const size_t tab = ((rb * (h->full ? 12 : 4) * h->sell.ntypes) + 15) & ~(size_t)15;
     const uint32_t w = stage_capacity(h, B);
@@ -436,28 +436,37 @@ void configure_stage(asd_handle* h, int B, int mode) {
 // Project autotuner: time the first stage kind of the step (it writes only scratch buffers)
 // for every block size in {64, 128, 256} with and without staging, keep the fastest.
 void autotune(asd_handle* h) {
-    struct Cand { int B; int mode; };
+    struct Cand { uint32_t layout; int B; int mode; };
     static const char* names[3] = {"direct", "words", "words+spins"};
     std::vector<Cand> cs;
-    for (int B : {64, 128, 256}) {
-        cs.push_back({B, 0});
-        if (h->sell.typed && h->exch == ASD_EXCH_CSR) { cs.push_back({B, 1}); cs.push_back({B, 2}); }
-    }
+    // DIA input also exists as SELL-32: both device layouts are candidates
+    std::vector<uint32_t> layouts{h->dexch};
+    if (h->exch == ASD_EXCH_DIA && h->sell.slice_ptr) layouts = {ASD_EXCH_CSR, ASD_EXCH_DIA};
+    for (uint32_t lay : layouts)
+        for (int B : {64, 128, 256}) {
+            cs.push_back({lay, B, 0});
+            if (h->sell.typed && lay == ASD_EXCH_CSR) { cs.push_back({lay, B, 1}); cs.push_back({lay, B, 2}); }
+        }
     double best = 1e300;
-    Cand bc{256, 1};
+    Cand bc{layouts[0], 256, 1};
     std::string log;
     char buf[96];
     for (const Cand& cd : cs) {
+        h->dexch = cd.layout;
         configure_stage(h, cd.B, cd.mode);
         if ((int)h->sell.stage != cd.mode) continue;
         float ms = 0.f;
         CK(time_first_stage(h, 2, 8, &ms));
-        std::snprintf(buf, sizeof buf, "%sB=%d/%s:%.4f", log.empty() ? "" : " ", cd.B, names[cd.mode], (double)ms);
+        std::snprintf(buf, sizeof buf, "%s%sB=%d/%s:%.4f", log.empty() ? "" : " ",
+                      layouts.size() > 1 ? (cd.layout == ASD_EXCH_CSR ? "SELL:" : "DIA:") : "", cd.B, names[cd.mode],
+                      (double)ms);
         log += buf;
         if (ms < best) { best = ms; bc = cd; }
     }
+    h->dexch = bc.layout;
     configure_stage(h, bc.B, bc.mode);
-    std::snprintf(buf, sizeof buf, "block=%d staging=%s; ", h->block, names[h->sell.stage]);
+    std::snprintf(buf, sizeof buf, "%sblock=%d staging=%s; ", layouts.size() > 1 ? (bc.layout == ASD_EXCH_CSR ? "layout=SELL " : "layout=DIA ") : "",
+                  h->block, names[h->sell.stage]);
     h->tune = std::string(buf) + "ms per stage launch: " + log;
 }
 
@@ -574,6 +583,7 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         const uint32_t n = h->n;
         if (s0.lr == ASD_LR_FFT) REQUIRE(h->exch == ASD_EXCH_FFT || h->exch == ASD_EXCH_NONE, "FFT field excludes CSR/DIA exchange");
         if (h->exch == ASD_EXCH_FFT) REQUIRE(s0.lr == ASD_LR_FFT, "exchange method fft needs lr = ASD_LR_FFT");
+        h->dexch = h->exch;
         REQUIRE(!(p.precision == ASD_FP64_FUSED && s0.lr != ASD_LR_NONE), "FP64 fused form has no long-range field; use FP64 plain");
         // material constants (src/llg.cpp:591-592, src/geom.cpp:244)
         StepConst& sc = h->sc;
@@ -821,6 +831,30 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
                     }
                     h->dia.vald = dupload(v.data(), v.size());
                 }
+                // the same matrix as SELL-32 for the fused kernels: rows take their entries in
+                // ascending diagonal order, the order the DIA gather sums them in
+                {
+                    std::vector<uint32_t> cx(n + 1, 0), ca;
+                    std::vector<double> cv;
+                    for (uint32_t i = 0; i < n; i++) {
+                        for (uint32_t d = 0; d < s0.ndiag; d++) {
+                            const int64_t col = (int64_t)i + doff[d];
+                            if (col < 0 || col >= (int64_t)n) continue;
+                            double v9[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+                            bool any = false;
+                            for (int q = 0; q < 9; q++) {
+                                const double* cp = dia_comp(q);
+                                if (cp) { v9[q] = cp[(size_t)d * n + i]; any |= v9[q] != 0.0; }
+                            }
+                            if (!any) continue;
+                            ca.push_back((uint32_t)col);
+                            cv.insert(cv.end(), v9, v9 + 9);
+                        }
+                        cx[i + 1] = (uint32_t)ca.size();
+                    }
+                    build_sell(h, cx, ca, cv);
+                    h->dexch = ASD_EXCH_CSR;
+                }
             }
         }
         // ---- site fields
@@ -1033,6 +1067,23 @@ int asd_set_launch_shape(asd_handle* h, uint32_t block, uint32_t staging) {
         char b[64];
         std::snprintf(b, sizeof b, "block=%d staging=%s (set)", h->block, names[h->sell.stage]);
         h->tune = b;
+        if (h->graph_steps) build_graph(h, h->graph_steps);
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_set_device_layout(asd_handle* h, uint32_t layout) {
+    if (!h) return ASD_EINVAL;
+    try {
+        REQUIRE(layout == ASD_EXCH_CSR || layout == ASD_EXCH_DIA, "layout must be ASD_EXCH_CSR or ASD_EXCH_DIA");
+        if (h->p.precision == ASD_FP64_PLAIN) return ASD_OK;
+        REQUIRE(layout == h->exch || (h->exch == ASD_EXCH_DIA && h->sell.slice_ptr),
+                "a CSR matrix has no DIA device layout");
+        CK(cudaSetDevice(h->device));
+        CK(cudaStreamSynchronize(h->stream));
+        h->dexch = layout;
+        configure_stage(h, h->block, h->sell.stage);
+        h->tune = std::string(layout == ASD_EXCH_CSR ? "layout=SELL " : "layout=DIA ") + h->tune;
         if (h->graph_steps) build_graph(h, h->graph_steps);
     } catch (const Fail& f) { return fail(h, f); }
     return ASD_OK;

@@ -356,8 +356,8 @@ double stage_bytes(const asd_handle* h, const StageArgs<R>& a, bool comp) {
     const double vb = sizeof(R), n = h->n;
     const double c = h->full ? 9.0 : 3.0;
     double m = 0.0;
-    if (h->exch == ASD_EXCH_CSR) m = 4.0 + h->nnz_per_row * (h->sell.typed ? 4.0 : 4.0 + vb * c);
-    else if (h->exch == ASD_EXCH_DIA) m = h->nnz_per_row * (h->dia.dtype ? 1.0 : vb * c);
+    if (h->dexch == ASD_EXCH_CSR) m = 4.0 + h->nnz_per_row * (h->sell.typed ? 4.0 : 4.0 + vb * c);
+    else if (h->dexch == ASD_EXCH_DIA) m = h->nnz_per_row * (h->dia.dtype ? 1.0 : vb * c);
     double st = 3 * vb;                                  // src spin (gathered once)
     const int kind = a.kind;
     const bool final_spin = kind == 2 || (kind >= 10 && kind - 10 == a.nst - 1);
@@ -435,9 +435,9 @@ cudaError_t launch_stage_t(asd_handle* hd, const StageArgs<R>& a) {
 
 template <typename R, bool COMP>
 cudaError_t launch_stage(asd_handle* hd, const StageArgs<R>& a) {
-    if (hd->exch == ASD_EXCH_CSR) {
+    if (hd->dexch == ASD_EXCH_CSR) {
         return hd->full ? launch_stage_t<R, ASD_EXCH_CSR, true, COMP>(hd, a) : launch_stage_t<R, ASD_EXCH_CSR, false, COMP>(hd, a);
-    } else if (hd->exch == ASD_EXCH_DIA) {
+    } else if (hd->dexch == ASD_EXCH_DIA) {
         return hd->full ? launch_stage_t<R, ASD_EXCH_DIA, true, COMP>(hd, a) : launch_stage_t<R, ASD_EXCH_DIA, false, COMP>(hd, a);
     }
     return launch_stage_t<R, ASD_EXCH_NONE, false, COMP>(hd, a);

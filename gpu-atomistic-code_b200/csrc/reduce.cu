@@ -154,11 +154,11 @@ cudaError_t field_t(asd_handle* h, double* out) {
     const float inv_p = h->lr.P ? 1.0f / (float)h->lr.P : 0.f;
     const unsigned g = nb(h->n, 256);
     const size_t cs = sizeof(R) * (h->full ? table_stride<true>() : table_stride<false>());
-    if (h->exch == ASD_EXCH_CSR) {
+    if (h->dexch == ASD_EXCH_CSR) {
         const size_t sm = h->sell.typed ? cs * h->sell.ntypes : 0;
         if (h->full) field_k<R, ASD_EXCH_CSR, true><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
         else field_k<R, ASD_EXCH_CSR, false><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
-    } else if (h->exch == ASD_EXCH_DIA) {
+    } else if (h->dexch == ASD_EXCH_DIA) {
         const size_t sm = h->dia.dtype ? cs * h->dia.ntypes : 0;
         if (h->full) field_k<R, ASD_EXCH_DIA, true><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
         else field_k<R, ASD_EXCH_DIA, false><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
