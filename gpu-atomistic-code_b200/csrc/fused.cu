@@ -109,15 +109,18 @@ __constant__ double FRK5B[5][5] = {
 __constant__ double FRK5C[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
 __constant__ double FRK4C[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
 
-// FP32 kernels are capped at 51 registers (5 blocks of 256 per SM, no spills);
-// the FP64 kernels keep the default cap.
-template <typename R>
-struct MinBlocks { static constexpr int value = sizeof(R) == 4 ? 5 : 1; };
+// Register caps of the FP32 kernels, chosen from ptxas reports so that none spills: 6 blocks
+// of 256 per SM (40 registers) for the full-tensor SELL and field-only kernels, 5 (48) for the
+// rest; the FP64 kernels keep the default cap.
+template <typename R, int EX, bool FULL>
+struct MinBlocks {
+    static constexpr int value = sizeof(R) != 4 ? 1 : ((EX == ASD_EXCH_CSR && FULL) || EX == ASD_EXCH_NONE) ? 6 : 5;
+};
 
 // K: the stage kind at compile time (1 Heun predictor, 2 Heun corrector, 3 RK stage before the
 // last, 4 last RK stage); a.kind still carries the RK stage index.
 template <typename R, int EX, bool FULL, bool COMP, int K>
-__global__ void __launch_bounds__(256, MinBlocks<R>::value)
+__global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
     stage_kernel(const StepConst c, const SellDev sell, const DiaDev dia, const StageArgs<R> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t stage_bar;
