@@ -289,7 +289,7 @@ class Handle:
         h = C.c_void_p()
         rc = lib.asd_create(C.byref(self._cp), csys, len(systems), C.byref(h))
         if rc != ASD_OK:
-            raise AsdError(rc, "asd_create failed")
+            raise AsdError(rc, "asd_create failed: " + (lib.asd_last_error(None) or b"").decode(errors="replace"))
         self.h = h
         self._keep = None
         ns = C.c_uint32()

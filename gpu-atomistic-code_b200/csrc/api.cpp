@@ -536,7 +536,11 @@ extern "C" {
 
 const char* asd_version(void) { return "asd-b200 0.1 (sm_100a)"; }
 
-const char* asd_last_error(const asd_handle* h) { return h ? h->err.c_str() : "null handle"; }
+namespace {
+thread_local std::string g_create_err;   // message of the calling thread's last failed asd_create
+}
+
+const char* asd_last_error(const asd_handle* h) { return h ? h->err.c_str() : g_create_err.c_str(); }
 
 int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_handle** out) {
     if (!out) return ASD_EINVAL;
@@ -930,11 +934,10 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         }
         CK(cudaStreamSynchronize(h->stream));
     } catch (const Fail& f) {
-        std::string msg = f.msg;
+        g_create_err = f.msg;
         int code = f.code;
         free_all(h);
         delete h;
-        (void)msg;
         return code;
     }
     *out = h;

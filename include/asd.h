@@ -130,6 +130,7 @@ typedef struct asd_handle asd_handle;
 int asd_create(const asd_params* p, const asd_system* sys, uint32_t nsys, asd_handle** out);
 /* cullg::deallocate_cuda_memory (src/cuda_util.cu:186-242). */
 int asd_destroy(asd_handle* h);
+/* Message of the last failure on h; with h == NULL, of the calling thread's last failed asd_create. */
 const char* asd_last_error(const asd_handle* h);
 const char* asd_version(void);
 
