@@ -317,13 +317,17 @@ class Handle:
         s = np.ascontiguousarray(s, dtype=np.float64).reshape(-1)
         _check(load_library().asd_set_spins(self.h, _p(s, C.c_double), len(s) // 3), self.h)
 
-    def _read(self, fn):
-        out = np.empty(3 * self.n, dtype=np.float64)
-        _check(fn(self.h, _p(out, C.c_double), self.n), self.h)
+    def _read(self, fn, out=None):
+        if out is None:
+            out = np.empty(3 * self.n, dtype=np.float64)
+        if out.dtype != np.float64 or out.size != 3 * self.n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of 3*nspins")
+        _check(fn(self.h, _p(out.reshape(-1), C.c_double), self.n), self.h)
         return out.reshape(self.n, 3)
 
-    def get_spins(self):
-        return self._read(load_library().asd_get_spins)
+    def get_spins(self, out=None):
+        """Spins [n, 3]; `out` (contiguous float64, e.g. pinned host memory) is filled if given."""
+        return self._read(load_library().asd_get_spins, out)
 
     def get_det_field(self):
         return self._read(load_library().asd_get_det_field)
@@ -425,9 +429,11 @@ class Handle:
         """staging 0: none, 1: typed words, 2: typed words and neighbour spins."""
         _check(load_library().asd_set_launch_shape(self.h, block, int(staging)), self.h)
 
-    def magnetisation(self):
-        out = np.empty(self.nrep * self.nsub * 3, dtype=np.float64)
-        _check(load_library().asd_magnetisation(self.h, _p(out, C.c_double), len(out)), self.h)
+    def magnetisation(self, out=None):
+        if out is None:
+            out = np.empty(self.nrep * self.nsub * 3, dtype=np.float64)
+        flat = out.reshape(-1)
+        _check(load_library().asd_magnetisation(self.h, _p(flat, C.c_double), len(flat)), self.h)
         return out.reshape(self.nrep, self.nsub, 3)
 
     def time_steps(self, n: int):
