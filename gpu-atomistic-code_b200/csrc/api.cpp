@@ -67,7 +67,7 @@ void free_all(asd_handle* h) {
         F(h->nzf[c]); F(h->nzd[c]);
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
-    F(h->d_err);
+    F(h->d_err); F(h->d_aos);
     F(h->sell.lwords); F(h->sell.span_ptr); F(h->sell.spans);
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
     F(h->sell.typed); F(h->sell.tab_f); F(h->sell.tab_d);
@@ -953,6 +953,13 @@ int asd_destroy(asd_handle* h) {
     return ASD_OK;
 }
 
+// Device staging buffer of 3N doubles for the spin / field transfers, allocated on first use
+// and kept (no allocation or device-wide synchronisation per call).
+static double* aos_buffer(asd_handle* h) {
+    if (!h->d_aos) h->d_aos = dalloc<double>(3 * (size_t)h->n);
+    return h->d_aos;
+}
+
 int asd_set_spins(asd_handle* h, const double* s, size_t n_spins) {
     if (!h) return ASD_EINVAL;
     try {
@@ -973,10 +980,10 @@ int asd_set_spins(asd_handle* h, const double* s, size_t n_spins) {
             CK(cudaMemcpyAsync(h->p_s, v.data(), v.size() * 8, cudaMemcpyHostToDevice, h->stream));
             CK(cudaStreamSynchronize(h->stream));
         } else {
-            double* d = dupload(s, 3 * n_spins);
-            cudaError_t e = launch_convert_spins_in(h, d);
+            double* d = aos_buffer(h);
+            cudaError_t e = cudaMemcpyAsync(d, s, 3 * n_spins * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+            if (e == cudaSuccess) e = launch_convert_spins_in(h, d);
             cudaError_t e2 = cudaStreamSynchronize(h->stream);
-            cudaFree(d);
             CK(e);
             CK(e2);
             h->lr_scattered = false;
@@ -995,11 +1002,10 @@ static int read_back(asd_handle* h, int what, double* out, size_t n_spins) {
             CK(cudaStreamSynchronize(h->stream));
             return ASD_OK;
         }
-        double* d = dalloc<double>(3 * n_spins);
+        double* d = aos_buffer(h);
         cudaError_t e = what == 2 ? launch_field_only(h, d) : launch_convert_out(h, what, d);
         if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, h->stream);
         cudaError_t e2 = cudaStreamSynchronize(h->stream);
-        cudaFree(d);
         CK(e);
         CK(e2);
     } catch (const Fail& f) { return fail(h, f); }
