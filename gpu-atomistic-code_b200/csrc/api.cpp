@@ -329,7 +329,7 @@ void setup_lr(asd_handle* h, const asd_system& s, bool plain) {
         const uint32_t mz = L.mesh[2];
         // pruned transform when the last axis is a power of two: z transforms only for the rows
         // of the spins' box, 2D transforms of the (x, y) planes by cuFFT
-        L.pruned = (mz >= 4 && mz <= 4096 && (mz & (mz - 1)) == 0 && h->n > 0) ? 1 : 0;
+        L.pruned = (mz >= 4 && mz <= 2048 && (mz & (mz - 1)) == 0 && h->n > 0) ? 1 : 0;   // z-pass smem <= 45 KB
         if (L.pruned) {
             for (int a = 0; a < 3; a++) { L.box0[a] = lo[a]; L.box1[a] = hi[a]; }
             L.k1 = dalloc<float2>(3 * L.Pk);

@@ -103,7 +103,7 @@ __global__ void real_to_cplx(size_t m, const double* __restrict__ r, double2* __
 // ---- pruned transform along z: M = mesh[2] = 2N real points per row, N complex points
 // z_n = x_2n + i x_2n+1 per row, radix-2 decimation in time in shared memory.
 struct ZPass {
-    uint32_t m0, m1, mz, N, logN, Kz, TY;
+    uint32_t m0, m1, mz, N, logN, Kz, TY, logTY;
     uint32_t bx0, by0, by1, bz0, bz1;   // box: x from bx0 (grid y), y in [by0, by1], z in [bz0, bz1]
     size_t P, Pk;                       // padded real points; spectrum points Kz*m0*m1
 };
@@ -115,12 +115,12 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
 // In-place radix-2 FFT of TY rows of N points (stride ld) already in bit-reversed order;
 // tw[j] = exp(-2 pi i j / N), conjugated for the inverse.
 __device__ __forceinline__ void smem_fft(float2* s, uint32_t ld, const float2* tw, const ZPass& A, bool inv) {
-    const uint32_t half_n = A.N / 2;
+    const uint32_t half_n = A.N / 2, lhn = A.logN - 1;
     for (uint32_t len = 2, lg = 1; len <= A.N; len <<= 1, lg++) {
         const uint32_t half = len >> 1, step = A.N >> lg;
         for (uint32_t b = threadIdx.x; b < A.TY * half_n; b += blockDim.x) {
-            const uint32_t r = b / half_n, q = b % half_n;
-            const uint32_t g = q / half, j = q % half;
+            const uint32_t r = b >> lhn, q = b & (half_n - 1);
+            const uint32_t g = q >> (lg - 1), j = q & (half - 1);
             const uint32_t i0 = r * ld + g * len + j, i1 = i0 + half;
             float2 w = tw[j * step];
             if (inv) w.y = -w.y;
@@ -132,11 +132,17 @@ __device__ __forceinline__ void smem_fft(float2* s, uint32_t ld, const float2* t
     }
 }
 
+// tw[j] = exp(-2 pi i j / N) for j < N/2, then ws[k] = exp(-i pi k / N) for k <= N at tw + N/2
 __device__ __forceinline__ void load_twiddles(float2* tw, uint32_t N) {
     for (uint32_t j = threadIdx.x; j < N / 2; j += blockDim.x) {
         float sn, cs;
         sincospif(-2.0f * (float)j / (float)N, &sn, &cs);
         tw[j] = make_float2(cs, sn);
+    }
+    for (uint32_t k = threadIdx.x; k <= N; k += blockDim.x) {
+        float sn, cs;
+        sincospif(-(float)k / (float)N, &sn, &cs);
+        tw[N / 2 + k] = make_float2(cs, sn);
     }
 }
 
@@ -150,7 +156,7 @@ __global__ void zpass_r2c(const float* __restrict__ mr, float2* __restrict__ k1,
     load_twiddles(tw, A.N);
     const float2* row0 = reinterpret_cast<const float2*>(mr + (size_t)c * A.P);
     for (uint32_t e = threadIdx.x; e < A.TY * A.N; e += blockDim.x) {
-        const uint32_t r = e / A.N, n = e % A.N, y = y0 + r;
+        const uint32_t r = e >> A.logN, n = e & (A.N - 1), y = y0 + r;
         float2 v = make_float2(0.f, 0.f);
         if (y <= A.by1 && 2 * n + 1 >= A.bz0 && 2 * n <= A.bz1)
             v = row0[(((size_t)x * A.m1 + y) * A.mz) / 2 + n];
@@ -159,15 +165,14 @@ __global__ void zpass_r2c(const float* __restrict__ mr, float2* __restrict__ k1,
     __syncthreads();
     smem_fft(zs, ld, tw, A, false);
     // X_k = E_k + w^k O_k, E = (Z_k + conj Z_{N-k}) / 2, O = -i (Z_k - conj Z_{N-k}) / 2, w = e^{-i pi / N}
+    const float2* ws = tw + A.N / 2;
     for (uint32_t e = threadIdx.x; e < (A.N + 1) * A.TY; e += blockDim.x) {
-        const uint32_t k = e / A.TY, r = e % A.TY, y = y0 + r;
+        const uint32_t k = e >> A.logTY, r = e & (A.TY - 1), y = y0 + r;
         if (y > A.by1) continue;
         const float2 zk = zs[r * ld + (k & (A.N - 1))], zm = zs[r * ld + ((A.N - k) & (A.N - 1))];
         const float2 E = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
         const float2 O = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
-        float sn, cs;
-        sincospif(-(float)k / (float)A.N, &sn, &cs);
-        const float2 wo = cmul(make_float2(cs, sn), O);
+        const float2 wo = cmul(ws[k], O);
         k1[(((size_t)c * A.Kz + k) * A.m0 + x) * A.m1 + y] = make_float2(E.x + wo.x, E.y + wo.y);
     }
 }
@@ -182,26 +187,25 @@ __global__ void zpass_c2r(const float2* __restrict__ k2, float* __restrict__ hr,
     const uint32_t c = blockIdx.z, x = A.bx0 + blockIdx.y, y0 = A.by0 + blockIdx.x * A.TY;
     load_twiddles(tw, A.N);
     for (uint32_t e = threadIdx.x; e < (A.N + 1) * A.TY; e += blockDim.x) {
-        const uint32_t k = e / A.TY, r = e % A.TY, y = y0 + r;
+        const uint32_t k = e >> A.logTY, r = e & (A.TY - 1), y = y0 + r;
         xs[r * ldx + k] = y <= A.by1 ? k2[(((size_t)c * A.Kz + k) * A.m0 + x) * A.m1 + y] : make_float2(0.f, 0.f);
     }
     __syncthreads();
     // Z_k = (X_k + conj X_{N-k}) + i e^{+i pi k / N} (X_k - conj X_{N-k}), k < N, bit-reversed
+    const float2* ws = tw + A.N / 2;
     for (uint32_t e = threadIdx.x; e < A.TY * A.N; e += blockDim.x) {
-        const uint32_t r = e / A.N, k = e % A.N;
+        const uint32_t r = e >> A.logN, k = e & (A.N - 1);
         const float2 xk = xs[r * ldx + k], xm = xs[r * ldx + (A.N - k)];
         const float2 sp = make_float2(xk.x + xm.x, xk.y - xm.y);
         const float2 df = make_float2(xk.x - xm.x, xk.y + xm.y);
-        float sn, cs;
-        sincospif((float)k / (float)A.N, &sn, &cs);
-        const float2 t = cmul(make_float2(cs, sn), df);
+        const float2 t = cmul(make_float2(ws[k].x, -ws[k].y), df);          // e^{+i pi k / N}
         s[r * ld + (__brev(k) >> (32 - A.logN))] = make_float2(sp.x - t.y, sp.y + t.x);
     }
     __syncthreads();
     smem_fft(s, ld, tw, A, true);
     float2* out0 = reinterpret_cast<float2*>(hr + (size_t)c * A.P);
     for (uint32_t e = threadIdx.x; e < A.TY * A.N; e += blockDim.x) {
-        const uint32_t r = e / A.N, n = e % A.N, y = y0 + r;
+        const uint32_t r = e >> A.logN, n = e & (A.N - 1), y = y0 + r;
         if (y > A.by1 || 2 * n + 1 < A.bz0 || 2 * n > A.bz1) continue;
         out0[(((size_t)x * A.m1 + y) * A.mz) / 2 + n] = s[r * ld + n];
     }
@@ -225,7 +229,9 @@ ZPass zpass_args(const LongRange& L) {
     A.logN = 0;
     while ((1u << A.logN) < A.N) A.logN++;
     A.Kz = A.N + 1;
-    A.TY = A.N >= 2048 ? 1 : std::min<uint32_t>(32, 2048 / A.N);
+    A.TY = A.N >= 2048 ? 1 : std::min<uint32_t>(32, 2048 / A.N);   // a power of two
+    A.logTY = 0;
+    while ((1u << A.logTY) < A.TY) A.logTY++;
     A.bx0 = L.box0[0]; A.by0 = L.box0[1]; A.by1 = L.box1[1]; A.bz0 = L.box0[2]; A.bz1 = L.box1[2];
     A.P = L.P; A.Pk = (size_t)A.Kz * A.m0 * A.m1;
     return A;
@@ -236,8 +242,9 @@ ZPass zpass_args(const LongRange& L) {
 // Pruned-transform sizes: shared memory of the two z-pass kernels.
 size_t zpass_smem(const LongRange& L, bool inverse) {
     const ZPass A = zpass_args(L);
-    if (!inverse) return sizeof(float2) * ((size_t)A.TY * (A.N + 1) + A.N / 2);
-    return sizeof(float2) * ((size_t)A.TY * (A.N + 2) + (size_t)A.TY * (A.N + 1) + A.N / 2);
+    const size_t tws = A.N / 2 + A.N + 1;                 // FFT twiddles + split twiddles
+    if (!inverse) return sizeof(float2) * ((size_t)A.TY * (A.N + 1) + tws);
+    return sizeof(float2) * ((size_t)A.TY * (A.N + 2) + (size_t)A.TY * (A.N + 1) + tws);
 }
 
 cudaError_t permute_nk_pruned(asd_handle* h) {
