@@ -67,7 +67,7 @@ void free_all(asd_handle* h) {
         F(h->nzf[c]); F(h->nzd[c]);
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
-    F(h->d_err); F(h->d_aos);
+    F(h->d_err); F(h->d_aos); F(h->d_rep_of_tile);
     F(h->sell.lwords); F(h->sell.span_ptr); F(h->sell.spans);
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
     F(h->sell.typed); F(h->sell.tab_f); F(h->sell.tab_d);
@@ -649,6 +649,16 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         sc.rep_sqrtT_f = h->d_rep_sqrtT_f;
         h->d_rep_stream = dupload(strm.data(), nsys);
         sc.rep_off = h->d_rep_off; sc.rep_sqrtT = h->d_rep_sqrtT; sc.rep_stream = h->d_rep_stream;
+        {
+            std::vector<uint32_t> rt((n + 31) / 32);
+            uint32_t r = 0;
+            for (size_t t = 0; t < rt.size(); t++) {
+                while (r + 1 < nsys && h->h_rep_off[r + 1] <= 32 * t) r++;
+                rt[t] = r;
+            }
+            h->d_rep_of_tile = dupload(rt.data(), rt.size());
+            sc.rep_of_tile = h->d_rep_of_tile;
+        }
         std::vector<double> dyn(DYN_COUNT, 0.0);
         for (int a = 0; a < 3; a++) dyn[DYN_APPLIED + a] = p.applied[a];
         dyn[DYN_STAG_SCALE] = 1.0;

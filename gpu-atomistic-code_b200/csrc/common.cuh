@@ -38,6 +38,7 @@ struct StepConst {
     uint64_t seed;
     const uint32_t* atom;      // per-spin unit-cell atom or nullptr (-> i % nmat)
     const uint32_t* rep_off;   // nrep+1
+    const uint32_t* rep_of_tile; // replica of the first spin of every 32-spin tile
     const double* rep_sqrtT;   // nrep: sqrt(T) per replica
     const uint32_t* rep_stream;
     const double* dyn;         // mutable scalars, see DYN_*
@@ -79,13 +80,13 @@ __device__ __forceinline__ uint32_t atom_of(const StepConst& c, uint32_t i) {
     return c.atom ? c.atom[i] : (c.nmat == 1 ? 0u : i % c.nmat);
 }
 
+// Replica of spin i: the replica of its 32-spin tile's first spin, advanced past the replica
+// boundaries that lie inside the tile (none unless a replica is shorter than the tile).
 __device__ __forceinline__ uint32_t replica_of(const StepConst& c, uint32_t i) {
-    uint32_t lo = 0, hi = c.nrep;
-    while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (__ldg(c.rep_off + mid) <= i) lo = mid; else hi = mid;
-    }
-    return lo;
+    if (c.nrep == 1) return 0;
+    uint32_t r = __ldg(c.rep_of_tile + (i >> 5));
+    while (r + 1 < c.nrep && __ldg(c.rep_off + r + 1) <= i) r++;
+    return r;
 }
 
 // ---------------------------------------------------------------------------

@@ -101,7 +101,9 @@ __global__ void real_to_cplx(size_t m, const double* __restrict__ r, double2* __
 }
 
 // ---- pruned transform along z: M = mesh[2] = 2N real points per row, N complex points
-// z_n = x_2n + i x_2n+1 per row, radix-2 decimation in time in shared memory.
+// z_n = x_2n + i x_2n+1 per row.  N = N1 * N2 in {4, ..., 256} runs as two register passes
+// (Cooley-Tukey: N1-point DFTs of the N2 strided subsequences, twiddle, N2-point DFTs); other
+// sizes use a radix-2 pass per stage in shared memory.
 struct ZPass {
     uint32_t m0, m1, mz, N, logN, Kz, TY, logTY;
     uint32_t bx0, by0, by1, bz0, bz1;   // box: x from bx0 (grid y), y in [by0, by1], z in [bz0, bz1]
@@ -112,9 +114,24 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
     return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// In-place radix-2 FFT of TY rows of N points (stride ld) already in bit-reversed order;
-// tw[j] = exp(-2 pi i j / N), conjugated for the inverse.
-__device__ __forceinline__ void smem_fft(float2* s, uint32_t ld, const float2* tw, const ZPass& A, bool inv) {
+// tw[j] = exp(-2 pi i j / N) for j < N, then the split twiddles ws[k] = exp(-i pi k / N) for
+// k <= N at tw + N.
+__device__ __forceinline__ void load_twiddles(float2* tw, uint32_t N) {
+    for (uint32_t j = threadIdx.x; j < N; j += blockDim.x) {
+        float sn, cs;
+        sincospif(-2.0f * (float)j / (float)N, &sn, &cs);
+        tw[j] = make_float2(cs, sn);
+    }
+    for (uint32_t k = threadIdx.x; k <= N; k += blockDim.x) {
+        float sn, cs;
+        sincospif(-(float)k / (float)N, &sn, &cs);
+        tw[N + k] = make_float2(cs, sn);
+    }
+}
+
+// In-place radix-2 FFT of TY rows of N points (stride ld) already in bit-reversed order.
+template <bool INV>
+__device__ __forceinline__ void smem_fft(float2* s, uint32_t ld, const float2* tw, const ZPass& A) {
     const uint32_t half_n = A.N / 2, lhn = A.logN - 1;
     for (uint32_t len = 2, lg = 1; len <= A.N; len <<= 1, lg++) {
         const uint32_t half = len >> 1, step = A.N >> lg;
@@ -123,7 +140,7 @@ __device__ __forceinline__ void smem_fft(float2* s, uint32_t ld, const float2* t
             const uint32_t g = q >> (lg - 1), j = q & (half - 1);
             const uint32_t i0 = r * ld + g * len + j, i1 = i0 + half;
             float2 w = tw[j * step];
-            if (inv) w.y = -w.y;
+            if (INV) w.y = -w.y;
             const float2 u = s[i0], v = cmul(s[i1], w);
             s[i0] = make_float2(u.x + v.x, u.y + v.y);
             s[i1] = make_float2(u.x - v.x, u.y - v.y);
@@ -132,25 +149,94 @@ __device__ __forceinline__ void smem_fft(float2* s, uint32_t ld, const float2* t
     }
 }
 
-// tw[j] = exp(-2 pi i j / N) for j < N/2, then ws[k] = exp(-i pi k / N) for k <= N at tw + N/2
-__device__ __forceinline__ void load_twiddles(float2* tw, uint32_t N) {
-    for (uint32_t j = threadIdx.x; j < N / 2; j += blockDim.x) {
-        float sn, cs;
-        sincospif(-2.0f * (float)j / (float)N, &sn, &cs);
-        tw[j] = make_float2(cs, sn);
+template <int R>
+__device__ __forceinline__ constexpr int brev_c(int k) {
+    int r = 0;
+    for (int b = 1, o = R >> 1; b < R; b <<= 1, o >>= 1)
+        if (k & b) r |= o;
+    return r;
+}
+
+// R-point DFT in registers (radix-2, decimation in time); the twiddle of a length-len
+// butterfly is w_len^j = tw[j N / len].
+template <int R, bool INV>
+__device__ __forceinline__ void reg_dft(float2 (&v)[R], const float2* tw, uint32_t N) {
+    float2 a[R];
+#pragma unroll
+    for (int k = 0; k < R; k++) a[brev_c<R>(k)] = v[k];
+#pragma unroll
+    for (int len = 2; len <= R; len <<= 1) {
+        const uint32_t step = N / (uint32_t)len;
+#pragma unroll
+        for (int g = 0; g < R; g += len)
+#pragma unroll
+            for (int j = 0; j < len / 2; j++) {
+                float2 t = a[g + j + len / 2];
+                if (j != 0) {
+                    float2 w = tw[j * step];
+                    if (INV) w.y = -w.y;
+                    t = cmul(t, w);
+                }
+                const float2 u = a[g + j];
+                a[g + j] = make_float2(u.x + t.x, u.y + t.y);
+                a[g + j + len / 2] = make_float2(u.x - t.x, u.y - t.y);
+            }
     }
-    for (uint32_t k = threadIdx.x; k <= N; k += blockDim.x) {
-        float sn, cs;
-        sincospif(-(float)k / (float)N, &sn, &cs);
-        tw[N / 2 + k] = make_float2(cs, sn);
+#pragma unroll
+    for (int k = 0; k < R; k++) v[k] = a[k];
+}
+
+// N = N1 N2 point DFT of TY rows (natural order in and out, in place), TY * max(N1, N2) <= 256:
+// X[m + N1 q] = sum_t w_N2^{t q} w_N^{t m} sum_k w_N1^{k m} z[t + N2 k].
+template <int N1, int N2, bool INV>
+__device__ __forceinline__ void fft2pass(float2* s, uint32_t ld, const float2* tw, uint32_t TY) {
+    constexpr uint32_t N = N1 * N2;
+    {
+        const uint32_t it = threadIdx.x, r = it / N2, t = it % N2;
+        const bool act = it < TY * N2;
+        float2 v[N1];
+        if (act) {
+#pragma unroll
+            for (int k = 0; k < N1; k++) v[k] = s[r * ld + t + N2 * k];
+            reg_dft<N1, INV>(v, tw, N);
+#pragma unroll
+            for (int m = 1; m < N1; m++) {
+                float2 w = tw[t * m];
+                if (INV) w.y = -w.y;
+                v[m] = cmul(v[m], w);
+            }
+        }
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int m = 0; m < N1; m++) s[r * ld + m * N2 + t] = v[m];
+        }
+        __syncthreads();
+    }
+    {
+        const uint32_t it = threadIdx.x, r = it / N1, m = it % N1;
+        const bool act = it < TY * N1;
+        float2 u[N2];
+        if (act) {
+#pragma unroll
+            for (int t = 0; t < N2; t++) u[t] = s[r * ld + m * N2 + t];
+            reg_dft<N2, INV>(u, tw, N);
+        }
+        __syncthreads();
+        if (act) {
+#pragma unroll
+            for (int q = 0; q < N2; q++) s[r * ld + m + N1 * q] = u[q];
+        }
+        __syncthreads();
     }
 }
 
 // M_r rows (c, x, y in the box) -> half spectrum k1[c][kz][x][y], kz = 0..N.
-// grid: (y tiles of TY rows, box rows in x, 3 components).
+// grid: (y tiles of TY rows, box rows in x, 3 components).  N1 = 0: radix-2 fallback.
+template <int N1, int N2>
 __global__ void zpass_r2c(const float* __restrict__ mr, float2* __restrict__ k1, const ZPass A) {
     extern __shared__ float2 zs[];
-    const uint32_t ld = A.N + 1;
+    const uint32_t ld = A.N + 2;
     float2* tw = zs + A.TY * ld;
     const uint32_t c = blockIdx.z, x = A.bx0 + blockIdx.y, y0 = A.by0 + blockIdx.x * A.TY;
     load_twiddles(tw, A.N);
@@ -160,12 +246,14 @@ __global__ void zpass_r2c(const float* __restrict__ mr, float2* __restrict__ k1,
         float2 v = make_float2(0.f, 0.f);
         if (y <= A.by1 && 2 * n + 1 >= A.bz0 && 2 * n <= A.bz1)
             v = row0[(((size_t)x * A.m1 + y) * A.mz) / 2 + n];
-        zs[r * ld + (__brev(n) >> (32 - A.logN))] = v;
+        if constexpr (N1 > 0) zs[r * ld + n] = v;
+        else zs[r * ld + (__brev(n) >> (32 - A.logN))] = v;
     }
     __syncthreads();
-    smem_fft(zs, ld, tw, A, false);
+    if constexpr (N1 > 0) fft2pass<N1, N2, false>(zs, ld, tw, A.TY);
+    else smem_fft<false>(zs, ld, tw, A);
     // X_k = E_k + w^k O_k, E = (Z_k + conj Z_{N-k}) / 2, O = -i (Z_k - conj Z_{N-k}) / 2, w = e^{-i pi / N}
-    const float2* ws = tw + A.N / 2;
+    const float2* ws = tw + A.N;
     for (uint32_t e = threadIdx.x; e < (A.N + 1) * A.TY; e += blockDim.x) {
         const uint32_t k = e >> A.logTY, r = e & (A.TY - 1), y = y0 + r;
         if (y > A.by1) continue;
@@ -177,37 +265,59 @@ __global__ void zpass_r2c(const float* __restrict__ mr, float2* __restrict__ k1,
     }
 }
 
+// Z'_k = (X_k + conj X_{N-k}) + i e^{+i pi k / N} (X_k - conj X_{N-k}): twice the spectrum of
+// z_n = x_2n + i x_2n+1, so that the unnormalised inverse gives 2N x (cuFFT's C2R scaling).
+__device__ __forceinline__ float2 c2r_pre(float2 xk, float2 xm, float2 wsk) {
+    const float2 sp = make_float2(xk.x + xm.x, xk.y - xm.y);
+    const float2 df = make_float2(xk.x - xm.x, xk.y + xm.y);
+    const float2 t = cmul(make_float2(wsk.x, -wsk.y), df);
+    return make_float2(sp.x - t.y, sp.y + t.x);
+}
+
 // Spectrum k2[c][kz][x][y] of the box rows -> H_r rows, unnormalised like cuFFT's C2R.
+template <int N1, int N2>
 __global__ void zpass_c2r(const float2* __restrict__ k2, float* __restrict__ hr, const ZPass A) {
     extern __shared__ float2 zs[];
-    const uint32_t ldx = A.N + 2, ld = A.N + 1;
-    float2* xs = zs;                         // [TY][N+1] spectrum rows
-    float2* s = zs + A.TY * ldx;             // [TY][N] complex rows for the inverse FFT
-    float2* tw = s + A.TY * ld;
+    const uint32_t ld = A.N + 2;
     const uint32_t c = blockIdx.z, x = A.bx0 + blockIdx.y, y0 = A.by0 + blockIdx.x * A.TY;
+    float2* s = zs;                          // [TY][N+2]: spectrum rows, then Z' in place
+    float2* xs2 = zs + A.TY * ld;            // fallback only: [TY][N+1] bit-reversed Z'
+    float2* tw = N1 > 0 ? xs2 : xs2 + A.TY * (A.N + 1);
     load_twiddles(tw, A.N);
     for (uint32_t e = threadIdx.x; e < (A.N + 1) * A.TY; e += blockDim.x) {
         const uint32_t k = e >> A.logTY, r = e & (A.TY - 1), y = y0 + r;
-        xs[r * ldx + k] = y <= A.by1 ? k2[(((size_t)c * A.Kz + k) * A.m0 + x) * A.m1 + y] : make_float2(0.f, 0.f);
+        s[r * ld + k] = y <= A.by1 ? k2[(((size_t)c * A.Kz + k) * A.m0 + x) * A.m1 + y] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    // Z_k = (X_k + conj X_{N-k}) + i e^{+i pi k / N} (X_k - conj X_{N-k}), k < N, bit-reversed
-    const float2* ws = tw + A.N / 2;
-    for (uint32_t e = threadIdx.x; e < A.TY * A.N; e += blockDim.x) {
-        const uint32_t r = e >> A.logN, k = e & (A.N - 1);
-        const float2 xk = xs[r * ldx + k], xm = xs[r * ldx + (A.N - k)];
-        const float2 sp = make_float2(xk.x + xm.x, xk.y - xm.y);
-        const float2 df = make_float2(xk.x - xm.x, xk.y + xm.y);
-        const float2 t = cmul(make_float2(ws[k].x, -ws[k].y), df);          // e^{+i pi k / N}
-        s[r * ld + (__brev(k) >> (32 - A.logN))] = make_float2(sp.x - t.y, sp.y + t.x);
+    const float2* ws = tw + A.N;
+    if constexpr (N1 > 0) {
+        // pairwise in place: thread (r, k) for k in [0, N/2] writes Z'_k and Z'_{N-k}
+        const uint32_t half = A.N / 2, nh = half + 1;
+        for (uint32_t e = threadIdx.x; e < A.TY * nh; e += blockDim.x) {
+            const uint32_t r = e / nh, k = e % nh;
+            const float2 xk = s[r * ld + k], xm = s[r * ld + (A.N - k)];
+            const float2 zk = c2r_pre(xk, xm, ws[k]);
+            if (k != 0 && k != half) s[r * ld + (A.N - k)] = c2r_pre(xm, xk, ws[A.N - k]);
+            s[r * ld + k] = zk;
+        }
+        __syncthreads();
+        fft2pass<N1, N2, true>(s, ld, tw, A.TY);
+    } else {
+        const uint32_t ld2 = A.N + 1;
+        for (uint32_t e = threadIdx.x; e < A.TY * A.N; e += blockDim.x) {
+            const uint32_t r = e >> A.logN, k = e & (A.N - 1);
+            xs2[r * ld2 + (__brev(k) >> (32 - A.logN))] = c2r_pre(s[r * ld + k], s[r * ld + (A.N - k)], ws[k]);
+        }
+        __syncthreads();
+        smem_fft<true>(xs2, ld2, tw, A);
+        s = xs2;
     }
-    __syncthreads();
-    smem_fft(s, ld, tw, A, true);
+    const uint32_t lds = N1 > 0 ? ld : A.N + 1;
     float2* out0 = reinterpret_cast<float2*>(hr + (size_t)c * A.P);
     for (uint32_t e = threadIdx.x; e < A.TY * A.N; e += blockDim.x) {
         const uint32_t r = e >> A.logN, n = e & (A.N - 1), y = y0 + r;
         if (y > A.by1 || 2 * n + 1 < A.bz0 || 2 * n > A.bz1) continue;
-        out0[(((size_t)x * A.m1 + y) * A.mz) / 2 + n] = s[r * ld + n];
+        out0[(((size_t)x * A.m1 + y) * A.mz) / 2 + n] = s[r * lds + n];
     }
 }
 
@@ -223,13 +333,24 @@ __global__ void permute_nk(size_t Pk, uint32_t ncomp, uint32_t m0, uint32_t m1, 
     out[q * Pk + (size_t)kz * m0 * m1 + xy] = in[e];
 }
 
+// (N1, N2) of the two-pass transform for N complex points, (0, 0) for the radix-2 fallback.
+void zpass_split(uint32_t N, int* n1, int* n2) {
+    static const int tab[][3] = {{4, 2, 2}, {8, 4, 2}, {16, 4, 4}, {32, 8, 4}, {64, 8, 8}, {128, 16, 8}, {256, 16, 16}};
+    *n1 = 0; *n2 = 0;
+    for (const auto& t : tab)
+        if ((uint32_t)t[0] == N) { *n1 = t[1]; *n2 = t[2]; }
+}
+
 ZPass zpass_args(const LongRange& L) {
     ZPass A{};
     A.m0 = L.mesh[0]; A.m1 = L.mesh[1]; A.mz = L.mesh[2]; A.N = A.mz / 2;
     A.logN = 0;
     while ((1u << A.logN) < A.N) A.logN++;
     A.Kz = A.N + 1;
-    A.TY = A.N >= 2048 ? 1 : std::min<uint32_t>(32, 2048 / A.N);   // a power of two
+    int n1, n2;
+    zpass_split(A.N, &n1, &n2);
+    if (n1) A.TY = 256 / (uint32_t)std::max(n1, n2);             // every thread busy in both passes
+    else A.TY = A.N >= 2048 ? 1 : std::min<uint32_t>(32, 2048 / A.N);
     A.logTY = 0;
     while ((1u << A.logTY) < A.TY) A.logTY++;
     A.bx0 = L.box0[0]; A.by0 = L.box0[1]; A.by1 = L.box1[1]; A.bz0 = L.box0[2]; A.bz1 = L.box1[2];
@@ -242,9 +363,39 @@ ZPass zpass_args(const LongRange& L) {
 // Pruned-transform sizes: shared memory of the two z-pass kernels.
 size_t zpass_smem(const LongRange& L, bool inverse) {
     const ZPass A = zpass_args(L);
-    const size_t tws = A.N / 2 + A.N + 1;                 // FFT twiddles + split twiddles
-    if (!inverse) return sizeof(float2) * ((size_t)A.TY * (A.N + 1) + tws);
-    return sizeof(float2) * ((size_t)A.TY * (A.N + 2) + (size_t)A.TY * (A.N + 1) + tws);
+    int n1, n2;
+    zpass_split(A.N, &n1, &n2);
+    const size_t tws = 2 * (size_t)A.N + 1;                 // FFT twiddles + split twiddles
+    const size_t rows = (size_t)A.TY * (A.N + 2);
+    if (!inverse || n1) return sizeof(float2) * (rows + tws);
+    return sizeof(float2) * (rows + (size_t)A.TY * (A.N + 1) + tws);
+}
+
+// Launch the z-pass of the right (N1, N2) instantiation.
+static cudaError_t zpass_run(asd_handle* h, bool inverse) {
+    LongRange& L = h->lr;
+    const ZPass A = zpass_args(L);
+    int n1, n2;
+    zpass_split(A.N, &n1, &n2);
+    const dim3 grid((A.by1 - A.by0 + A.TY) / A.TY, L.box1[0] - L.box0[0] + 1, 3);
+    const size_t sm = zpass_smem(L, inverse);
+    float* hr = L.r + 3 * L.P;
+#define ZP(a, b)                                                                                      \
+    if (inverse) zpass_c2r<a, b><<<grid, 256, sm, h->stream>>>(L.k2, hr, A);                          \
+    else zpass_r2c<a, b><<<grid, 256, sm, h->stream>>>(L.r, L.k1, A);
+    switch (A.N) {
+    case 4: ZP(2, 2) break;
+    case 8: ZP(4, 2) break;
+    case 16: ZP(4, 4) break;
+    case 32: ZP(8, 4) break;
+    case 64: ZP(8, 8) break;
+    case 128: ZP(16, 8) break;
+    case 256: ZP(16, 16) break;
+    default: ZP(0, 0) break;
+    }
+#undef ZP
+    h->launches += 1;
+    return cudaGetLastError();
 }
 
 cudaError_t permute_nk_pruned(asd_handle* h) {
@@ -281,17 +432,16 @@ cudaError_t launch_lr_eval_f32(asd_handle* h) {
     LongRange& L = h->lr;
     if (L.pruned) {
         const ZPass A = zpass_args(L);
-        const dim3 grid((A.by1 - A.by0 + A.TY) / A.TY, L.box1[0] - L.box0[0] + 1, 3);
-        zpass_r2c<<<grid, 256, zpass_smem(L, false), h->stream>>>(L.r, L.k1, A);
+        cudaError_t e = zpass_run(h, false);
+        if (e != cudaSuccess) return e;
         if (cufftExecC2C(L.c2c, (cufftComplex*)L.k1, (cufftComplex*)L.k2, CUFFT_FORWARD) != CUFFT_SUCCESS)
             return cudaErrorUnknown;
         if (L.ncomp == 6 && L.nk_real) kconv6r<<<nb(A.Pk, 256), 256, 0, h->stream>>>(A.Pk, L.nkr, L.k2);
         else kconv9c<<<nb(A.Pk, 256), 256, 0, h->stream>>>(A.Pk, L.nkc, L.k2);
+        h->launches += 1;
         if (cufftExecC2C(L.c2c, (cufftComplex*)L.k2, (cufftComplex*)L.k2, CUFFT_INVERSE) != CUFFT_SUCCESS)
             return cudaErrorUnknown;
-        zpass_c2r<<<grid, 256, zpass_smem(L, true), h->stream>>>(L.k2, L.r + 3 * L.P, A);
-        h->launches += 3;
-        return cudaGetLastError();
+        return zpass_run(h, true);
     }
     if (cufftExecR2C(L.r2c, (cufftReal*)L.r, (cufftComplex*)L.k) != CUFFT_SUCCESS) return cudaErrorUnknown;
     if (L.ncomp == 6 && L.nk_real) kconv6r<<<nb(L.Pk, 256), 256, 0, h->stream>>>(L.Pk, L.nkr, L.k);

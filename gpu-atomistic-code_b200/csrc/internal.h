@@ -168,6 +168,7 @@ struct asd_handle {
     std::vector<uint32_t> h_words;       // typed SELL words (host copy, for the local words)
     uint32_t* d_err = nullptr;           // device error bits (staging wait timeouts)
     double* d_aos = nullptr;             // [3N] staging buffer of the spin / field transfers
+    uint32_t* d_rep_of_tile = nullptr;   // replica of each 32-spin tile's first spin
     std::string tune;                    // autotuner result, "B=.. stage=.. (ms ...)"
     bool lr_scattered = false;
     double nnz_per_row = 0.0;

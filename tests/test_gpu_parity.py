@@ -144,9 +144,10 @@ def test_fp32_finite_temperature_close(gpu):
     assert maxdiff(g, o) <= 1e-5, maxdiff(g, o)
 
 
-# mesh 2L per axis: L = 6 takes the full 3D transform (last axis 12), (8, 6, 4) and (5, 7, 8)
-# the pruned one (last axis 8 / 16; odd box extents in x and y)
-@pytest.mark.parametrize("L", [6, (8, 6, 4), (5, 7, 8)])
+# mesh 2L per axis: L = 6 takes the full 3D transform (last axis 12); the others the pruned one
+# with N = m_z/2 = 4, 8 (odd box extents in x and y), 64, 128, 256 (two register passes) and 512
+# (radix-2 passes in shared memory)
+@pytest.mark.parametrize("L", [6, (8, 6, 4), (5, 7, 8), (6, 5, 64), (4, 3, 128), (2, 2, 256), (2, 2, 512)])
 def test_dipole_csr_plain_and_fp32(gpu, L):
     s = LT.sc_ferromagnet(L, pbc=(0, 0, 0), dipole=True)
     g, o, _, _ = pair(s, 40, A.FP64_PLAIN, update=1)
