@@ -44,7 +44,8 @@ EXPORTED = [
     "asd_reset_magnetisation_stats", "asd_sq_setup", "asd_sq_sample", "asd_sq_get",
     "asd_sq_spectrum", "asd_tuning", "asd_set_launch_shape",
     "asd_time_kernels_cold", "asd_time_steps_cold", "asd_read_ucf", "asd_read_exch", "asd_read_csr_exch",
-    "asd_write_csr_exch", "asd_plan_spin_spans", "asd_set_device_layout",
+    "asd_write_csr_exch", "asd_plan_spin_spans", "asd_set_device_layout", "asd_set_ttm",
+    "asd_get_ttm_temperatures",
 ]
 
 
@@ -57,6 +58,16 @@ class UcfAtom(C.Structure):
     _fields_ = [("sublattice", C.c_uint32), ("xred", C.c_double * 3), ("mesh_point", C.c_int32 * 3),
                 ("mu", C.c_double), ("damping", C.c_double), ("gamma", C.c_double), ("element", C.c_char * 16),
                 ("init_spin", C.c_double * 3), ("k1u", C.c_double), ("k1u_dir", C.c_double * 3)]
+
+
+TTM_MAX_PULSES = 16
+
+
+class Ttm(C.Structure):
+    _fields_ = [("gamma_e", C.c_double), ("Cl", C.c_double), ("G_ep", C.c_double), ("pump_time", C.c_double),
+                ("pump_fluence", C.c_double), ("cooling_time", C.c_double), ("initial_T", C.c_double),
+                ("npulses", C.c_uint32), ("bath_is_electrons", C.c_uint32),
+                ("pulse_scale", C.c_double * TTM_MAX_PULSES), ("pulse_delay", C.c_double * TTM_MAX_PULSES)]
 
 
 class Params(C.Structure):
@@ -146,6 +157,8 @@ def load_library(path: str = LIB_PATH):
         "asd_time_steps_cold": ([P, C.c_uint64, C.c_uint64, dp, C.POINTER(C.c_uint64)], C.c_int),
         "asd_set_launch_shape": ([P, C.c_uint32, C.c_uint32], C.c_int),
         "asd_set_device_layout": ([P, C.c_uint32], C.c_int),
+        "asd_set_ttm": ([P, C.c_void_p], C.c_int),
+        "asd_get_ttm_temperatures": ([P, dp, dp], C.c_int),
         "asd_sq_spectrum": ([P, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                              dp, dp, C.c_size_t, u32p, u32p], C.c_int),
         "asd_build_csr": ([u32p, C.POINTER(C.c_int), C.c_uint32, dp, C.c_uint32, u32p, u32p, i32p, dp, C.c_double,
@@ -420,6 +433,26 @@ class Handle:
         buf = C.create_string_buffer(512)
         _check(load_library().asd_tuning(self.h, buf, len(buf)), self.h)
         return buf.value.decode()
+
+    def set_ttm(self, gamma_e=None, Cl=None, G_ep=None, pump_time=None, pump_fluence=None, cooling_time=3000e-9,
+                initial_T=None, pulses=((1.0, 0.0),), bath_is_electrons=True, off=False):
+        """Start (or with off=True stop) the two-temperature model at the current step; pulses are
+        (scale, delay [s]) pairs."""
+        if off:
+            _check(load_library().asd_set_ttm(self.h, None), self.h)
+            return
+        m = Ttm()
+        m.gamma_e, m.Cl, m.G_ep, m.pump_time = gamma_e, Cl, G_ep, pump_time
+        m.pump_fluence, m.cooling_time, m.initial_T = pump_fluence, cooling_time, initial_T
+        m.npulses, m.bath_is_electrons = len(pulses), int(bath_is_electrons)
+        for q, (sc, dl) in enumerate(pulses):
+            m.pulse_scale[q], m.pulse_delay[q] = sc, dl
+        _check(load_library().asd_set_ttm(self.h, C.byref(m)), self.h)
+
+    def ttm_temperatures(self):
+        te, tl = C.c_double(), C.c_double()
+        _check(load_library().asd_get_ttm_temperatures(self.h, C.byref(te), C.byref(tl)), self.h)
+        return te.value, tl.value
 
     def set_device_layout(self, layout: int):
         """EXCH_DIA or EXCH_CSR (SELL-32) for a DIA matrix."""

@@ -67,7 +67,7 @@ void free_all(asd_handle* h) {
         F(h->nzf[c]); F(h->nzd[c]);
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
-    F(h->d_err); F(h->d_aos); F(h->d_rep_of_tile);
+    F(h->d_err); F(h->d_aos); F(h->d_rep_of_tile); F(h->d_ttm);
     F(h->sell.lwords); F(h->sell.span_ptr); F(h->sell.spans);
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
     F(h->sell.typed); F(h->sell.tab_f); F(h->sell.tab_d);
@@ -1104,6 +1104,49 @@ int asd_set_device_layout(asd_handle* h, uint32_t layout) {
         configure_stage(h, h->block, h->sell.stage);
         h->tune = std::string(layout == ASD_EXCH_CSR ? "layout=SELL " : "layout=DIA ") + h->tune;
         if (h->graph_steps) build_graph(h, h->graph_steps);
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_set_ttm(asd_handle* h, const asd_ttm* m) {
+    if (!h) return ASD_EINVAL;
+    try {
+        CK(cudaSetDevice(h->device));
+        CK(cudaStreamSynchronize(h->stream));
+        if (!m) {
+            if (h->d_ttm) { CK(cudaFree(h->d_ttm)); h->d_ttm = nullptr; }
+        } else {
+            // the model divides by gamma_e Te, Cl and the cooling time (src/laser_heating.cpp:79-83)
+            REQUIRE(m->initial_T > 1e-5 && std::isfinite(m->initial_T), "initial temperature must be > 1e-5 K");
+            REQUIRE(m->gamma_e > 0 && m->Cl > 0 && m->cooling_time > 0 && m->pump_time > 0,
+                    "gamma_e, Cl, cooling_time and pump_time must be positive");
+            REQUIRE(std::isfinite(m->G_ep) && std::isfinite(m->pump_fluence), "G_ep, pump_fluence");
+            REQUIRE(m->npulses <= ASD_TTM_MAX_PULSES, "too many pulses");
+            TtmDev d{};
+            d.Te = d.Tl = d.T0 = m->initial_T;
+            d.G = m->G_ep; d.Cl = m->Cl; d.ge = m->gamma_e; d.dt = h->p.dt; d.ct = m->cooling_time;
+            d.tau = m->pump_time; d.P = m->pump_fluence; d.t0 = h->step; d.np = m->npulses;
+            d.bath_e = m->bath_is_electrons ? 1u : 0u;
+            for (uint32_t q = 0; q < m->npulses; q++) { d.scale[q] = m->pulse_scale[q]; d.delay[q] = m->pulse_delay[q]; }
+            if (!h->d_ttm) CK(cudaMalloc(&h->d_ttm, sizeof(TtmDev)));
+            CK(cudaMemcpy(h->d_ttm, &d, sizeof d, cudaMemcpyHostToDevice));
+            for (auto& T : h->h_rep_T) T = m->initial_T;   // the bath is hot from now on
+        }
+        if (h->graph_steps) build_graph(h, h->graph_steps);   // the step kernels change
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_get_ttm_temperatures(asd_handle* h, double* Te, double* Tl) {
+    if (!h || !Te || !Tl) return ASD_EINVAL;
+    try {
+        if (!h->d_ttm) throw Fail{ASD_ESTATE, "the two-temperature model is not running"};
+        CK(cudaSetDevice(h->device));
+        TtmDev d{};
+        CK(cudaMemcpyAsync(&d, h->d_ttm, sizeof d, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        *Te = d.Te;
+        *Tl = d.Tl;
     } catch (const Fail& f) { return fail(h, f); }
     return ASD_OK;
 }

@@ -491,6 +491,8 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
     LrArgs none{};
     none.P = L.P; none.idx = L.mesh_idx; none.w = L.w; none.inv_p = L.P ? 1.0f / (float)L.P : 0.f;
     cudaError_t e;
+    cudaError_t e0;
+    if (h->d_ttm && (e0 = launch_ttm_step(h, h->d_step, rel)) != cudaSuccess) return e0;
     auto run = [&](const StageArgs<R>& a0) {
         StageArgs<R> aa = a0;
         set_prefetch(aa, comp);

@@ -112,6 +112,15 @@ struct SqSampler {
     cufftHandle plan = 0;
 };
 
+// Two-temperature model state and parameters (device copy; Te, Tl advance in place).
+struct TtmDev {
+    double Te, Tl;
+    double G, Cl, ge, dt, T0, ct, tau, P;
+    uint64_t t0;                 // step at which the model started
+    uint32_t np, bath_e;
+    double scale[ASD_TTM_MAX_PULSES], delay[ASD_TTM_MAX_PULSES];
+};
+
 struct KernelTimer {
     std::string name;
     double total_ms = 0.0;
@@ -169,6 +178,7 @@ struct asd_handle {
     uint32_t* d_err = nullptr;           // device error bits (staging wait timeouts)
     double* d_aos = nullptr;             // [3N] staging buffer of the spin / field transfers
     uint32_t* d_rep_of_tile = nullptr;   // replica of each 32-spin tile's first spin
+    asd::TtmDev* d_ttm = nullptr;        // two-temperature model (null: off)
     std::string tune;                    // autotuner result, "B=.. stage=.. (ms ...)"
     bool lr_scattered = false;
     double nnz_per_row = 0.0;
@@ -204,6 +214,8 @@ cudaError_t launch_plain_ramp(asd_handle* h, double rv);
 cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v);
 cudaError_t launch_set_scalar_f(asd_handle* h, float* dst, float v);
 cudaError_t launch_mag_push(asd_handle* h);
+// one two-temperature-model step for step t (device counter + rel when step_base is set, else t)
+cudaError_t launch_ttm_step(asd_handle* h, const uint64_t* step_base, uint64_t t);
 cudaError_t time_first_stage(asd_handle* h, int warm, int reps, float* ms);
 cudaError_t launch_sq_sample(asd_handle* h);
 cudaError_t launch_sq_spectrum(asd_handle* h, int window, double alpha, double beta, uint32_t pixelwidth,

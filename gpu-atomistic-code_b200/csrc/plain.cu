@@ -343,6 +343,7 @@ cudaError_t launch_plain_step(asd_handle* h, uint64_t t) {
     PlainSpin ps{h->p_sigma, h->p_llgpf, h->p_lambda, h->p_k1u, h->p_k1udir, h->p_hstg};
     const uint32_t upd = h->p.update ? h->p.update : 1;
     const bool dip_refresh = h->lr.mode == ASD_LR_DIPOLE && (t % upd) == 0;
+    if (h->d_ttm && (e = launch_ttm_step(h, nullptr, t)) != cudaSuccess) return e;
     if (h->pulse_amp != 0.0 && h->has_site) {
         // the driver-side rampStag of every step (src/cuda.cu:38-41) with the pulse envelope
         const double x = ((double)t * h->p.dt - h->pulse_t0) / h->pulse_sigma;

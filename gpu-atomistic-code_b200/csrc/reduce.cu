@@ -201,6 +201,33 @@ cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v) {
     return cudaGetLastError();
 }
 
+// Two-temperature model, one step (src/laser_heating.cpp:884-895), then the spin bath
+// temperature of every replica.
+__global__ void ttm_step_k(TtmDev* s, const uint64_t* step_base, uint64_t t, uint32_t nrep, double* sq,
+                           float* sqf) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint64_t step = step_base ? *step_base + t : t;
+    const double time = (double)(step - s->t0) * s->dt;
+    double P = 0.0;
+    for (uint32_t p = 0; p < s->np; p++) {
+        const double x = (time - s->delay[p]) / s->tau;
+        P += s->P * s->scale[p] * exp(-(x * x));
+    }
+    const double Te = s->Te, Tl = s->Tl;
+    const double Ten = (-s->G * (Te - Tl) + P) * s->dt / (s->ge * Te) + Te;
+    const double Tln = (s->G * (Ten - Tl) - s->Cl * (Tl - s->T0) / s->ct) * s->dt / s->Cl + Tl;
+    s->Te = Ten;
+    s->Tl = Tln;
+    const double r = sqrt(s->bath_e ? Ten : Tln);
+    for (uint32_t q = 0; q < nrep; q++) { sq[q] = r; sqf[q] = (float)r; }
+}
+
+cudaError_t launch_ttm_step(asd_handle* h, const uint64_t* step_base, uint64_t t) {
+    ttm_step_k<<<1, 32, 0, h->stream>>>(h->d_ttm, step_base, t, h->nrep, h->d_rep_sqrtT, h->d_rep_sqrtT_f);
+    h->launches += 1;
+    return cudaGetLastError();
+}
+
 cudaError_t launch_mag_push(asd_handle* h) {
     const uint32_t m = h->nrep * h->nsub;
     mag_push_k<<<nb(m, 128), 128, 0, h->stream>>>(m, h->d_mag, h->d_stats);

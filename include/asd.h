@@ -205,6 +205,33 @@ int asd_sq_setup(asd_handle* h, uint32_t qaxis, const double* uo, const uint32_t
 int asd_sq_sample(asd_handle* h);
 /* Copy the recorded series out: out[(sample*nk + k)*2 + {re, im}]; *nsamples = samples recorded. */
 int asd_sq_get(asd_handle* h, double* out, size_t out_len, uint32_t* nsamples);
+/* Two-temperature model of the laser-heating driver (src/laser_heating.cpp:648-676, CalcTe at
+ * :884-895): every step, before integrating it, the electron and lattice temperatures advance as
+ *   P  = fluence * sum_p scale_p exp(-((t - delay_p) / pump_time)^2),  t = (step - start) dt
+ *   Te = (-G (Te - Tl) + P) dt / (gamma_e Te) + Te
+ *   Tl = ( G (Te - Tl) - Cl (Tl - T0) / cooling_time) dt / Cl + Tl      (with the new Te)
+ * and every replica's spin bath takes Te (bath_is_electrons) or Tl.  Runs on the device inside
+ * the step, so the temperature never crosses to the host. */
+#define ASD_TTM_MAX_PULSES 16
+typedef struct asd_ttm {
+    double gamma_e;        /* Ce(Te) = gamma_e Te */
+    double Cl;             /* lattice specific heat */
+    double G_ep;           /* electron-phonon coupling */
+    double pump_time;      /* Gaussian width tau [s] */
+    double pump_fluence;   /* laser power */
+    double cooling_time;   /* [s] */
+    double initial_T;      /* T0 = Te = Tl at the start [K], > 1e-5 */
+    uint32_t npulses;      /* <= ASD_TTM_MAX_PULSES */
+    uint32_t bath_is_electrons;
+    double pulse_scale[ASD_TTM_MAX_PULSES];
+    double pulse_delay[ASD_TTM_MAX_PULSES];
+} asd_ttm;
+/* Start the two-temperature model at the current step (NULL stops it; the spin bath keeps the
+ * last temperature). */
+int asd_set_ttm(asd_handle* h, const asd_ttm* ttm);
+/* Current electron and lattice temperatures of the model. */
+int asd_get_ttm_temperatures(asd_handle* h, double* Te, double* Tl);
+
 /* Dynamic structure factor of the recorded series, per k-point, on the device: replaces the
  * time-series analysis tool fourier_space_analysis/src/timeseries.cpp:142-275.
  *   window 0: none; 1: generalised Hamming alpha - beta cos(2 pi t / (ns - 1))   (:185-189)

@@ -7,6 +7,7 @@ CPU legs of bench.py; never by the product.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -165,6 +166,7 @@ class Oracle:
         roff = au32(np.concatenate([[0], np.cumsum([s.nspins for s in systems])]))
         T = a64([s.temperature for s in systems])
         st = au32([s.stream for s in systems])
+        self._off, self._T, self._stream = roff, T, st
         L.orc_set_replicas(self.c, len(systems), _ptr(roff, C.c_uint32), _ptr(T, C.c_double), _ptr(st, C.c_uint32))
         s0 = systems[0]
         if s0.exch == 2:  # CSR (asd_b200.EXCH_CSR)
@@ -210,6 +212,14 @@ class Oracle:
             olib().orc_destroy(self.c)
         except Exception:
             pass
+
+    def set_temperatures(self, T):
+        """Replica temperatures [K] for the following steps (the spin bath of a driver that changes
+        T between steps)."""
+        L = olib()
+        self._T = a64(T)
+        L.orc_set_replicas(self.c, len(self._T), _ptr(self._off, C.c_uint32), _ptr(self._T, C.c_double),
+                           _ptr(self._stream, C.c_uint32))
 
     def set_pulse(self, amp, t0, sigma, dt):
         L = olib()
@@ -482,3 +492,21 @@ def ref_csr_to_dia(n, xadj, adjncy, val9, offdiag=True):
                            C.byref(nd), _ptr(off, C.c_int32), _ptr(data, C.c_double), nd.value)
     assert rc == 0
     return off, data.reshape(9, nd.value * n)
+
+
+def ttm_step(state, prm, step, dt):
+    """One two-temperature-model step, src/laser_heating.cpp:884-895 (CalcTe): the electron
+    temperature first, then the lattice with the new Te.  state = [Te, Tl] is updated in place;
+    prm: gamma_e, Cl, G_ep, pump_time, pump_fluence, cooling_time, initial_T, pulses, t0 (start
+    step).  Returns the bath temperature (Te or Tl)."""
+    time = (step - prm["t0"]) * dt
+    P = 0.0
+    for sc, dl in prm["pulses"]:
+        x = (time - dl) / prm["pump_time"]
+        P += prm["pump_fluence"] * sc * math.exp(-(x * x))
+    Te, Tl = state
+    G, Cl = prm["G_ep"], prm["Cl"]
+    Te_n = (-G * (Te - Tl) + P) * dt / (prm["gamma_e"] * Te) + Te
+    Tl_n = (G * (Te_n - Tl) - Cl * (Tl - prm["initial_T"]) / prm["cooling_time"]) * dt / Cl + Tl
+    state[0], state[1] = Te_n, Tl_n
+    return Te_n if prm.get("bath_is_electrons", True) else Tl_n

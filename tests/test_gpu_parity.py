@@ -446,3 +446,38 @@ def test_dia_input_on_both_device_layouts_bit_identical(gpu, prec):
                 out.append((h.get_spins(), h.get_field()))
         assert np.array_equal(out[0][0], out[1][0])
         assert np.array_equal(out[0][1], out[1][1])
+
+
+TTM = dict(gamma_e=3.0e3, Cl=2.0e6, G_ep=1.0e17, pump_time=2e-15, pump_fluence=4e21, cooling_time=1e-12,
+           initial_T=40.0, pulses=[(1.0, 3e-15), (0.5, 6e-15)])
+
+
+@pytest.mark.parametrize("prec,tol", [(A.FP64_PLAIN, 1e-12), (A.FP32, 1e-5)])
+def test_two_temperature_model_drives_the_bath(gpu, prec, tol):
+    """The device two-temperature model (CalcTe, src/laser_heating.cpp:884-895) advances Te and Tl
+    like the restatement, and the spins follow the oracle stepped at the same bath temperature."""
+    s = LT.sc_ferromagnet(5, T=0.0)
+    S0 = LT.random_spins(s.nspins, 3)
+    dt, nsteps, start = 1e-16, 60, 7
+    o = O.Oracle(s, dt=dt, seed=5)
+    o.set_spins(S0)
+    o.step(start)
+    prm = dict(TTM, t0=start)
+    st = [TTM["initial_T"], TTM["initial_T"]]
+    flags = A.FLAG_COMPENSATED if prec == A.FP32 else 0
+    with A.Handle(A.RunParams(precision=prec, dt=dt, seed=5, flags=flags), s) as h:
+        h.set_spins(S0)
+        h.step(start)
+        h.set_ttm(**TTM)
+        for k in range(nsteps):
+            T = O.ttm_step(st, prm, start + k, dt)
+            o.set_temperatures([T])
+            o.step(1)
+            h.step(1)
+            if k % 10 == 9:
+                te, tl = h.ttm_temperatures()
+                assert abs(te - st[0]) <= 1e-12 * st[0] and abs(tl - st[1]) <= 1e-12 * st[1]
+        assert st[0] > 2 * TTM["initial_T"]          # the pulses heated the electrons
+        assert maxdiff(h.get_spins(), o.spins()) <= tol
+        h.set_ttm(off=True)
+        h.step(3)
