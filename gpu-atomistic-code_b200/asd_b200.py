@@ -45,7 +45,7 @@ EXPORTED = [
     "asd_sq_spectrum", "asd_tuning", "asd_set_launch_shape",
     "asd_time_kernels_cold", "asd_time_steps_cold", "asd_read_ucf", "asd_read_exch", "asd_read_csr_exch",
     "asd_write_csr_exch", "asd_plan_spin_spans", "asd_set_device_layout", "asd_set_ttm",
-    "asd_get_ttm_temperatures",
+    "asd_get_ttm_temperatures", "asd_set_four_spin",
 ]
 
 
@@ -158,6 +158,7 @@ def load_library(path: str = LIB_PATH):
         "asd_set_launch_shape": ([P, C.c_uint32, C.c_uint32], C.c_int),
         "asd_set_device_layout": ([P, C.c_uint32], C.c_int),
         "asd_set_ttm": ([P, C.c_void_p], C.c_int),
+        "asd_set_four_spin": ([P, u32p, u32p, u32p, u32p, C.c_double, C.c_int], C.c_int),
         "asd_get_ttm_temperatures": ([P, dp, dp], C.c_int),
         "asd_sq_spectrum": ([P, C.c_uint32, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                              dp, dp, C.c_size_t, u32p, u32p], C.c_int),
@@ -453,6 +454,15 @@ class Handle:
         te, tl = C.c_double(), C.c_double()
         _check(load_library().asd_get_ttm_temperatures(self.h, C.byref(te), C.byref(tl)), self.h)
         return te.value, tl.value
+
+    def set_four_spin(self, xadj, j, k, l, jq, divide_by_3=True):
+        """Four-spin quartets (j, k, l) of every spin, CSR over spins; xadj None removes the term."""
+        if xadj is None:
+            _check(load_library().asd_set_four_spin(self.h, None, None, None, None, 0.0, 0), self.h)
+            return
+        self._q4 = [np.ascontiguousarray(a, dtype=np.uint32) for a in (xadj, j, k, l)]
+        _check(load_library().asd_set_four_spin(self.h, *[_p(a, C.c_uint32) for a in self._q4], jq,
+                                                int(divide_by_3)), self.h)
 
     def set_device_layout(self, layout: int):
         """EXCH_DIA or EXCH_CSR (SELL-32) for a DIA matrix."""

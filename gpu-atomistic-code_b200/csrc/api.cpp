@@ -67,7 +67,7 @@ void free_all(asd_handle* h) {
         F(h->nzf[c]); F(h->nzd[c]);
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
-    F(h->d_err); F(h->d_aos); F(h->d_rep_of_tile); F(h->d_ttm);
+    F(h->d_err); F(h->d_aos); F(h->d_rep_of_tile); F(h->d_ttm); F(h->d_q4ptr); F(h->d_q4jkl);
     F(h->sell.lwords); F(h->sell.span_ptr); F(h->sell.spans);
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
     F(h->sell.typed); F(h->sell.tab_f); F(h->sell.tab_d);
@@ -1104,6 +1104,39 @@ int asd_set_device_layout(asd_handle* h, uint32_t layout) {
         configure_stage(h, h->block, h->sell.stage);
         h->tune = std::string(layout == ASD_EXCH_CSR ? "layout=SELL " : "layout=DIA ") + h->tune;
         if (h->graph_steps) build_graph(h, h->graph_steps);
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_set_four_spin(asd_handle* h, const uint32_t* xadj_jkl, const uint32_t* adj_j, const uint32_t* adj_k,
+                      const uint32_t* adj_l, double JQ, int divide_by_3) {
+    if (!h) return ASD_EINVAL;
+    try {
+        CK(cudaSetDevice(h->device));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->d_q4ptr) { CK(cudaFree(h->d_q4ptr)); h->d_q4ptr = nullptr; }
+        if (h->d_q4jkl) { CK(cudaFree(h->d_q4jkl)); h->d_q4jkl = nullptr; }
+        h->sc.q4_ptr = nullptr;
+        h->sc.q4_jkl = nullptr;
+        if (xadj_jkl) {
+            REQUIRE(adj_j && adj_k && adj_l && std::isfinite(JQ), "quartet lists and a finite JQ are required");
+            REQUIRE(xadj_jkl[0] == 0, "xadj_jkl[0] must be 0");
+            for (uint32_t i = 0; i < h->n; i++) REQUIRE(xadj_jkl[i + 1] >= xadj_jkl[i], "xadj_jkl must not decrease");
+            const uint32_t nq = xadj_jkl[h->n];
+            std::vector<uint4> q(std::max<uint32_t>(nq, 1), make_uint4(0, 0, 0, 0));
+            for (uint32_t k = 0; k < nq; k++) {
+                REQUIRE(adj_j[k] < h->n && adj_k[k] < h->n && adj_l[k] < h->n, "quartet spin index out of range");
+                q[k] = make_uint4(adj_j[k], adj_k[k], adj_l[k], 0);
+            }
+            h->d_q4ptr = dupload(xadj_jkl, (size_t)h->n + 1);
+            h->d_q4jkl = dupload(q.data(), q.size());
+            h->sc.q4_ptr = h->d_q4ptr;
+            h->sc.q4_jkl = h->d_q4jkl;
+            h->sc.q4_jq = JQ;
+            h->sc.q4_div3 = divide_by_3 ? 1 : 0;
+            h->sc.q4_jq_f = (float)(divide_by_3 ? JQ / 3.0 : JQ);
+        }
+        if (h->graph_steps) build_graph(h, h->graph_steps);   // the step kernels carry the constants
     } catch (const Fail& f) { return fail(h, f); }
     return ASD_OK;
 }

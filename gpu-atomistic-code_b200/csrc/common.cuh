@@ -39,6 +39,11 @@ struct StepConst {
     const uint32_t* atom;      // per-spin unit-cell atom or nullptr (-> i % nmat)
     const uint32_t* rep_off;   // nrep+1
     const uint32_t* rep_of_tile; // replica of the first spin of every 32-spin tile
+    const uint32_t* q4_ptr;      // four-spin quartets of spin i: q4_jkl[q4_ptr[i] .. q4_ptr[i+1])
+    const uint4* q4_jkl;         // (j, k, l, 0)
+    double q4_jq;                // JQ [T]
+    float q4_jq_f;               // JQ (/3 when divided) for the FP32 form
+    int q4_div3;                 // the GPU path's division by 3
     const double* rep_sqrtT;   // nrep: sqrt(T) per replica
     const uint32_t* rep_stream;
     const double* dyn;         // mutable scalars, see DYN_*
@@ -78,6 +83,27 @@ __device__ __forceinline__ double site_scale_d(const double* dyn, uint64_t t, do
 
 __device__ __forceinline__ uint32_t atom_of(const StepConst& c, uint32_t i) {
     return c.atom ? c.atom[i] : (c.nmat == 1 ? 0u : i % c.nmat);
+}
+
+// Four-spin field of spin i, accumulated from zero in quartet order (src/cufields.cu:59-90);
+// get(j, v) loads spin j.
+template <typename R, typename Get>
+__device__ __forceinline__ void four_spin(const StepConst& c, uint32_t i, Get get, R h4[3]) {
+    h4[0] = h4[1] = h4[2] = R(0);
+    const uint32_t q0 = __ldg(c.q4_ptr + i), q1 = __ldg(c.q4_ptr + i + 1);
+    for (uint32_t q = q0; q < q1; q++) {
+        const uint4 jkl = __ldg(c.q4_jkl + q);
+        R sj[3], sk[3], sl[3];
+        get(jkl.x, sj); get(jkl.y, sk); get(jkl.z, sl);
+        const R skdotsl = sk[0] * sl[0] + sk[1] * sl[1] + sk[2] * sl[2];
+        const R sjdotsl = sj[0] * sl[0] + sj[1] * sl[1] + sj[2] * sl[2];
+        const R skdotsj = sk[0] * sj[0] + sk[1] * sj[1] + sk[2] * sj[2];
+        for (int a = 0; a < 3; a++) {
+            const R v = sj[a] * skdotsl + sk[a] * sjdotsl + sl[a] * skdotsj;
+            if constexpr (sizeof(R) == 8) h4[a] -= c.q4_div3 ? (c.q4_jq * v) / 3.0 : c.q4_jq * v;
+            else h4[a] -= c.q4_jq_f * v;
+        }
+    }
 }
 
 // Replica of spin i: the replica of its 32-spin tile's first spin, advanced past the replica

@@ -227,6 +227,11 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
     R h[3] = {R(0), R(0), R(0)};
     if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, a.src, tab, h, staged, wbase, sspin);
     if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, a.src, tab, h);
+    if (c.q4_ptr) {
+        R h4[3];
+        four_spin<R>(c, i, [&](uint32_t j, R v[3]) { v[0] = a.src.p[0][j]; v[1] = a.src.p[1][j]; v[2] = a.src.p[2][j]; }, h4);
+        h[0] += h4[0]; h[1] += h4[1]; h[2] += h4[2];
+    }
     uint32_t midx = 0;
     if (a.lr.hr || a.lr.mr) midx = __ldg(a.lr.idx + i);
     if (a.lr.hr) {

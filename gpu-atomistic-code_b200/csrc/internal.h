@@ -179,6 +179,8 @@ struct asd_handle {
     double* d_aos = nullptr;             // [3N] staging buffer of the spin / field transfers
     uint32_t* d_rep_of_tile = nullptr;   // replica of each 32-spin tile's first spin
     asd::TtmDev* d_ttm = nullptr;        // two-temperature model (null: off)
+    uint32_t* d_q4ptr = nullptr;         // four-spin quartet offsets [N+1]
+    uint4* d_q4jkl = nullptr;            // four-spin quartets (j, k, l, 0)
     std::string tune;                    // autotuner result, "B=.. stage=.. (ms ...)"
     bool lr_scattered = false;
     double nnz_per_row = 0.0;

@@ -317,7 +317,28 @@ cudaError_t launch_lr_eval_plain(asd_handle* h, const double* s, double* out, bo
     return cudaGetLastError();
 }
 
+// CH += four-spin field (src/cufields.cu:59-90; launched after the SpMV as src/cuda.cu:143-146).
+__global__ void plain_four_spin(const StepConst c, const double* __restrict__ s, double* __restrict__ ch) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= c.n) return;
+    double h4[3];
+    four_spin<double>(c, i, [&](uint32_t j, double v[3]) { v[0] = s[3 * (size_t)j]; v[1] = s[3 * (size_t)j + 1]; v[2] = s[3 * (size_t)j + 2]; }, h4);
+    ch[3 * (size_t)i] += h4[0];
+    ch[3 * (size_t)i + 1] += h4[1];
+    ch[3 * (size_t)i + 2] += h4[2];
+}
+
+static cudaError_t plain_field_exch(asd_handle* h, const double* s, double* ch);
+
 static cudaError_t plain_field(asd_handle* h, const double* s, double* ch) {
+    cudaError_t e = plain_field_exch(h, s, ch);
+    if (e != cudaSuccess || !h->sc.q4_ptr) return e;
+    plain_four_spin<<<nb(h->n, 256), 256, 0, h->stream>>>(h->sc, s, ch);
+    h->launches += 1;
+    return cudaGetLastError();
+}
+
+static cudaError_t plain_field_exch(asd_handle* h, const double* s, double* ch) {
     const int B = 256;
     cudaStream_t st = h->stream;
     const int zz = (h->p.flags & ASD_FLAG_GPU_DZZ_FROM_DYY) ? 1 : 0;

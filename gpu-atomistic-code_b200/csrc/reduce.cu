@@ -124,6 +124,11 @@ __global__ void field_k(StepConst c, SellDev sell, DiaDev dia, const R* __restri
     const CVec3<R> src{{sx, sy, sz}};
     if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, src, tab, hr3);
     if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, src, tab, hr3);
+    if (c.q4_ptr) {
+        R h4[3];
+        four_spin<R>(c, i, [&](uint32_t j, R v[3]) { v[0] = src.p[0][j]; v[1] = src.p[1][j]; v[2] = src.p[2][j]; }, h4);
+        hr3[0] += h4[0]; hr3[1] += h4[1]; hr3[2] += h4[2];
+    }
     double h[3] = {(double)hr3[0], (double)hr3[1], (double)hr3[2]};
     if (hr) {
         const uint32_t m = idx[i];

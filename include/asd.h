@@ -205,6 +205,15 @@ int asd_sq_setup(asd_handle* h, uint32_t qaxis, const double* uo, const uint32_t
 int asd_sq_sample(asd_handle* h);
 /* Copy the recorded series out: out[(sample*nk + k)*2 + {re, im}]; *nsamples = samples recorded. */
 int asd_sq_get(asd_handle* h, double* out, size_t out_len, uint32_t* nsamples);
+/* Four-spin exchange, cufields::CSpMV_CSR_FourSpin (src/cufields.cu:59-90) and llgCPU
+ * (src/llgCPU.cpp:142-170): for each quartet (j, k, l) of spin i, listed CSR-style in
+ * adj_j/adj_k/adj_l[xadj_jkl[i] .. xadj_jkl[i+1]),
+ *   H_i -= JQ (S_j (S_k.S_l) + S_k (S_j.S_l) + S_l (S_k.S_j))    [/ 3 on the GPU path: divide_by_3]
+ * added to the exchange field at every field evaluation.  JQ in tesla.  xadj_jkl == NULL removes
+ * the term. */
+int asd_set_four_spin(asd_handle* h, const uint32_t* xadj_jkl, const uint32_t* adj_j, const uint32_t* adj_k,
+                      const uint32_t* adj_l, double JQ, int divide_by_3);
+
 /* Two-temperature model of the laser-heating driver (src/laser_heating.cpp:648-676, CalcTe at
  * :884-895): every step, before integrating it, the electron and lattice temperatures advance as
  *   P  = fluence * sum_p scale_p exp(-((t - delay_p) / pump_time)^2),  t = (step - start) dt

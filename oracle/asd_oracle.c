@@ -37,6 +37,9 @@ struct orc_ctx {
     uint64_t seed;
     double* nbuf;
     size_t nbuf_len, nbuf_pos;
+    uint32_t *q4ptr, *q4j, *q4k, *q4l;   /* four-spin quartets (CSR over spins), or NULL */
+    double q4jq;
+    int q4div3;
 };
 
 /* ------------------------------------------------------------------ */
@@ -275,6 +278,7 @@ void orc_destroy(orc_ctx* c) {
     freep(c->rep_off); freep(c->rep_stream); freep(c->rep_T);
     freep(c->xadj); freep(c->adjncy); freep(c->csr); freep(c->doff); freep(c->dia);
     freep(c->mesh_xyz); freep(c->spec); freep(c->nr); freep(c->w); freep(c->nbuf);
+    freep(c->q4ptr); freep(c->q4j); freep(c->q4k); freep(c->q4l);
     free(c);
 }
 
@@ -491,10 +495,35 @@ static void longrange_field(const orc_ctx* c, const double* src, double* out) {
     }
 }
 
-/* CH for a stage: (HDemag + exchange sum) (src/cufields.cu:201-203) or the FFT field. */
+/* CH += four-spin field, accumulated from zero per spin in quartet order:
+ * cufields::CSpMV_CSR_FourSpin (src/cufields.cu:59-90), launched after the SpMV
+ * (src/cuda.cu:143-146); without the division by 3, llgCPU's H4s (src/llgCPU.cpp:142-170). */
+static void four_spin_add(const orc_ctx* c, const double* src, double* ch) {
+    if (!c->q4ptr) return;
+    for (uint32_t i = 0; i < c->n; i++) {
+        double h[3] = {0.0, 0.0, 0.0};
+        for (uint32_t q = c->q4ptr[i]; q < c->q4ptr[i + 1]; q++) {
+            const double* sj = src + 3 * (size_t)c->q4j[q];
+            const double* sk = src + 3 * (size_t)c->q4k[q];
+            const double* sl = src + 3 * (size_t)c->q4l[q];
+            const double skdotsl = sk[0] * sl[0] + sk[1] * sl[1] + sk[2] * sl[2];
+            const double sjdotsl = sj[0] * sl[0] + sj[1] * sl[1] + sj[2] * sl[2];
+            const double skdotsj = sk[0] * sj[0] + sk[1] * sj[1] + sk[2] * sj[2];
+            for (int a = 0; a < 3; a++) {
+                const double v = sj[a] * skdotsl + sk[a] * sjdotsl + sl[a] * skdotsj;
+                h[a] -= c->q4div3 ? (c->q4jq * v) / 3.0 : c->q4jq * v;
+            }
+        }
+        for (int a = 0; a < 3; a++) ch[3 * (size_t)i + a] += h[a];
+    }
+}
+
+/* CH for a stage: (HDemag + exchange sum) (src/cufields.cu:201-203) or the FFT field, then the
+ * four-spin term. */
 static void stage_field(orc_ctx* c, const double* src, double* ch) {
     if (c->lr == ORC_LR_FFT) {
         longrange_field(c, src, ch);
+        four_spin_add(c, src, ch);
         return;
     }
     for (uint32_t i = 0; i < c->n; i++) {
@@ -502,6 +531,26 @@ static void stage_field(orc_ctx* c, const double* src, double* ch) {
         exch_sum(c, src, i, dot);
         for (int a = 0; a < 3; a++) ch[3 * (size_t)i + a] = c->hdemag[3 * (size_t)i + a] + dot[a];
     }
+    four_spin_add(c, src, ch);
+}
+
+int orc_set_four_spin(orc_ctx* c, const uint32_t* ptr, const uint32_t* j, const uint32_t* k, const uint32_t* l,
+                      double jq, int div3) {
+    freep(c->q4ptr); freep(c->q4j); freep(c->q4k); freep(c->q4l);
+    c->q4ptr = c->q4j = c->q4k = c->q4l = NULL;
+    if (!ptr) return 0;
+    const uint32_t nq = ptr[c->n];
+    c->q4ptr = (uint32_t*)malloc(sizeof(uint32_t) * (c->n + 1));
+    c->q4j = (uint32_t*)malloc(sizeof(uint32_t) * (nq + 1));
+    c->q4k = (uint32_t*)malloc(sizeof(uint32_t) * (nq + 1));
+    c->q4l = (uint32_t*)malloc(sizeof(uint32_t) * (nq + 1));
+    memcpy(c->q4ptr, ptr, sizeof(uint32_t) * (c->n + 1));
+    memcpy(c->q4j, j, sizeof(uint32_t) * nq);
+    memcpy(c->q4k, k, sizeof(uint32_t) * nq);
+    memcpy(c->q4l, l, sizeof(uint32_t) * nq);
+    c->q4jq = jq;
+    c->q4div3 = div3;
+    return 0;
 }
 
 int orc_field(orc_ctx* c, double* h) {

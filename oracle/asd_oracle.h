@@ -76,6 +76,10 @@ int orc_set_dia(orc_ctx* c, int full, uint32_t ndiag, const int32_t* offsets, co
 int orc_set_site_field(orc_ctx* c, const double* hstag, double scale);
 /* Gaussian time envelope of the site field: multiplier amp exp(-((t dt - t0)/sigma)^2 / 2). */
 int orc_set_pulse(orc_ctx* c, double amp, double t0, double sigma, double dt);
+/* Four-spin quartets (CSR over spins, ptr[n+1]; j, k, l) with JQ [T]; div3 selects the GPU
+ * path's division by 3 (src/cufields.cu:76-78).  ptr NULL removes the term. */
+int orc_set_four_spin(orc_ctx* c, const uint32_t* ptr, const uint32_t* j, const uint32_t* k, const uint32_t* l,
+                      double jq, int div3);
 /* Long-range field by direct summation on the periodic padded mesh:
  * H_i = sum_j Nr[s_i][s_j][a][b][(x_i-x_j) mod n] * w_j * S_j[b], with w_j = mu_j for
  * ORC_LR_DIPOLE (src/cufields.cu:355) and 1 for ORC_LR_FFT (src/cufields.cu:381).

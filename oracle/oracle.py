@@ -78,6 +78,8 @@ def olib():
         L.orc_set_site_field.argtypes = [C.c_void_p, dp, C.c_double]
         L.orc_set_longrange.argtypes = [C.c_void_p, C.c_int, u32p, u32p, C.c_uint32, u32p, dp, dp, C.c_uint32]
         L.orc_set_flags.argtypes = [C.c_void_p, C.c_uint32]
+        L.orc_set_four_spin.restype = C.c_int
+        L.orc_set_four_spin.argtypes = [C.c_void_p, u32p, u32p, u32p, u32p, C.c_double, C.c_int]
         L.orc_set_noise.argtypes = [C.c_void_p, C.c_int, C.c_uint64, C.c_uint32, C.c_uint32, dp, C.c_size_t]
         L.orc_set_spins.argtypes = [C.c_void_p, dp]
         L.orc_get_spins.argtypes = [C.c_void_p, dp]
@@ -212,6 +214,11 @@ class Oracle:
             olib().orc_destroy(self.c)
         except Exception:
             pass
+
+    def set_four_spin(self, xadj, j, k, l, jq, div3=True):
+        L = olib()
+        self._q4 = [au32(xadj), au32(j), au32(k), au32(l)]
+        L.orc_set_four_spin(self.c, *[_ptr(a, C.c_uint32) for a in self._q4], C.c_double(jq), int(div3))
 
     def set_temperatures(self, T):
         """Replica temperatures [K] for the following steps (the spin bath of a driver that changes
