@@ -65,16 +65,23 @@ __global__ void scatter_k(uint32_t n, size_t P, const float* __restrict__ sx, co
     mr[2 * P + m] = sz[i] * wv;
 }
 
-// Largest |Re| and |Im| of the FP64 half spectrum (non-negative doubles order like their bits).
+// Largest |Re| and |Im| of the FP64 half spectrum (non-negative doubles order like their bits):
+// grid-stride per thread, warp and block maxima, one atomic per block.
 __global__ void nk_extent(size_t m, const double2* __restrict__ z, unsigned long long* mx) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double sre[32], sim[32];
     double re = 0.0, im = 0.0;
-    if (i < m) { re = fabs(z[i].x); im = fabs(z[i].y); }
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (size_t)gridDim.x * blockDim.x) {
+        re = fmax(re, fabs(z[i].x));
+        im = fmax(im, fabs(z[i].y));
+    }
     for (int o = 16; o > 0; o >>= 1) {
         re = fmax(re, __shfl_xor_sync(0xffffffffu, re, o));
         im = fmax(im, __shfl_xor_sync(0xffffffffu, im, o));
     }
-    if ((threadIdx.x & 31) == 0) {
+    if ((threadIdx.x & 31) == 0) { sre[threadIdx.x >> 5] = re; sim[threadIdx.x >> 5] = im; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (uint32_t w = 1; w < blockDim.x / 32; w++) { re = fmax(re, sre[w]); im = fmax(im, sim[w]); }
         atomicMax(mx, (unsigned long long)__double_as_longlong(re));
         atomicMax(mx + 1, (unsigned long long)__double_as_longlong(im));
     }
@@ -480,7 +487,7 @@ cudaError_t build_nk_f32(asd_handle* h, const double* d_nr) {
     unsigned long long* mx = nullptr;
     cudaMalloc(&mx, 2 * sizeof(unsigned long long));
     cudaMemsetAsync(mx, 0, 2 * sizeof(unsigned long long), h->stream);
-    nk_extent<<<nb(nc * L.Pk, 256), 256, 0, h->stream>>>(nc * L.Pk, z, mx);
+    nk_extent<<<std::min<unsigned>(nb(nc * L.Pk, 256), 148 * 8), 256, 0, h->stream>>>(nc * L.Pk, z, mx);
     unsigned long long hm[2] = {0, 0};
     cudaMemcpyAsync(hm, mx, sizeof(hm), cudaMemcpyDeviceToHost, h->stream);
     cudaStreamSynchronize(h->stream);
