@@ -15,6 +15,7 @@
 struct orc_ctx {
     uint32_t n;
     double *s, *es, *fn, *h, *hdemag, *det, *noise, *k[6], *hstag;
+    double* h4s;                         /* llgCPU's separate four-spin field (CPU_SUM_ORDER only) */
     double *llgpf, *lambda, *sigma, *k1u, *k1udir;
     double k2perp, k2perpdir[3], k2par, k2pardir[3], k4perp, k4perpdirs[9], k4par, k4pardirs[9], basemm;
     int integrator;
@@ -254,6 +255,7 @@ orc_ctx* orc_create(uint32_t n) {
     c->n = n;
     c->s = dalloc(3 * (size_t)n); c->es = dalloc(3 * (size_t)n); c->fn = dalloc(3 * (size_t)n);
     c->h = dalloc(3 * (size_t)n); c->hdemag = dalloc(3 * (size_t)n); c->det = dalloc(3 * (size_t)n);
+    c->h4s = dalloc(3 * (size_t)n);
     c->noise = dalloc(3 * (size_t)n); c->hstag = dalloc(3 * (size_t)n);
     for (int k = 0; k < 6; k++) c->k[k] = dalloc(3 * (size_t)n);
     c->llgpf = dalloc(n); c->lambda = dalloc(n); c->sigma = dalloc(n); c->k1u = dalloc(n);
@@ -271,7 +273,7 @@ orc_ctx* orc_create(uint32_t n) {
 static void freep(void* p) { if (p) free(p); }
 void orc_destroy(orc_ctx* c) {
     if (!c) return;
-    freep(c->s); freep(c->es); freep(c->fn); freep(c->h); freep(c->hdemag); freep(c->det);
+    freep(c->s); freep(c->es); freep(c->fn); freep(c->h); freep(c->hdemag); freep(c->det); freep(c->h4s);
     freep(c->noise); freep(c->hstag);
     for (int k = 0; k < 6; k++) freep(c->k[k]);
     freep(c->llgpf); freep(c->lambda); freep(c->sigma); freep(c->k1u); freep(c->k1udir);
@@ -597,13 +599,15 @@ static void total_field(const orc_ctx* c, uint32_t i, const double* ch_exch, con
     const double hs[3] = {c->cur_scale * c->hstag[3 * (size_t)i], c->cur_scale * c->hstag[3 * (size_t)i + 1],
                           c->cur_scale * c->hstag[3 * (size_t)i + 2]};
     if (c->flags & ORC_CPU_SUM_ORDER) {
-        /* llgCPU: Hx holds the exchange only, HDemag is separate, H4s = 0. */
+        /* llgCPU: Hx holds the exchange only, HDemag and H4s are separate terms
+         * (src/llgCPU.cpp:180). */
         const double* hx = ch_exch + 3 * (size_t)i;
         const double* hd = c->hdemag + 3 * (size_t)i;
+        const double* h4 = c->h4s + 3 * (size_t)i;
         const double thz = (c->flags & ORC_CPU_THERMAL_Z_FROM_X) ? lrn[0] : lrn[2];
-        h[0] = c->applied[0] + lrn[0] + hx[0] + hd[0] + 0.0 + hs[0];
-        h[1] = c->applied[1] + lrn[1] + hx[1] + hd[1] + 0.0 + hs[1];
-        h[2] = hx[2] + thz + c->applied[2] + hd[2] + 0.0 + hs[2];
+        h[0] = c->applied[0] + lrn[0] + hx[0] + hd[0] + h4[0] + hs[0];
+        h[1] = c->applied[1] + lrn[1] + hx[1] + hd[1] + h4[1] + hs[1];
+        h[2] = hx[2] + thz + c->applied[2] + hd[2] + h4[2] + hs[2];
         if (c->flags & ORC_CPU_THERMAL_Z_FROM_X) lrn[2] = thz;
     } else {
         const double* ch = ch_exch + 3 * (size_t)i;
@@ -674,12 +678,15 @@ static void heun_step(orc_ctx* c, uint64_t t) {
             for (size_t q = 0; q < 3 * (size_t)n; q++) c->hdemag[q] = (double)(float)c->hdemag[q];
     }
     if (c->flags & ORC_CPU_SUM_ORDER) {
-        /* llgCPU: Hx = 0 + exchange sum; HDemag added as a separate term. */
+        /* llgCPU: Hx = 0 + exchange sum; HDemag and H4s (recomputed from zero at each stage,
+         * src/llgCPU.cpp:142-170,275-297) added as separate terms. */
         for (uint32_t i = 0; i < n; i++) {
             double dot[3];
             exch_sum(c, c->s, i, dot);
             for (int a = 0; a < 3; a++) c->h[3 * (size_t)i + a] = 0.0 + dot[a];
         }
+        memset(c->h4s, 0, 3 * (size_t)n * sizeof(double));
+        four_spin_add(c, c->s, c->h4s);
     } else {
         stage_field(c, c->s, c->h);
     }
@@ -704,6 +711,8 @@ static void heun_step(orc_ctx* c, uint64_t t) {
                 else c->h[3 * (size_t)i + a] = 0.0 + dot[a];
             }
         }
+        memset(c->h4s, 0, 3 * (size_t)n * sizeof(double));
+        four_spin_add(c, c->es, c->h4s);
     } else if (!stale) {
         if (c->flags & ORC_CPU_CORRECTOR_ACCUM) {
             hsave = dalloc(3 * (size_t)n);

@@ -1,5 +1,6 @@
 """ctypes wrappers of the checkers: liboracle.so (the FP64 CPU restatement) and
-_ref/libref_llgcpu*.so (the reference's own llgCPU compiled from source).
+_ref/libref_llgcpu*.so (the reference's own llgCPU compiled from source) and
+_ref/libref_cuda.so (the reference's own CUDA step kernels compiled from source).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
 CPU legs of bench.py; never by the product.
@@ -17,6 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_llgcpu.so")
 REF_REPLAY_SO = os.path.join(HERE, "_ref", "libref_llgcpu_replay.so")
+REF_CUDA_SO = os.path.join(HERE, "_ref", "libref_cuda.so")
 
 CPU_CORRECTOR_ACCUM = 1 << 0
 CPU_THERMAL_Z_FROM_X = 1 << 1
@@ -301,8 +303,9 @@ def thermal_normals(seed, stream, n, step):
 class RefLLGCPU:
     """The reference's own llgCPU::llgCPU (src/llgCPU.cpp:56-361) behind ref_harness.cpp."""
 
-    def __init__(self, system, dt=1e-16, applied=(0, 0, 0), replay=False, seed=(1, 101)):
-        path = REF_REPLAY_SO if replay else REF_SO
+    def __init__(self, system, dt=1e-16, applied=(0, 0, 0), replay=False, seed=(1, 101), path=None,
+                 anis=None):
+        path = path or (REF_REPLAY_SO if replay else REF_SO)
         if not os.path.exists(path):
             build()
         # each instance gets its own copy of the globals: load a private copy of the library
@@ -334,7 +337,17 @@ class RefLLGCPU:
                     _ptr(atoms, C.c_uint32), dt, s.temperature, _ptr(ap, C.c_double))
         k1u = a64([2.0 * mats[a].k1u / (MUB * mats[a].mu) for a in atoms])
         k1d = a64([mats[a].k1u_dir for a in atoms])
-        L.refh_set_anis(_ptr(k1u, C.c_double), _ptr(k1d, C.c_double), 0.0, None, 0.0, None, 0.0, None, 0.0, None)
+        # anis: the global K2/K4 terms in J as in anis:: (k2perp, k2perpdir, k2par, k2pardir,
+        # k4perp, k4perpdirs[3][3], k4par, k4pardirs[3][3])
+        a = dict(anis or {})
+        dirs = {k: a64(a.get(k, np.zeros(9 if k.startswith("k4") else 3))).reshape(-1)
+                for k in ("k2perpdir", "k2pardir", "k4perpdirs", "k4pardirs")}
+        self._anis = dirs
+        L.refh_set_anis(_ptr(k1u, C.c_double), _ptr(k1d, C.c_double),
+                        float(a.get("k2perp", 0.0)), _ptr(dirs["k2perpdir"], C.c_double),
+                        float(a.get("k2par", 0.0)), _ptr(dirs["k2pardir"], C.c_double),
+                        float(a.get("k4perp", 0.0)), _ptr(dirs["k4perpdirs"], C.c_double),
+                        float(a.get("k4par", 0.0)), _ptr(dirs["k4pardirs"], C.c_double))
         if s.exch == 2:
             xadj, adj, val = au32(s.xadj), au32(s.adjncy), a64(s.csr_val)
             self._keep = [xadj, adj, val]
@@ -350,9 +363,16 @@ class RefLLGCPU:
             hs = a64(s.site_field)
             self._keep.append(hs)
             L.refh_set_site_fields(_ptr(hs, C.c_double), None)
-        if not replay:
+        if not replay and path != REF_CUDA_SO:
             L.refh_seed(*seed)
         self.t = 0
+
+    def set_four_spin(self, xadj, j, k, l, jq):
+        """Quartets as exch::xadj_j / adjncy_j,k,l and JQ(0) [T] (src/exch_read_4_spin.cpp)."""
+        q = [au32(a) for a in (xadj, j, k, l)]
+        self._q4 = q
+        self.L.refh_set_four_spin.argtypes = [C.c_uint, u32p, u32p, u32p, u32p, C.c_double]
+        self.L.refh_set_four_spin(len(q[1]), *[_ptr(a, C.c_uint32) for a in q], float(jq))
 
     def set_noise(self, xi):
         x = a64(xi).reshape(-1)
@@ -372,6 +392,58 @@ class RefLLGCPU:
         rc = self.L.refh_run(self.t, k)
         self.t += k
         return rc
+
+
+class RefCUDA(RefLLGCPU):
+    """The reference's own CUDA step kernels (CHeun1/2, CSpMV_*, CdetRK4k*/RK5k*, src/cuint.cu,
+    src/cufields.cu, src/cuintRK4.cu, src/cuintRK5.cu) launched in the order of src/cuda.cu:43-258,
+    src/cudaRK4.cu:38-233 and src/cudaRK5.cu, behind ref_cuda_harness.cu.  Needs a GPU.  The
+    globals are filled exactly as for RefLLGCPU; set_spins() uploads everything, so call the
+    setters (four-spin, temperature) before it.  Crand (float normals) is set by the caller and
+    reused by every step until set again."""
+
+    def __init__(self, system, dt=1e-16, applied=(0, 0, 0), integrator=HEUN, block=128, dzz_from_dyy=False,
+                 anis=None):
+        super().__init__(system, dt=dt, applied=applied, path=REF_CUDA_SO, anis=anis)
+        L = self.L
+        L.refg_init.argtypes = [C.c_uint, C.c_int]
+        L.refg_set_noise.argtypes = [C.POINTER(C.c_float), C.c_size_t]
+        L.refg_run.argtypes = [C.c_int, C.c_uint]
+        L.refg_get_spins.argtypes = [dp]
+        L.refg_get_det_field.argtypes = [dp]
+        self.integrator, self.block, self.dzz = integrator, block, bool(dzz_from_dyy)
+
+    def set_spins(self, s):
+        super().set_spins(s)
+        rc = self.L.refg_init(self.block, 1 if self.dzz else 0)
+        if rc != 0:
+            raise RuntimeError(f"refg_init failed ({rc})")
+
+    def set_noise(self, xi):
+        x = np.ascontiguousarray(np.asarray(xi, dtype=np.float32).reshape(-1))
+        rc = self.L.refg_set_noise(_ptr(x, C.c_float), len(x))
+        if rc != 0:
+            raise RuntimeError(f"refg_set_noise failed ({rc})")
+
+    def step(self, k):
+        rc = self.L.refg_run(self.integrator, k)
+        if rc != 0:
+            raise RuntimeError(f"refg_run failed ({rc})")
+        self.t += k
+        return rc
+
+    def spins(self):
+        out = np.empty(3 * self.n)
+        self.L.refg_get_spins(_ptr(out, C.c_double))
+        return out.reshape(self.n, 3)
+
+    def det_field(self):
+        out = np.empty(3 * self.n)
+        self.L.refg_get_det_field(_ptr(out, C.c_double))
+        return out.reshape(self.n, 3)
+
+    def close(self):
+        self.L.refg_free()
 
 
 def sq_psi_k(S, sub, uo, mesh, mesh_xyz, kpoints, qaxis=2):

@@ -215,6 +215,24 @@ int refh_set_dia(int offdiag, unsigned ndiag, const int* offsets, const double* 
     return 0;
 }
 
+// Four-spin quartets (exch::xadj_j / adjncy_j,k,l, src/exch_read_4_spin.cpp:147-270) and the
+// constant JQ(0) in T; llgCPU adds -JQ (Sj (Sk.Sl) + Sk (Sj.Sl) + Sl (Sk.Sj)) per quartet
+// (src/llgCPU.cpp:148-170).
+int refh_set_four_spin(unsigned nq, const unsigned* xadj_jkl, const unsigned* adj_j, const unsigned* adj_k,
+                       const unsigned* adj_l, double jq) {
+    unsigned n = geom::nspins;
+    exch::inc4spin = true;
+    exch::xadj_j.resize(n + 1);
+    for (unsigned i = 0; i <= n; i++) exch::xadj_j[i] = xadj_jkl[i];
+    exch::adjncy_j.resize(nq); exch::adjncy_k.resize(nq); exch::adjncy_l.resize(nq);
+    for (unsigned q = 0; q < nq; q++) {
+        exch::adjncy_j[q] = adj_j[q]; exch::adjncy_k[q] = adj_k[q]; exch::adjncy_l[q] = adj_l[q];
+    }
+    exch::JQ.resize(1);
+    exch::JQ[0] = jq;
+    return 0;
+}
+
 int refh_set_site_fields(const double* hstag, const double* hdemag) {
     unsigned n = geom::nspins;
     fill3(fields::Hstagx, fields::Hstagy, fields::Hstagz, hstag, n);

@@ -13,10 +13,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-sys.path[:0] = [REPO, os.path.join(REPO, "gpu-atomistic-code_b200")]
+sys.path[:0] = [REPO, os.path.join(REPO, "gpu-atomistic-code_b200"), os.path.dirname(HERE)]
 
 import asd_lattice as LT  # noqa: E402
 from oracle import oracle as O  # noqa: E402
+from helpers import plaquette_quartets  # noqa: E402
 
 
 def save(name, s, S0, out, **extra):
@@ -56,6 +57,17 @@ def main():
     xi = np.concatenate([O.thermal_normals(5, 0, s.nspins, t).reshape(-1) for t in range(20)])
     r = O.RefLLGCPU(s, replay=True); r.set_noise(xi); r.set_spins(S2); r.step(20)
     save("ref_sc4_open_T300_replay_20.npz", s, S2, r.spins(), steps=20, noise=xi)
+    four_spin_case()
+
+
+def four_spin_case():
+    """llgCPU with the four-spin term (src/llgCPU.cpp:142-170,275-297) on xy plaquettes, MWC noise."""
+    s = LT.sc_ferromagnet(5, T=300.0)
+    S0 = LT.random_spins(s.nspins, 3)
+    q = plaquette_quartets(5)
+    r = O.RefLLGCPU(s, seed=(7, 107)); r.set_four_spin(*q, 30.0); r.set_spins(S0); r.step(30)
+    save("ref_sc5_fourspin_T300_mwc_30.npz", s, S0, r.spins(), steps=30, mwc=np.array([7, 107]),
+         q4_xadj=q[0], q4_j=q[1], q4_k=q[2], q4_l=q[3], q4_jq=30.0)
 
 
 if __name__ == "__main__":

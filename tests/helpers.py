@@ -26,3 +26,17 @@ def load(name):
 
 def maxdiff(a, b):
     return float(np.abs(np.asarray(a) - np.asarray(b)).max())
+
+
+def plaquette_quartets(L):
+    """For every spin of an L^3 periodic sc lattice, the (j, k, l) of the four xy plaquettes it
+    belongs to, ordered around the plaquette."""
+    idx = lambda x, y, z: ((x % L) * L + (y % L)) * L + (z % L)
+    xadj, J, K, Lq = [0], [], [], []
+    for x in range(L):
+        for y in range(L):
+            for z in range(L):
+                for dx, dy in ((1, 1), (-1, 1), (-1, -1), (1, -1)):
+                    J.append(idx(x + dx, y, z)); K.append(idx(x + dx, y + dy, z)); Lq.append(idx(x, y + dy, z))
+                xadj.append(len(J))
+    return [np.array(a, dtype=np.uint32) for a in (xadj, J, K, Lq)]

@@ -11,7 +11,7 @@ import pytest
 
 import asd_b200 as A
 import asd_lattice as LT
-from helpers import maxdiff
+from helpers import maxdiff, plaquette_quartets
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -483,27 +483,13 @@ def test_two_temperature_model_drives_the_bath(gpu, prec, tol):
         h.step(3)
 
 
-def _plaquette_quartets(L):
-    """For every spin of an L^3 periodic sc lattice, the (j, k, l) of the four xy plaquettes it
-    belongs to, ordered around the plaquette."""
-    idx = lambda x, y, z: ((x % L) * L + (y % L)) * L + (z % L)
-    xadj, J, K, Lq = [0], [], [], []
-    for x in range(L):
-        for y in range(L):
-            for z in range(L):
-                for dx, dy in ((1, 1), (-1, 1), (-1, -1), (1, -1)):
-                    J.append(idx(x + dx, y, z)); K.append(idx(x + dx, y + dy, z)); Lq.append(idx(x, y + dy, z))
-                xadj.append(len(J))
-    return [np.array(a, dtype=np.uint32) for a in (xadj, J, K, Lq)]
-
-
 @pytest.mark.parametrize("div3", [True, False])
 def test_four_spin_term(gpu, div3):
     """Four-spin exchange (src/cufields.cu:59-90): the FP64 plain form equals the oracle bit for bit
     (with and without the GPU path's division by 3), the fused forms to their tolerances."""
     L = 5
     s = LT.sc_ferromagnet(L, T=100.0)
-    q = _plaquette_quartets(L)
+    q = plaquette_quartets(L)
     jq = 30.0                                   # [T], comparable to the exchange field
     S0 = LT.random_spins(s.nspins, 9)
     for prec, tol in ((A.FP64_PLAIN, 0.0), (A.FP64_FUSED, 1e-10), (A.FP32, 1e-5)):

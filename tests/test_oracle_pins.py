@@ -44,6 +44,18 @@ def test_oracle_compat_reproduces_reference_llgcpu_recorded_noise():
     assert np.array_equal(o.spins(), d["out"]), maxdiff(o.spins(), d["out"])
 
 
+def test_oracle_compat_reproduces_reference_llgcpu_four_spin():
+    """llgCPU's four-spin field H4s (no division by 3, recomputed at each stage) as a separate term."""
+    d = load("ref_sc5_fourspin_T300_mwc_30.npz")
+    s = system_from_npz(d)
+    a, b = (int(x) for x in d["mwc"])
+    o = O.Oracle(s, flags=COMPAT, noise=O.NOISE_MWC, mwc=(a, b))
+    o.set_four_spin(d["q4_xadj"], d["q4_j"], d["q4_k"], d["q4_l"], float(d["q4_jq"]), False)
+    o.set_spins(d["S0"])
+    o.step(int(d["steps"]))
+    assert np.array_equal(o.spins(), d["out"]), maxdiff(o.spins(), d["out"])
+
+
 def test_recorded_noise_is_the_philox_stream():
     d = load("ref_sc4_open_T300_replay_20.npz")
     n = int(d["nspins"])
