@@ -45,7 +45,7 @@ EXPORTED = [
     "asd_sq_spectrum", "asd_tuning", "asd_set_launch_shape",
     "asd_time_kernels_cold", "asd_time_steps_cold", "asd_read_ucf", "asd_read_exch", "asd_read_csr_exch",
     "asd_write_csr_exch", "asd_plan_spin_spans", "asd_set_device_layout", "asd_set_ttm",
-    "asd_get_ttm_temperatures", "asd_set_four_spin",
+    "asd_get_ttm_temperatures", "asd_set_four_spin", "asd_spins_random", "asd_spins_pattern",
 ]
 
 
@@ -167,6 +167,8 @@ def load_library(path: str = LIB_PATH):
         "asd_csr_to_dia": ([C.c_uint32, u32p, u32p, dp, C.c_uint32, i32p, dp, u32p], C.c_int),
         "asd_build_dipole_nr": ([u32p, u32p, dp, C.c_double, C.c_double, dp], C.c_int),
         "asd_fold_exchange_nr": ([u32p, C.c_uint32, i32p, dp, C.c_double, dp, u32p], C.c_int),
+        "asd_spins_random": ([C.c_uint32, u32p, dp], C.c_int),
+        "asd_spins_pattern": ([C.c_uint32, C.c_uint32, i32p, u32p, dp, dp], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -550,6 +552,27 @@ def read_csr_exch(path: str, nspins: int):
     _read_check(lib.asd_read_csr_exch(path.encode(), nspins, C.byref(nnz), _p(xadj, C.c_uint32), _p(adj, C.c_uint32),
                                       _p(val, C.c_double), nnz.value, err, 256), err)
     return xadj, adj, val
+
+
+def spins_random(n: int, mwc=(1, 101)):
+    """spins::setSpinsRandom on the reference's MWC1616 stream seeded (a, b): returns the n x 3
+    spins and the stream state after them (to hand on to the next consumer of the stream)."""
+    st = np.array(mwc, dtype=np.uint32)
+    out = np.zeros((n, 3))
+    _check(load_library().asd_spins_random(n, _p(st, C.c_uint32), _p(out, C.c_double)))
+    return out, (int(st[0]), int(st[1]))
+
+
+def spins_pattern(n: int, axis: int, coords=None, atom_of_spin=None, init_spin=None):
+    """setSpinsChequerX/Y/Z (axis 0..2, cell coordinates n x 3) or setSpinsConfig (axis 3: the
+    initial spin of each spin's unit-cell atom)."""
+    c = None if coords is None else np.ascontiguousarray(coords, dtype=np.int32)
+    a = None if atom_of_spin is None else np.ascontiguousarray(atom_of_spin, dtype=np.uint32)
+    s0 = None if init_spin is None else np.ascontiguousarray(init_spin, dtype=np.float64)
+    out = np.zeros((n, 3))
+    _check(load_library().asd_spins_pattern(n, axis, _p(c, C.c_int32), _p(a, C.c_uint32), _p(s0, C.c_double),
+                                            _p(out, C.c_double)))
+    return out
 
 
 def write_csr_exch(path: str, xadj, adjncy, val9):

@@ -169,6 +169,50 @@ int asd_fold_exchange_nr(const uint32_t mesh[3], uint32_t nshell, const int32_t*
 
 }  // extern "C"
 
+// ---- initial spins
+extern "C" int asd_spins_random(uint32_t n, uint32_t mwc[2], double* out) {
+    if (!mwc || !out || mwc[0] == 0 || mwc[1] == 0) return ASD_EINVAL;
+    uint32_t x = mwc[0], y = mwc[1];
+    // multiply-with-carry pair of 16-bit lags 18000 and 30903, scaled by 1/(2^32-1)
+    auto next = [&]() -> double {
+        x = 18000u * (x & 0xFFFFu) + (x >> 16);
+        y = 30903u * (y & 0xFFFFu) + (y >> 16);
+        return (double)((x << 16) + (y & 0xFFFFu)) * (1.0 / 4294967295.0);
+    };
+    for (uint32_t i = 0; i < n; i++) {
+        double v1 = 0.0, v2 = 0.0, s = 2.0;
+        while (s > 1.0) {
+            v1 = 2.0 * next() - 1.0;
+            v2 = 2.0 * next() - 1.0;
+            s = v1 * v1 + v2 * v2;
+        }
+        const double ss = std::sqrt(1.0 - s);
+        out[3 * (size_t)i] = 2.0 * v1 * ss;
+        out[3 * (size_t)i + 1] = 2.0 * v2 * ss;
+        out[3 * (size_t)i + 2] = 1.0 - 2.0 * s;
+    }
+    mwc[0] = x; mwc[1] = y;
+    return ASD_OK;
+}
+
+extern "C" int asd_spins_pattern(uint32_t n, uint32_t axis, const int32_t* coords, const uint32_t* atom_of_spin,
+                                 const double* init_spin, double* out) {
+    if (!out || axis > 3) return ASD_EINVAL;
+    if (axis < 3 && !coords) return ASD_EINVAL;
+    if (axis == 3 && (!atom_of_spin || !init_spin)) return ASD_EINVAL;
+    for (uint32_t i = 0; i < n; i++) {
+        double* o = out + 3 * (size_t)i;
+        if (axis == 3) {
+            for (int c = 0; c < 3; c++) o[c] = init_spin[3 * (size_t)atom_of_spin[i] + c];
+        } else {
+            const int32_t* r = coords + 3 * (size_t)i;
+            o[0] = o[1] = o[2] = 0.0;
+            o[axis] = ((r[0] + r[1] + r[2]) % 2 == 0) ? 1.0 : -1.0;
+        }
+    }
+    return ASD_OK;
+}
+
 // ---- neighbour-spin staging plan of the fused stage kernel
 namespace {
 constexpr uint32_t SPIN_SMEM_MAX = 64 * 1024;   // bytes of staged spins (3 components) per block

@@ -314,6 +314,18 @@ int asd_build_dipole_nr(const uint32_t dim[3], const uint32_t nk[3], const doubl
 int asd_fold_exchange_nr(const uint32_t mesh[3], uint32_t nshell, const int32_t* shell_vec,
                          const double* J9, double mu_muB, double* nr, uint32_t* count);
 
+/* Initial spins of the reference's spin-config modes (host only), n x 3 doubles out.
+ * random: spins::setSpinsRandom (src/spins.cpp:265-281), Marsaglia's (1972) point on the sphere
+ * from Random::rand of the MWC1616 stream (src/random.cpp:17-40) whose state (x, y) is taken
+ * from and returned in mwc[2] (both non-zero, as Random::seed demands). */
+int asd_spins_random(uint32_t n, uint32_t mwc[2], double* out);
+/* chequer: spins::setSpinsChequerX/Y/Z (src/spins.cpp:282-341): +e_axis where the cell
+ * coordinates (geom::lu(i,0..2), n x 3) sum to an even number, -e_axis elsewhere; axis 0..2.
+ * config (axis 3): spins::setSpinsConfig (src/spins.cpp:254-264), the initial spin of each
+ * spin's unit-cell atom, init_spin[3 * atom_of_spin[i] + c] (coords unused). */
+int asd_spins_pattern(uint32_t n, uint32_t axis, const int32_t* coords, const uint32_t* atom_of_spin,
+                      const double* init_spin, double* out);
+
 /* Neighbour-spin staging plan of the fused stage kernel (host only, no device needed).  For
  * SELL-32 slices (nslices, slice_ptr[nslices+1]) of typed words (column in the low colbits bits)
  * and blocks of `block` rows: each block's distinct columns are merged into spans (gaps of at

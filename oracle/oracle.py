@@ -446,6 +446,36 @@ class RefCUDA(RefLLGCPU):
         self.L.refg_free()
 
 
+def spins_random(n, mwc=(1, 101)):
+    """spins::setSpinsRandom (src/spins.cpp:265-281): Marsaglia's point on the sphere, v1, v2 =
+    2 rand - 1 until v1^2 + v2^2 <= 1, S = (2 v1 sqrt(1-s), 2 v2 sqrt(1-s), 1 - 2 s), with
+    rand() the oracle's MWC1616 (src/random.cpp:17-40)."""
+    L = olib()
+    L.orc_mwc_seed(int(mwc[0]), int(mwc[1]))
+    out = np.zeros((n, 3))
+    for i in range(n):
+        v1 = v2 = 0.0
+        s = 2.0
+        while s > 1.0:
+            v1 = 2.0 * L.orc_mwc_rand() - 1.0
+            v2 = 2.0 * L.orc_mwc_rand() - 1.0
+            s = v1 * v1 + v2 * v2
+        ss = math.sqrt(1.0 - s)
+        out[i] = (2.0 * v1 * ss, 2.0 * v2 * ss, 1.0 - 2.0 * s)
+    return out
+
+
+def ref_rand_stream(k, mwc=(1, 101)):
+    """k values of the reference's own Random::rand (src/random.cpp:37-40), compiled from source."""
+    if not os.path.exists(REF_SO):
+        build()
+    L = C.CDLL(REF_SO, mode=os.RTLD_LOCAL)
+    L.refh_seed.argtypes = [C.c_uint, C.c_uint]
+    L.refh_rand.restype = C.c_double
+    L.refh_seed(int(mwc[0]), int(mwc[1]))
+    return np.array([L.refh_rand() for _ in range(k)])
+
+
 def sq_psi_k(S, sub, uo, mesh, mesh_xyz, kpoints, qaxis=2):
     """psi_k of one sample: psi = uo_a S_a + i uo_b S_b on the mesh (a, b transverse to the
     quantisation axis), forward 3D FFT (FFTW sign), values at the k-points

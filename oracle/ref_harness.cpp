@@ -277,6 +277,8 @@ void refh_seed(unsigned a, unsigned b) { Random::seed(a, b); }
 
 double refh_normal() { return Random::normal(); }
 
+double refh_rand() { return Random::rand(); }
+
 #ifdef ASD_REF_REPLAY
 int refh_set_noise(const double* xi, size_t n) {
     Random::g_noise.assign(xi, xi + n);

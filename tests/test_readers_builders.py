@@ -204,3 +204,38 @@ def test_reference_example_inputs_drive_the_builder():
         bonds = list(zip(s1, s2, vec, J))
         rx, ra, rv = O.ref_exchunitcell((4, 4, 4), (1, 1, 1), [a["mu"] for a in atoms], bonds, offdiag=True)
         assert np.array_equal(rx, s.xadj) and np.array_equal(ra, s.adjncy) and np.array_equal(rv, s.csr_val)
+
+
+def test_spins_random_is_the_reference_marsaglia_on_its_mwc_stream():
+    """asd_spins_random == the oracle's restatement of spins::setSpinsRandom bit for bit, and the
+    oracle's MWC1616 == the reference's own Random::rand compiled from source."""
+    for mwc in ((1, 101), (7, 107), (123456789, 987654321)):
+        got, st = A.spins_random(2000, mwc)
+        ref = O.spins_random(2000, mwc)
+        assert np.array_equal(got, ref)
+        assert np.allclose(np.linalg.norm(got, axis=1), 1.0, atol=1e-15)
+        # the returned state continues the stream where the spins left it
+        nxt, _ = A.spins_random(5, st)
+        assert np.array_equal(nxt, O.spins_random(2005, mwc)[2000:])
+    if os.path.exists(O.REF_SO):
+        L = O.olib()
+        L.orc_mwc_seed(7, 107)
+        mine = np.array([L.orc_mwc_rand() for _ in range(5000)])
+        assert np.array_equal(mine, O.ref_rand_stream(5000, (7, 107)))
+    with pytest.raises(A.AsdError):
+        A.spins_random(4, (0, 5))           # Random::seed rejects a zero seed
+
+
+def test_spins_patterns():
+    L = 3
+    coords = np.array([(x, y, z) for x in range(L) for y in range(L) for z in range(L)], dtype=np.int32)
+    for axis in range(3):
+        s = A.spins_pattern(len(coords), axis, coords=coords)
+        sign = np.where(coords.sum(axis=1) % 2 == 0, 1.0, -1.0)
+        want = np.zeros((len(coords), 3))
+        want[:, axis] = sign
+        assert np.array_equal(s, want)
+    init = np.array([[0.0, 0.0, 1.0], [0.6, 0.0, -0.8]])
+    atom = np.arange(10, dtype=np.uint32) % 2
+    s = A.spins_pattern(10, 3, atom_of_spin=atom, init_spin=init)
+    assert np.array_equal(s, init[atom])
