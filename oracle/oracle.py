@@ -19,6 +19,7 @@ ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libref_llgcpu.so")
 REF_REPLAY_SO = os.path.join(HERE, "_ref", "libref_llgcpu_replay.so")
 REF_CUDA_SO = os.path.join(HERE, "_ref", "libref_cuda.so")
+REF_SHIM_SO = os.path.join(HERE, "_ref", "libref_shim.so")
 
 CPU_CORRECTOR_ACCUM = 1 << 0
 CPU_THERMAL_Z_FROM_X = 1 << 1
@@ -444,6 +445,44 @@ class RefCUDA(RefLLGCPU):
 
     def close(self):
         self.L.refg_free()
+
+
+class RefShim(RefLLGCPU):
+    """The library driven through the reference-side binding gpu-atomistic-code_b200/shim/cullg_asd.cpp:
+    the reference's namespace globals are filled as for RefLLGCPU, then cullg::cuinit and
+    cullg::llgGPU / llgGPURK4 / llgGPURK5 run as llg::integrate calls them; spins are read back
+    from the spins::Sx/Sy/Sz mirror the shim refreshes every `update` steps.  Needs a GPU."""
+
+    def __init__(self, system, dt=1e-16, applied=(0, 0, 0), integrator=HEUN, precision=2, flags=0, seed=1,
+                 update=1, anis=None):
+        super().__init__(system, dt=dt, applied=applied, path=REF_SHIM_SO, anis=anis)
+        L = self.L
+        s = system
+        atoms = au32(s.atom if s.atom is not None else np.arange(s.nspins) % len(s.materials))
+        coords = np.zeros((s.nspins, 3), dtype=np.int32)
+        L.refs_set_lu.argtypes = [C.c_uint, u32p, i32p]
+        L.refs_set_ucm.argtypes = [C.c_uint, dp, dp, u32p]
+        L.refs_configure.argtypes = [C.c_uint] * 5
+        L.refs_run.argtypes = [C.c_uint, C.c_uint]
+        L.refs_set_lu(s.nspins, _ptr(atoms, C.c_uint32), _ptr(coords, C.c_int32))
+        k1u = a64([m.k1u for m in s.materials])
+        dirs = a64([m.k1u_dir for m in s.materials]).reshape(-1)
+        sub = au32([m.sublattice for m in s.materials])
+        L.refs_set_ucm(len(s.materials), _ptr(k1u, C.c_double), _ptr(dirs, C.c_double), _ptr(sub, C.c_uint32))
+        L.refs_configure(integrator, seed, update, precision, flags)
+        self._keep_shim = [atoms, coords, k1u, dirs, sub]
+
+    def set_spins(self, s):
+        super().set_spins(s)
+        self.L.refs_cuinit()
+
+    def step(self, k):
+        self.L.refs_run(self.t, k)
+        self.t += k
+        return 0
+
+    def close(self):
+        self.L.refs_free()
 
 
 def spins_random(n, mwc=(1, 101)):

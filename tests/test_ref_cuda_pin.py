@@ -117,3 +117,29 @@ def test_heun_finite_temperature_same_normals(gpu):
     assert d <= 1e-7, d
     g32, _, _, _ = run_both(s, 40, A.FP32, noise=True)
     assert maxdiff(g32, r) <= 1e-5
+
+
+@pytest.mark.skipif(not os.path.exists(O.REF_SHIM_SO), reason="oracle/_ref/libref_shim.so not built")
+@pytest.mark.parametrize("T", [0.0, 300.0])
+def test_reference_side_binding(gpu, T):
+    """The library behind the reference's own data contract: the namespace globals filled as the
+    reference fills them, cullg::cuinit + cullg::llgGPU of gpu-atomistic-code_b200/shim/cullg_asd.cpp
+    as llg::integrate calls them.  Equal bit for bit to the same run through asd_b200 directly,
+    and (T = 0) to the reference's own kernels within the FP64 bound."""
+    s = LT.sc_ferromagnet(6, T=T)
+    S0 = LT.random_spins(s.nspins, 0)
+    shim = O.RefShim(s, precision=A.FP64_PLAIN, seed=3)
+    shim.set_spins(S0)
+    shim.step(50)
+    got = shim.spins()
+    shim.close()
+    with A.Handle(A.RunParams(precision=A.FP64_PLAIN, seed=3), s) as h:
+        h.set_spins(S0)
+        h.step(50)
+        assert np.array_equal(got, h.get_spins())
+    if T == 0.0:
+        ref = O.RefCUDA(s)
+        ref.set_spins(S0)
+        ref.step(50)
+        assert maxdiff(got, ref.spins()) <= 1e-10
+        ref.close()
