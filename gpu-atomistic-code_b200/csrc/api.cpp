@@ -67,7 +67,6 @@ void free_all(asd_handle* h) {
         F(h->nzf[c]); F(h->nzd[c]);
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
-    for (int q = 0; q < 3; q++) F(h->s4[q]);
     F(h->d_err); F(h->d_aos); F(h->d_rep_of_tile); F(h->d_ttm); F(h->d_q4ptr); F(h->d_q4jkl);
     F(h->sell.lwords); F(h->sell.span_ptr); F(h->sell.spans);
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
@@ -762,8 +761,6 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
                 if (bytes == 4) {
                     h->sf[c] = dalloc<float>(n + SPIN_PAD); h->esf[c] = dalloc<float>(n + SPIN_PAD);
                     h->fnf[c] = dalloc<float>(n + SPIN_PAD);
-                    if (c == 0)
-                        for (int q = 0; q < 3; q++) h->s4[q] = dalloc<float4>(n);
                     h->nzf[c] = dalloc<float>(n);
                     h->detf[c] = dalloc<float>(n);
                     if (p.flags & ASD_FLAG_COMPENSATED) h->sl[c] = dalloc<float>(n);

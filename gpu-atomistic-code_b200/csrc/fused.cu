@@ -26,8 +26,6 @@ struct LrArgs {
 template <typename R>
 struct StageArgs {
     CVec3<R> src;        // spins the field is gathered from (S or a stage spin)
-    const float4* src4;  // FP32 form: packed (x, y, z, 0) copy of src, read by the gathers
-    float4* out4;        // FP32 form: packed copy of out, written beside it
     CVec3<R> base;       // S (hi part)
     CVec3<float> base_lo;// S lo part (compensated storage) or nullptrs
     Vec3<R> out;         // next stage spin or new S (hi)
@@ -227,8 +225,8 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
         stage_timeout = true;
     }
     R h[3] = {R(0), R(0), R(0)};
-    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, a.src, a.src4, tab, h, staged, wbase, sspin);
-    if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, a.src, a.src4, tab, h);
+    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, a.src, tab, h, staged, wbase, sspin);
+    if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, a.src, tab, h);
     if (c.q4_ptr) {
         R h4[3];
         four_spin<R>(c, i, [&](uint32_t j, R v[3]) { v[0] = a.src.p[0][j]; v[1] = a.src.p[1][j]; v[2] = a.src.p[2][j]; }, h4);
@@ -293,7 +291,6 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
         const float inv = rsqrtf(o[0] * o[0] + o[1] * o[1] + o[2] * o[2]);
         for (int j = 0; j < 3; j++) out[j] = (R)(o[j] * inv);
         for (int j = 0; j < 3; j++) a.out.p[j][i] = out[j];
-        a.out4[i] = make_float4(out[0], out[1], out[2], 0.0f);
     } else {
         // new S (and every stage of the FP64 fused form): FP64 accumulation from the
         // full-precision base, FP64 renormalisation
@@ -336,11 +333,11 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
             }
         }
         renorm(o);
-        for (int j = 0; j < 3; j++) out[j] = (R)o[j];
-        if constexpr (F32) a.out4[i] = make_float4((float)out[0], (float)out[1], (float)out[2], 0.0f);
         for (int j = 0; j < 3; j++) {
-            a.out.p[j][i] = out[j];
-            if constexpr (COMP && final_spin) a.out_lo.p[j][i] = (float)(o[j] - (double)out[j]);
+            const R hi = (R)o[j];
+            out[j] = hi;
+            a.out.p[j][i] = hi;
+            if constexpr (COMP && final_spin) a.out_lo.p[j][i] = (float)(o[j] - (double)hi);
         }
     }
     if (a.lr.mr) {
@@ -482,22 +479,6 @@ void set_prefetch(StageArgs<R>& a, bool comp) {
     a.npf = k;
 }
 
-// The packed (x, y, z, 0) copy kept beside an FP32 spin buffer (S, es or fn), or nullptr.
-template <typename R>
-float4* packed_of(const asd_handle* h, R* const* p) {
-    if constexpr (sizeof(R) == 4) {
-        if (p == h->sf) return h->s4[0];
-        if (p == h->esf) return h->s4[1];
-        if (p == h->fnf) return h->s4[2];
-    }
-    return nullptr;
-}
-
-template <typename R>
-void set_src(const asd_handle* h, StageArgs<R>& a, R* const* p) { a.src = c3<R>(p); a.src4 = packed_of<R>(h, p); }
-template <typename R>
-void set_out(const asd_handle* h, StageArgs<R>& a, R* const* p) { a.out = v3<R>(p); a.out4 = packed_of<R>(h, p); }
-
 template <typename R>
 cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
     R* const* s; R* const* es; R* const* fn; R* const* det; R* const* stag;
@@ -525,7 +506,7 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
     };
     if (h->p.integrator == ASD_HEUN) {
         // predictor
-        set_src<R>(h, a, s); set_out<R>(h, a, es); a.fn = v3<R>(fn); a.kind = 1; a.nz_mode = 1;
+        a.src = c3<R>(s); a.out = v3<R>(es); a.fn = v3<R>(fn); a.kind = 1; a.nz_mode = 1;
         a.lr = none;
         if (L.mode == ASD_LR_FFT) {
             if ((e = launch_lr_eval_f32(h)) != cudaSuccess) return e;   // field of S (scattered before)
@@ -536,7 +517,7 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
         }
         if ((e = run(a)) != cudaSuccess) return e;
         // corrector
-        set_src<R>(h, a, es); set_out<R>(h, a, s); a.kind = 2; a.det = v3<R>(det); a.nz_mode = 2;
+        a.src = c3<R>(es); a.out = v3<R>(s); a.kind = 2; a.det = v3<R>(det); a.nz_mode = 2;
         if (comp) a.out_lo = Vec3<float>{{h->sl[0], h->sl[1], h->sl[2]}};
         a.lr = none;
         if (L.mode == ASD_LR_FFT) {
@@ -555,7 +536,7 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
     for (int st = 0; st < nst; st++) {
         a.kind = 10 + st;
         a.nz_mode = st == 0 ? 1 : 2;
-        set_src<R>(h, a, st == 0 ? s : pp[(st - 1) & 1]);
+        a.src = st == 0 ? c3<R>(s) : c3<R>(pp[(st - 1) & 1]);
         for (int q = 0; q < 6; q++) {
             if constexpr (sizeof(R) == 4) a.k[q] = v3<R>(h->kf[q]); else a.k[q] = v3<R>(h->kd[q]);
         }
@@ -568,10 +549,10 @@ cudaError_t fused_step_t(asd_handle* h, uint32_t rel) {
             if (st == nst - 1 && (t + 1) % upd == 0) a.lr.mr = L.r;
         }
         if (st == nst - 1) {
-            set_out<R>(h, a, s);
+            a.out = v3<R>(s);
             if (comp) a.out_lo = Vec3<float>{{h->sl[0], h->sl[1], h->sl[2]}};
         } else {
-            set_out<R>(h, a, pp[st & 1]);
+            a.out = v3<R>(pp[st & 1]);
         }
         if ((e = run(a)) != cudaSuccess) return e;
     }
@@ -587,8 +568,8 @@ cudaError_t time_first_stage_t(asd_handle* h, int warm, int reps, float* ms) {
     const bool comp = sizeof(R) == 4 && (h->p.flags & ASD_FLAG_COMPENSATED);
     StageArgs<R> a{};
     a.base = c3<R>(s);
-    set_src<R>(h, a, s);
-    set_out<R>(h, a, es);
+    a.src = c3<R>(s);
+    a.out = v3<R>(es);
     a.fn = v3<R>(fn);
     if (stag[0]) a.stag = c3<R>(stag);
     a.lr.P = h->lr.P; a.lr.idx = h->lr.mesh_idx; a.lr.w = h->lr.w;

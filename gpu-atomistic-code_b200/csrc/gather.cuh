@@ -100,19 +100,6 @@ __device__ __forceinline__ const R* table_of(const DiaDev& m) {
 template <bool FULL>
 __host__ __device__ constexpr uint32_t table_stride() { return FULL ? 12u : 4u; }
 
-// Neighbour spin j: one 16-byte load from the packed copy in the FP32 form, three loads from the
-// component arrays in the FP64 form.
-template <typename R>
-__device__ __forceinline__ void load_spin(const CVec3<R>& s, const float4* s4, uint32_t j, R& x, R& y, R& z) {
-    if constexpr (sizeof(R) == 4) {
-        const float4 v = __ldg(s4 + j);
-        x = v.x; y = v.y; z = v.z;
-    } else {
-        (void)s4;
-        x = __ldg(s.p[0] + j); y = __ldg(s.p[1] + j); z = __ldg(s.p[2] + j);
-    }
-}
-
 // h += J_t (x, y, z) for tensor id t of the shared-memory table (type-major rows).
 template <typename R, bool FULL>
 __device__ __forceinline__ void accumulate_typed(const R* tab, uint32_t t, R x, R y, R z, R h[3]) {
@@ -144,9 +131,9 @@ __device__ __forceinline__ void accumulate_typed(const R* tab, uint32_t t, R x, 
 
 // h += sum over the row's entries of J_e S_col(e), SELL-32 layout (one warp per slice).
 template <typename R, bool FULL>
-__device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const CVec3<R>& s, const float4* s4,
-                                            const R* tab, R h[3], const uint32_t* staged = nullptr,
-                                            uint32_t wbase = 0, const R* sspin = nullptr) {
+__device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const CVec3<R>& s, const R* tab, R h[3],
+                                            const uint32_t* staged = nullptr, uint32_t wbase = 0,
+                                            const R* sspin = nullptr) {
     const uint32_t sl = i >> 5, lane = i & 31u;
     const uint32_t p0 = __ldg(m.slice_ptr + sl), p1 = __ldg(m.slice_ptr + sl + 1);
     if (m.typed && staged && sspin) {
@@ -163,24 +150,22 @@ __device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const 
     if (m.typed && staged) {
         // this block's words are in shared memory, indexed from the block's first entry
         const uint32_t mask = (1u << m.colbits) - 1u, cb = m.colbits;
-#pragma unroll 2
+#pragma unroll 4
         for (uint32_t e = p0 - wbase + lane; e < p1 - wbase; e += 32) {
             const uint32_t w = staged[e];
             const uint32_t j = w & mask, t = w >> cb;
-            R x, y, z;
-            load_spin<R>(s, s4, j, x, y, z);
+            const R x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
             accumulate_typed<R, FULL>(tab, t, x, y, z, h);
         }
         return;
     }
     if (m.typed) {
         const uint32_t mask = (1u << m.colbits) - 1u, cb = m.colbits;
-#pragma unroll 2
+#pragma unroll 4
         for (uint32_t e = p0 + lane; e < p1; e += 32) {
             const uint32_t w = ldcs(m.typed + e);
             const uint32_t j = w & mask, t = w >> cb;
-            R x, y, z;
-            load_spin<R>(s, s4, j, x, y, z);
+            const R x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
             accumulate_typed<R, FULL>(tab, t, x, y, z, h);
         }
         return;
@@ -190,8 +175,7 @@ __device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const 
         for (uint32_t e = p0 + lane; e < p1; e += 32) {
             const float4 a = ldcs(m.a + e);
             const int j = __float_as_int(a.x);
-            float x, y, z;
-            load_spin<R>(s, s4, (uint32_t)j, x, y, z);
+            const float x = __ldg(s.p[0] + j), y = __ldg(s.p[1] + j), z = __ldg(s.p[2] + j);
             if (!FULL) {
                 h[0] = fmaf(a.y, x, h[0]);
                 h[1] = fmaf(a.z, y, h[1]);
@@ -225,8 +209,8 @@ __device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const 
 
 // h += sum over diagonals d with 0 <= i+off[d] < n of J_{d,i} S_{i+off[d]}, row-aligned DIA.
 template <typename R, bool FULL>
-__device__ __forceinline__ void gather_dia(const DiaDev& m, uint32_t n, uint32_t i, const CVec3<R>& s,
-                                           const float4* s4, const R* tab, R h[3]) {
+__device__ __forceinline__ void gather_dia(const DiaDev& m, uint32_t n, uint32_t i, const CVec3<R>& s, const R* tab,
+                                           R h[3]) {
     // the warp walks its tile's active diagonals (warp-uniform list)
     const uint32_t k0 = __ldg(m.tile_ptr + (i >> 5)), k1 = __ldg(m.tile_ptr + (i >> 5) + 1);
     if (m.dtype) {
@@ -236,8 +220,7 @@ __device__ __forceinline__ void gather_dia(const DiaDev& m, uint32_t n, uint32_t
             if (col < 0 || col >= (int64_t)n) continue;
             const uint32_t t = ldcs(m.dtype + (size_t)d * n + i);
             if (t == 0) continue;
-            R x, y, z;
-            load_spin<R>(s, s4, (uint32_t)col, x, y, z);
+            const R x = __ldg(s.p[0] + col), y = __ldg(s.p[1] + col), z = __ldg(s.p[2] + col);
             accumulate_typed<R, FULL>(tab, t, x, y, z, h);
         }
         return;
@@ -250,8 +233,7 @@ __device__ __forceinline__ void gather_dia(const DiaDev& m, uint32_t n, uint32_t
         const int64_t col = (int64_t)i + __ldg(m.off + d);
         if (col < 0 || col >= (int64_t)n) continue;
         const size_t a = (size_t)d * n + i;
-        R x, y, z;
-        load_spin<R>(s, s4, (uint32_t)col, x, y, z);
+        const R x = __ldg(s.p[0] + col), y = __ldg(s.p[1] + col), z = __ldg(s.p[2] + col);
         if (!FULL) {
             h[0] += ldcs(v + a) * x;
             h[1] += ldcs(v + ND + a) * y;

@@ -152,7 +152,6 @@ struct asd_handle {
     uint64_t* d_step = nullptr;
     // FP32 / FP64-fused state, SoA
     float *sf[3] = {nullptr}, *sl[3] = {nullptr}, *esf[3] = {nullptr}, *fnf[3] = {nullptr};
-    float4* s4[3] = {nullptr, nullptr, nullptr};   // packed (x, y, z, 0) copies of sf, esf, fnf for the gathers
     float *kf[6][3] = {{nullptr}};
     float *detf[3] = {nullptr}, *stagf[3] = {nullptr};
     double *sd[3] = {nullptr}, *esd[3] = {nullptr}, *fnd[3] = {nullptr}, *kd[6][3] = {{nullptr}};

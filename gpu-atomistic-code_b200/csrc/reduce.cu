@@ -83,8 +83,7 @@ __global__ void mag_final(uint32_t nrep, uint32_t nsub, uint32_t nchunk, const d
 
 template <typename R>
 __global__ void spins_in_k(uint32_t n, const double* __restrict__ aos, R* __restrict__ x, R* __restrict__ y,
-                           R* __restrict__ z, float* __restrict__ lx, float* __restrict__ ly, float* __restrict__ lz,
-                           float4* __restrict__ packed) {
+                           R* __restrict__ z, float* __restrict__ lx, float* __restrict__ ly, float* __restrict__ lz) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double v[3] = {aos[3 * (size_t)i], aos[3 * (size_t)i + 1], aos[3 * (size_t)i + 2]};
@@ -92,7 +91,6 @@ __global__ void spins_in_k(uint32_t n, const double* __restrict__ aos, R* __rest
     v[0] /= m; v[1] /= m; v[2] /= m;
     const R hx = (R)v[0], hy = (R)v[1], hz = (R)v[2];
     x[i] = hx; y[i] = hy; z[i] = hz;
-    if (packed) packed[i] = make_float4((float)hx, (float)hy, (float)hz, 0.0f);
     if (lx) { lx[i] = (float)(v[0] - (double)hx); ly[i] = (float)(v[1] - (double)hy); lz[i] = (float)(v[2] - (double)hz); }
 }
 
@@ -110,8 +108,8 @@ __global__ void soa_out_k(uint32_t n, const R* __restrict__ x, const R* __restri
 // Exchange (+ held long-range) field of the current spins, AoS double out.
 template <typename R, int EX, bool FULL>
 __global__ void field_k(StepConst c, SellDev sell, DiaDev dia, const R* __restrict__ sx, const R* __restrict__ sy,
-                        const R* __restrict__ sz, const float4* __restrict__ s4, const float* __restrict__ hr,
-                        float inv_p, size_t P, const uint32_t* __restrict__ idx, double* __restrict__ out) {
+                        const R* __restrict__ sz, const float* __restrict__ hr, float inv_p, size_t P,
+                        const uint32_t* __restrict__ idx, double* __restrict__ out) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R* tab = reinterpret_cast<R*>(smem_raw);
     if constexpr (EX == ASD_EXCH_CSR) {
@@ -124,11 +122,11 @@ __global__ void field_k(StepConst c, SellDev sell, DiaDev dia, const R* __restri
     if (i >= c.n) return;
     R hr3[3] = {R(0), R(0), R(0)};
     const CVec3<R> src{{sx, sy, sz}};
-    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, src, s4, tab, hr3);
-    if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, src, s4, tab, hr3);
+    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, src, tab, hr3);
+    if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, src, tab, hr3);
     if (c.q4_ptr) {
         R h4[3];
-        four_spin<R>(c, i, [&](uint32_t j, R v[3]) { load_spin<R>(src, s4, j, v[0], v[1], v[2]); }, h4);
+        four_spin<R>(c, i, [&](uint32_t j, R v[3]) { v[0] = src.p[0][j]; v[1] = src.p[1][j]; v[2] = src.p[2][j]; }, h4);
         hr3[0] += h4[0]; hr3[1] += h4[1]; hr3[2] += h4[2];
     }
     double h[3] = {(double)hr3[0], (double)hr3[1], (double)hr3[2]};
@@ -150,7 +148,6 @@ template <typename R>
 cudaError_t field_t(asd_handle* h, double* out) {
     R* s[3];
     state<R>(h, s);
-    const float4* s4 = sizeof(R) == 4 ? h->s4[0] : nullptr;
     const float* hr = nullptr;
     if (h->lr.mode != ASD_LR_NONE) {
         if (h->lr.mode == ASD_LR_FFT) {
@@ -164,14 +161,14 @@ cudaError_t field_t(asd_handle* h, double* out) {
     const size_t cs = sizeof(R) * (h->full ? table_stride<true>() : table_stride<false>());
     if (h->dexch == ASD_EXCH_CSR) {
         const size_t sm = h->sell.typed ? cs * h->sell.ntypes : 0;
-        if (h->full) field_k<R, ASD_EXCH_CSR, true><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], s4, hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
-        else field_k<R, ASD_EXCH_CSR, false><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], s4, hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        if (h->full) field_k<R, ASD_EXCH_CSR, true><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        else field_k<R, ASD_EXCH_CSR, false><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
     } else if (h->dexch == ASD_EXCH_DIA) {
         const size_t sm = h->dia.dtype ? cs * h->dia.ntypes : 0;
-        if (h->full) field_k<R, ASD_EXCH_DIA, true><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], s4, hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
-        else field_k<R, ASD_EXCH_DIA, false><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], s4, hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        if (h->full) field_k<R, ASD_EXCH_DIA, true><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        else field_k<R, ASD_EXCH_DIA, false><<<g, 256, sm, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
     } else {
-        field_k<R, ASD_EXCH_NONE, false><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], s4, hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
+        field_k<R, ASD_EXCH_NONE, false><<<g, 256, 0, h->stream>>>(h->sc, h->sell, h->dia, s[0], s[1], s[2], hr, inv_p, h->lr.P, h->lr.mesh_idx, out);
     }
     h->launches += 1;
     return cudaGetLastError();
@@ -284,10 +281,9 @@ cudaError_t launch_convert_spins_in(asd_handle* h, const double* d_aos) {
     if (h->p.precision == ASD_FP32) {
         const bool comp = (h->p.flags & ASD_FLAG_COMPENSATED) != 0;
         spins_in_k<float><<<g, 256, 0, h->stream>>>(h->n, d_aos, h->sf[0], h->sf[1], h->sf[2], comp ? h->sl[0] : nullptr,
-                                                     comp ? h->sl[1] : nullptr, comp ? h->sl[2] : nullptr, h->s4[0]);
+                                                     comp ? h->sl[1] : nullptr, comp ? h->sl[2] : nullptr);
     } else {
-        spins_in_k<double><<<g, 256, 0, h->stream>>>(h->n, d_aos, h->sd[0], h->sd[1], h->sd[2], nullptr, nullptr, nullptr,
-                                                      nullptr);
+        spins_in_k<double><<<g, 256, 0, h->stream>>>(h->n, d_aos, h->sd[0], h->sd[1], h->sd[2], nullptr, nullptr, nullptr);
     }
     h->launches += 1;
     return cudaGetLastError();
