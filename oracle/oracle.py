@@ -443,6 +443,21 @@ class RefCUDA(RefLLGCPU):
         self.L.refg_get_det_field(_ptr(out, C.c_double))
         return out.reshape(self.n, 3)
 
+    def enable_curand(self, seed):
+        """Draw Crand with cuRAND XORWOW every step, seeded as cullg::cuinit does (src/cuda.cu:345-368)."""
+        self.L.refg_enable_curand.argtypes = [C.c_ulonglong]
+        if self.L.refg_enable_curand(seed) != 0:
+            raise RuntimeError("refg_enable_curand failed")
+
+    def time_steps_cold(self, nsteps, flush_bytes=256 << 20):
+        """Device ms of nsteps Heun steps, each after an untimed L2 flush, CUDA events per step."""
+        ms = C.c_double()
+        self.L.refg_time_steps.argtypes = [C.c_int, C.c_uint, C.c_size_t, dp]
+        rc = self.L.refg_time_steps(self.integrator, nsteps, flush_bytes, C.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"refg_time_steps failed ({rc})")
+        return ms.value
+
     def close(self):
         self.L.refg_free()
 

@@ -16,6 +16,7 @@
 // links it.
 #include <cuda_runtime.h>
 #include <cufft.h>
+#include <curand.h>
 #include <libconfig.h++>
 #include "../inc/arrays.h"
 #include "../inc/exch.h"
@@ -52,6 +53,7 @@ struct Dev {
     std::vector<void*> owned;
 };
 Dev g;
+curandGenerator_t gen = nullptr;   // set: every step draws Crand as src/cuda.cu:148 does
 
 template <class T>
 T* upload(const T* src, size_t n) {
@@ -179,10 +181,12 @@ int refg_run(int integrator, unsigned nsteps) {
     const unsigned nb = (g.n + g.block - 1) / g.block;
     const double T = llg::T, ax = llg::applied[0], ay = llg::applied[1], az = llg::applied[2];
     for (unsigned t = 0; t < nsteps; t++) {
+        if (integrator != 0 && gen) curandGenerateNormal(gen, g.rand, g.curand_n, 0.0f, 1.0f);  // src/cudaRK4.cu:41
         if (integrator == 0) {
             spmv(g.spin);
             if (exch::inc4spin)
                 cufields::CSpMV_CSR_FourSpin<<<nb, g.block>>>(g.n, g.q_xadj, g.q_j, g.q_k, g.q_l, g.h, g.spin);
+            if (gen) curandGenerateNormal(gen, g.rand, g.curand_n, 0.0f, 1.0f);                  // src/cuda.cu:148
             cuint::CHeun1<<<nb, g.block>>>(g.n, T, ax, ay, az, g.h, g.spin, g.espin, g.rand, g.fn, g.sigma, g.llgpf,
                                            g.lambda, g.k1u, g.k1udir, g.hstg);
             spmv(g.espin);
@@ -233,6 +237,62 @@ int refg_run(int integrator, unsigned nsteps) {
     return status();
 }
 
+// cuRAND XORWOW seeded as cullg::cuinit does (src/cuda.cu:345-368); from then on every step
+// draws its own Crand like the reference instead of reading the caller's.
+int refg_enable_curand(unsigned long long seed) {
+    if (gen) { curandDestroyGenerator(gen); gen = nullptr; }
+    if (curandCreateGenerator(&gen, CURAND_RNG_PSEUDO_DEFAULT) != CURAND_STATUS_SUCCESS) { gen = nullptr; return -1; }
+    if (curandSetPseudoRandomGeneratorSeed(gen, seed) != CURAND_STATUS_SUCCESS) return -1;
+    if (curandGenerateSeeds(gen) != CURAND_STATUS_SUCCESS) return -1;
+    return status();
+}
+
+// Device time of nsteps steps, each preceded by an untimed write of flush_bytes (the L2
+// flushed as the library's cold timers do) and bracketed by its own CUDA events.
+int refg_time_steps(int integrator, unsigned nsteps, size_t flush_bytes, double* ms) {
+    if (!g.spin || !ms) return -1;
+    void* flush = nullptr;
+    if (flush_bytes && cudaMalloc(&flush, flush_bytes) != cudaSuccess) return -2;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double total = 0.0;
+    int rc = 0;
+    for (unsigned t = 0; t < nsteps && rc == 0; t++) {
+        if (flush) cudaMemset(flush, t & 0xFF, flush_bytes);
+        cudaEventRecord(e0, 0);
+        const unsigned nb = (g.n + g.block - 1) / g.block;
+        // one step, without the synchronising status() of refg_run
+        const double T = llg::T, ax = llg::applied[0], ay = llg::applied[1], az = llg::applied[2];
+        if (integrator == 0) {
+            spmv(g.spin);
+            if (exch::inc4spin)
+                cufields::CSpMV_CSR_FourSpin<<<nb, g.block>>>(g.n, g.q_xadj, g.q_j, g.q_k, g.q_l, g.h, g.spin);
+            if (gen) curandGenerateNormal(gen, g.rand, g.curand_n, 0.0f, 1.0f);
+            cuint::CHeun1<<<nb, g.block>>>(g.n, T, ax, ay, az, g.h, g.spin, g.espin, g.rand, g.fn, g.sigma, g.llgpf,
+                                           g.lambda, g.k1u, g.k1udir, g.hstg);
+            spmv(g.espin);
+            if (exch::inc4spin)
+                cufields::CSpMV_CSR_FourSpin<<<nb, g.block>>>(g.n, g.q_xadj, g.q_j, g.q_k, g.q_l, g.h, g.espin);
+            cuint::CHeun2<<<nb, g.block>>>(g.n, T, ax, ay, az, g.h, g.spin, g.espin, g.rand, g.fn, g.sigma, g.llgpf,
+                                           g.lambda, g.k1u, g.k1udir, g.det, g.hstg);
+        } else {
+            rc = -1;
+        }
+        cudaEventRecord(e1, 0);
+        if (cudaEventSynchronize(e1) != cudaSuccess) rc = -3;
+        float m = 0.f;
+        cudaEventElapsedTime(&m, e0, e1);
+        total += m;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (flush) cudaFree(flush);
+    *ms = total;
+    const int st = status();
+    return rc ? rc : st;
+}
+
 int refg_get_spins(double* out) {
     if (!g.spin) return -1;
     cudaMemcpy(out, g.spin, 3 * (size_t)g.n * sizeof(double), cudaMemcpyDeviceToHost);
@@ -246,5 +306,8 @@ int refg_get_det_field(double* out) {
     return status();
 }
 
-void refg_free() { release(); }
+void refg_free() {
+    release();
+    if (gen) { curandDestroyGenerator(gen); gen = nullptr; }
+}
 }

@@ -143,3 +143,37 @@ def test_reference_side_binding(gpu, T):
         ref.step(50)
         assert maxdiff(got, ref.spins()) <= 1e-10
         ref.close()
+
+
+@pytest.mark.parametrize("name,builder", [
+    ("bct2_64", lambda: LT.bct2_antiferromagnet(64, layout="csr", T=300.0)),
+    ("bct2_64_dia", lambda: LT.bct2_antiferromagnet(64, layout="dia", T=300.0)),
+    ("sc16", lambda: LT.sc_ferromagnet(16, T=300.0)),
+])
+def test_reference_kernels_timed(gpu, name, builder):
+    """The reference's own Heun step on this GPU (cuRAND XORWOW draw, SpMV, CHeun1, SpMV, CHeun2 at
+    256 threads per block, src/cuda.cu:43-258), timed like the library: untimed 256 MB write before
+    each step, CUDA events per step.  Prints one JSON line per workload beside the library's FP32
+    form on the same lattice; checks only that both ran and kept unit spins."""
+    import json
+    s = builder()
+    S0 = LT.random_spins(s.nspins, 0)
+    ref = O.RefCUDA(s, block=256)
+    ref.enable_curand(1)
+    ref.set_spins(S0)
+    ref.step(3)
+    steps = 20
+    ms_ref = ref.time_steps_cold(steps)
+    rs = ref.spins()
+    ref.close()
+    assert np.allclose(np.linalg.norm(rs, axis=1), 1.0, atol=1e-12)
+    p = A.RunParams(precision=A.FP32, flags=A.FLAG_COMPENSATED | A.FLAG_AUTOTUNE, seed=1)
+    with A.Handle(p, s) as h:
+        h.set_spins(S0)
+        h.step(3)
+        ms_ours, _ = h.time_steps_cold(steps)
+        assert np.allclose(np.linalg.norm(h.get_spins(), axis=1), 1.0, atol=1e-6)
+    line = {"workload": name, "nspins": s.nspins, "steps": steps,
+            "reference_cuda_fp64_spin_updates_per_s": s.nspins * steps / (ms_ref * 1e-3),
+            "library_fp32_spin_updates_per_s": s.nspins * steps / (ms_ours * 1e-3)}
+    print("REFTIMING " + json.dumps(line))
