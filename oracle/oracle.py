@@ -443,6 +443,13 @@ class RefCUDA(RefLLGCPU):
         self.L.refg_get_det_field(_ptr(out, C.c_double))
         return out.reshape(self.n, 3)
 
+    def buffer(self, which):
+        """Work array after the last step: 0..5 CRKk1..6, 6 Cespin, 7 CH."""
+        out = np.empty(3 * self.n)
+        self.L.refg_get_buffer.argtypes = [C.c_int, dp]
+        self.L.refg_get_buffer(which, _ptr(out, C.c_double))
+        return out.reshape(self.n, 3)
+
     def enable_curand(self, seed):
         """Draw Crand with cuRAND XORWOW every step, seeded as cullg::cuinit does (src/cuda.cu:345-368)."""
         self.L.refg_enable_curand.argtypes = [C.c_ulonglong]
@@ -487,12 +494,20 @@ class RefShim(RefLLGCPU):
         L.refs_configure(integrator, seed, update, precision, flags)
         self._keep_shim = [atoms, coords, k1u, dirs, sub]
 
+    def _check(self, what):
+        self.L.refh_last_error.restype = C.c_char_p
+        msg = self.L.refh_last_error().decode()
+        if msg:
+            raise RuntimeError(f"{what}: {msg}")
+
     def set_spins(self, s):
         super().set_spins(s)
         self.L.refs_cuinit()
+        self._check("cullg::cuinit")
 
     def step(self, k):
         self.L.refs_run(self.t, k)
+        self._check("cullg::llgGPU")
         self.t += k
         return 0
 

@@ -299,6 +299,14 @@ int refg_get_spins(double* out) {
     return status();
 }
 
+// A work array after the last step: 0..5 CRKk1..CRKk6, 6 Cespin, 7 CH (3N doubles each).
+int refg_get_buffer(int which, double* out) {
+    if (!g.spin || which < 0 || which > 7) return -1;
+    const double* src = which < 6 ? g.rk[which] : which == 6 ? g.espin : g.h;
+    cudaMemcpy(out, src, 3 * (size_t)g.n * sizeof(double), cudaMemcpyDeviceToHost);
+    return status();
+}
+
 // CDetFields: the Heun corrector's total field less the thermal term (src/cuint.cu:238).
 int refg_get_det_field(double* out) {
     if (!g.det) return -1;

@@ -28,6 +28,8 @@
 #include <cstring>
 #include <cstdio>
 #include <vector>
+#include <sstream>
+#include <string>
 
 namespace geom {
 unsigned int nspins = 0;
@@ -70,11 +72,14 @@ unsigned int exchm = 2, dipm = 0;
 bool inc_dip = false, offdiag = false;
 void printline(std::ofstream&) {}
 }
+// error::errMessage exits in the reference (src/error.cpp:19-28); here it records the message
+// for refh_last_error and returns.
+static std::string g_last_error;
 namespace error {
 void errPreamble(std::string, int) {}
 void errWarnPreamble(std::string, int) {}
-void errMessage(std::string) {}
-void errMessage(std::stringstream&) {}
+void errMessage(std::string m) { g_last_error = m; }
+void errMessage(std::stringstream& m) { g_last_error = m.str(); }
 void errWarning(std::string) {}
 }
 
@@ -152,6 +157,14 @@ int refh_init(unsigned n, unsigned nauc, const double* mu, const double* lam, co
 }
 
 void refh_set_temperature(double T) { llg::T = T; }
+
+// The last message passed to error::errMessage ("" if none), then cleared.
+const char* refh_last_error() {
+    static std::string out;
+    out = g_last_error;
+    g_last_error.clear();
+    return out.c_str();
+}
 
 // k1u per spin already scaled as in src/geom.cpp:244 (2K/(mu muB)).
 int refh_set_anis(const double* k1u, const double* k1udir, double k2perp, const double* k2perpdir,

@@ -133,6 +133,7 @@ def test_reference_side_binding(gpu, T):
     shim.step(50)
     got = shim.spins()
     shim.close()
+    assert maxdiff(got, S0) > 1e-3                 # the mirror was refreshed by real steps
     with A.Handle(A.RunParams(precision=A.FP64_PLAIN, seed=3), s) as h:
         h.set_spins(S0)
         h.step(50)
