@@ -902,7 +902,7 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         {
             uint32_t maxrep = 0;
             for (uint32_t r = 0; r < nsys; r++) maxrep = std::max(maxrep, h->h_rep_off[r + 1] - h->h_rep_off[r]);
-            const uint32_t nchunk = (maxrep + 8191) / 8192;
+            const uint32_t nchunk = (maxrep + MAG_CHUNK - 1) / MAG_CHUNK;
             h->magpart_len = (size_t)nsys * nchunk * h->nsub * 3;
             h->d_magpart = dalloc<double>(h->magpart_len);
             h->d_mag = dalloc<double>((size_t)nsys * h->nsub * 3);

@@ -43,6 +43,7 @@ struct SellDev {
     uint4* spans = nullptr;          // (start, len, off, 0) in elements
     uint32_t spin_slots = 0, spin_block = 0;
 };
+constexpr uint32_t MAG_CHUNK = 1024;  // spins per block of the magnetisation reduction
 constexpr uint32_t SPIN_PAD = 8;     // zeroed elements after every gather-source spin array
 
 // Row-aligned DIA, values component-major val[c][d*N+row], c = 3 (diag) or 9;

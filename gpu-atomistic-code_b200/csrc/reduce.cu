@@ -7,7 +7,6 @@ namespace asd {
 namespace {
 
 inline unsigned nb(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
-constexpr int MAG_CHUNK = 8192;
 constexpr int MAG_BLOCK = 256;
 
 __device__ __forceinline__ double block_sum(double v, double* sm) {
@@ -51,6 +50,44 @@ __global__ void mag_partial(StepConst c, uint32_t nsub, const uint32_t* __restri
 }
 
 // Plain form: AoS doubles.
+// One pass over the chunk for up to NS sublattices, each spin added to its own sublattice's
+// register accumulators (the general kernel above re-reads the chunk once per sublattice).
+template <typename R, int NS>
+__global__ void mag_partial_ns(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
+                               const R* __restrict__ sx, const R* __restrict__ sy, const R* __restrict__ sz,
+                               const float* __restrict__ lx, const float* __restrict__ ly,
+                               const float* __restrict__ lz, uint32_t nchunk, double* __restrict__ part) {
+    __shared__ double sm[32];
+    const uint32_t r = blockIdx.y, ch = blockIdx.x;
+    const uint32_t beg = c.rep_off[r] + ch * MAG_CHUNK;
+    const uint32_t end = min(c.rep_off[r + 1], beg + MAG_CHUNK);
+    double a[NS][3];
+#pragma unroll
+    for (int q = 0; q < NS; q++) a[q][0] = a[q][1] = a[q][2] = 0.0;
+    for (uint32_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+        const uint32_t s = NS == 1 ? 0u : sub_of_atom[atom_of(c, i)];
+        double v0 = (double)sx[i], v1 = (double)sy[i], v2 = (double)sz[i];
+        if (lx) { v0 += (double)lx[i]; v1 += (double)ly[i]; v2 += (double)lz[i]; }
+#pragma unroll
+        for (int q = 0; q < NS; q++)
+            if (s == (uint32_t)q) { a[q][0] += v0; a[q][1] += v1; a[q][2] += v2; }
+    }
+    for (uint32_t q = 0; q < nsub; q++) {
+        double t[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            double v = 0.0;
+#pragma unroll
+            for (int qq = 0; qq < NS; qq++) if ((uint32_t)qq == q) v = a[qq][k];
+            t[k] = block_sum(v, sm);
+        }
+        if (threadIdx.x == 0) {
+            double* o = part + (((size_t)r * nchunk + ch) * nsub + q) * 3;
+            o[0] = t[0]; o[1] = t[1]; o[2] = t[2];
+        }
+    }
+}
+
 __global__ void mag_partial_aos(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
                                 const double* __restrict__ s3, uint32_t nchunk, double* __restrict__ part) {
     __shared__ double sm[32];
@@ -264,9 +301,19 @@ cudaError_t launch_magnetisation(asd_handle* h) {
         mag_partial_aos<<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->p_s, grid.x, h->d_magpart);
     } else if (h->p.precision == ASD_FP32) {
         const bool comp = (h->p.flags & ASD_FLAG_COMPENSATED) != 0;
-        mag_partial<float><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1], h->sf[2],
-                                                             comp ? h->sl[0] : nullptr, comp ? h->sl[1] : nullptr,
-                                                             comp ? h->sl[2] : nullptr, grid.x, h->d_magpart);
+        const float* lo[3] = {comp ? h->sl[0] : nullptr, comp ? h->sl[1] : nullptr, comp ? h->sl[2] : nullptr};
+        if (nsub == 1)
+            mag_partial_ns<float, 1><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1],
+                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart);
+        else if (nsub == 2)
+            mag_partial_ns<float, 2><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1],
+                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart);
+        else if (nsub <= 4)
+            mag_partial_ns<float, 4><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1],
+                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart);
+        else
+            mag_partial<float><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1], h->sf[2],
+                                                                 lo[0], lo[1], lo[2], grid.x, h->d_magpart);
     } else {
         mag_partial<double><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sd[0], h->sd[1], h->sd[2],
                                                               nullptr, nullptr, nullptr, grid.x, h->d_magpart);

@@ -130,12 +130,13 @@ def test_reference_side_binding(gpu, T):
     S0 = LT.random_spins(s.nspins, 0)
     shim = O.RefShim(s, precision=A.FP64_PLAIN, seed=3)
     shim.set_spins(S0)
+    S0n = shim.spins()          # as spins::Sx/Sy/Sz hold them: divided by their length once already
     shim.step(50)
     got = shim.spins()
     shim.close()
     assert maxdiff(got, S0) > 1e-3                 # the mirror was refreshed by real steps
     with A.Handle(A.RunParams(precision=A.FP64_PLAIN, seed=3), s) as h:
-        h.set_spins(S0)
+        h.set_spins(S0n)
         h.step(50)
         assert np.array_equal(got, h.get_spins())
     if T == 0.0:
