@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
     R sv[3] = {a.src.p[0][i], a.src.p[1][i], a.src.p[2][i]};
     const int kind = a.kind;
     if constexpr (K >= 3) {
-        if (kind >= 11 && (c.flags & ASD_FLAG_RK_STAGE_SPIN_MIXED)) { sv[1] = a.base.p[1][i]; sv[2] = a.base.p[2][i]; }
+        if (kind >= 11 && (c.flags & ASD_FLAG_RK_STAGE_SPIN_MIXED)) sv[1] = a.base.p[1][i];
     }
     anis_field<R>(c, mc, sv, h);
     R f[3];

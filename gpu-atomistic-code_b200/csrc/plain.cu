@@ -192,7 +192,7 @@ __global__ void plain_rk_stage(StepConst c, PlainSpin ps, int nst, int st, const
     const double S[3] = {sp[3 * i], sp[3 * i + 1], sp[3 * i + 2]};
     double sv[3];
     if (st == 0) { sv[0] = S[0]; sv[1] = S[1]; sv[2] = S[2]; }
-    else if (mixed) { sv[0] = es[3 * i]; sv[1] = S[1]; sv[2] = S[2]; }
+    else if (mixed) { sv[0] = es[3 * i]; sv[1] = S[1]; sv[2] = es[3 * i + 2]; }
     else { sv[0] = es[3 * i]; sv[1] = es[3 * i + 1]; sv[2] = es[3 * i + 2]; }
     double h[3], lrn[3], k[3];
     plain_total_field(c, ps, i, ch, rnd, sv, h, lrn);

@@ -770,7 +770,7 @@ static void rk_step(orc_ctx* c, uint64_t t) {
             const double* S = c->s + 3 * (size_t)i;
             double sv[3];
             if (st == 0) memcpy(sv, S, sizeof(sv));
-            else if (mixed) { sv[0] = c->es[3 * (size_t)i]; sv[1] = S[1]; sv[2] = S[2]; }
+            else if (mixed) { sv[0] = c->es[3 * (size_t)i]; sv[1] = S[1]; sv[2] = c->es[3 * (size_t)i + 2]; }
             else memcpy(sv, c->es + 3 * (size_t)i, sizeof(sv));
             double h[3], lrn[3], k[3];
             total_field(c, i, c->h, sv, h, lrn);

@@ -28,7 +28,7 @@ extern "C" {
 #define ORC_CPU_CORRECTOR_ACCUM   (1u << 0)  /* src/llgCPU.cpp:58-60,253-274: corrector exchange = H(S)+H(S') */
 #define ORC_CPU_THERMAL_Z_FROM_X  (1u << 1)  /* src/llgCPU.cpp:180,302: z thermal uses Hthx */
 #define ORC_RK_DOUBLE_RDT         (1u << 2)  /* src/cuintRK4.cu:141-142, src/cuintRK5.cu:158-159: stage uses rdt*k with k incl. rdt */
-#define ORC_RK_STAGE_SPIN_MIXED   (1u << 3)  /* src/cuintRK4.cu:172,266,359; src/cuintRK5.cu:189,283,376,468,560: es={eS.x,S.y,S.z} */
+#define ORC_RK_STAGE_SPIN_MIXED   (1u << 3)  /* src/cuintRK4.cu:172,266,359; src/cuintRK5.cu:189,283,376,468,560: es={eS.x,S.y,eS.z} */
 #define ORC_GPU_CSR_DIP_STALE     (1u << 4)  /* src/cuda.cu:192-199: CSR+dipole+diag corrector keeps the predictor field */
 #define ORC_CPU_SUM_ORDER         (1u << 5)  /* src/llgCPU.cpp:180,302: llgCPU order of the field terms */
 #define ORC_GPU_DZZ_FROM_DYY      (1u << 6)  /* src/cuda_util.cu:308-312,373-377: zz exchange from yy */
