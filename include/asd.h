@@ -60,7 +60,7 @@ extern "C" {
 /* Reference-compatibility switches (asd_params.flags).  Default 0 = the CUDA
  * path's physics with its bugs fixed. */
 #define ASD_FLAG_RK_DOUBLE_RDT       (1u << 2)  /* src/cuintRK4.cu:141-142, src/cuintRK5.cu:158-159 */
-#define ASD_FLAG_RK_STAGE_SPIN_MIXED (1u << 3)  /* src/cuintRK4.cu:172: es={Cespin.x,Cspin.y,Cespin.z}: y from S */
+#define ASD_FLAG_RK_STAGE_SPIN_MIXED (1u << 3)  /* src/cuintRK4.cu:172: es={Cespin[3i],Cspin[3i+1],Cespin[3i+2]} */
 #define ASD_FLAG_GPU_CSR_DIP_STALE   (1u << 4)  /* src/cuda.cu:192-199 */
 #define ASD_FLAG_GPU_DZZ_FROM_DYY    (1u << 6)  /* src/cuda_util.cu:308-312,373-377 */
 #define ASD_FLAG_GPU_HDEMAG_FP32     (1u << 7)  /* CHDemag stored as float (src/cuda_glob.cu) */
