@@ -1210,11 +1210,9 @@ int asd_set_applied(asd_handle* h, const double applied[3]) {
     if (!h || !applied) return ASD_EINVAL;
     try {
         CK(cudaSetDevice(h->device));
-        for (int a = 0; a < 3; a++) {
-            REQUIRE(std::isfinite(applied[a]), "non-finite applied field");
-            h->p.applied[a] = applied[a];
-            set_dyn(h, DYN_APPLIED + a, applied[a]);
-        }
+        for (int a = 0; a < 3; a++) REQUIRE(std::isfinite(applied[a]), "non-finite applied field");
+        for (int a = 0; a < 3; a++) h->p.applied[a] = applied[a];
+        CK(launch_set_vec3(h, h->d_dyn + DYN_APPLIED, h->d_dynf + DYN_APPLIED, applied));
     } catch (const Fail& f) { return fail(h, f); }
     return ASD_OK;
 }

@@ -215,6 +215,7 @@ cudaError_t launch_field_only(asd_handle* h, double* d_out);
 cudaError_t launch_plain_field(asd_handle* h, double* d_out);
 cudaError_t launch_plain_ramp(asd_handle* h, double rv);
 cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v);
+cudaError_t launch_set_vec3(asd_handle* h, double* dst, float* dstf, const double v[3]);
 cudaError_t launch_set_scalar_f(asd_handle* h, float* dst, float v);
 cudaError_t launch_mag_push(asd_handle* h);
 // one two-temperature-model step for step t (device counter + rel when step_base is set, else t)

@@ -233,9 +233,28 @@ __global__ void mag_push_k(uint32_t m, const double* __restrict__ mag, double* _
 }
 
 __global__ void set_scalar_k(double* dst, double v) { *dst = v; }
+
+struct Dyn3 { double v[3]; };
+// dst[0..2] = v and, when dstf is set, dstf[0..2] = (float)v: the three components of one
+// mutable vector (the applied field) in one launch.
+__global__ void set_vec3_k(double* dst, float* dstf, Dyn3 v) {
+    const int k = threadIdx.x;
+    if (k < 3) {
+        dst[k] = v.v[k];
+        if (dstf) dstf[k] = (float)v.v[k];
+    }
+}
 __global__ void set_scalar_f_k(float* dst, float v) { *dst = v; }
 
 }  // namespace
+
+cudaError_t launch_set_vec3(asd_handle* h, double* dst, float* dstf, const double v[3]) {
+    Dyn3 d;
+    for (int k = 0; k < 3; k++) d.v[k] = v[k];
+    set_vec3_k<<<1, 32, 0, h->stream>>>(dst, dstf, d);
+    h->launches += 1;
+    return cudaGetLastError();
+}
 
 cudaError_t launch_set_scalar(asd_handle* h, double* dst, double v) {
     set_scalar_k<<<1, 1, 0, h->stream>>>(dst, v);
