@@ -380,9 +380,10 @@ constexpr size_t STAGE_SMEM_MAX = 96 * 1024;
 void free_spin_stage(asd_handle* h) {
     SellDev& m = h->sell;
     if (m.lwords) cudaFree(m.lwords);
+    if (m.lwords16) cudaFree(m.lwords16);
     if (m.span_ptr) cudaFree(m.span_ptr);
     if (m.spans) cudaFree(m.spans);
-    m.lwords = nullptr; m.span_ptr = nullptr; m.spans = nullptr;
+    m.lwords = nullptr; m.lwords16 = nullptr; m.lbits = 0; m.span_ptr = nullptr; m.spans = nullptr;
     m.spin_slots = 0; m.spin_block = 0;
 }
 
@@ -407,6 +408,23 @@ bool build_spin_stage(asd_handle* h, int B) {
         return false;
     SellDev& m = h->sell;
     m.lwords = dupload(lw.data(), lw.size());
+    // 16-bit words: slot in the low lbits bits, tensor id above, for the blocks with spans
+    uint32_t lbits = 1;
+    while ((1u << lbits) < slots) lbits++;
+    if (lbits < 16 && (uint64_t)h->sell.ntypes <= (1ull << (16 - lbits))) {
+        const uint32_t cmask = h->sell.colbits >= 32 ? 0xFFFFFFFFu : (1u << h->sell.colbits) - 1u;
+        std::vector<uint16_t> w16(lw.size(), 0);
+        for (uint32_t b = 0; b < nblk; b++) {
+            if (ptr[b + 1] == ptr[b]) continue;                  // no spans: global words, unstaged
+            const uint32_t e0 = sp[b * spb], e1 = sp[std::min((b + 1) * spb, ns)];
+            for (uint32_t e = e0; e < e1; e++) {
+                const uint32_t slot = lw[e] & cmask, t = lw[e] >> h->sell.colbits;
+                w16[e] = (uint16_t)(slot | (t << lbits));
+            }
+        }
+        m.lwords16 = dupload(w16.data(), w16.size());
+        m.lbits = lbits;
+    }
     m.span_ptr = dupload(ptr.data(), ptr.size());
     m.spans = reinterpret_cast<uint4*>(dupload(spans.data(), spans.size()));
     m.spin_slots = slots;

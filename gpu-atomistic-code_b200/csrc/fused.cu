@@ -137,6 +137,7 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
                 bulk_prefetch_l2(static_cast<const char*>(a.pf[q]) + (size_t)r0 * sizeof(R), bytes);
     }
     const uint32_t* staged = nullptr;
+    const uint16_t* staged16 = nullptr;
     const R* sspin = nullptr;
     uint32_t wbase = 0;
     if constexpr (EX == ASD_EXCH_CSR) {
@@ -155,7 +156,36 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
                     sp0 = __ldg(sell.span_ptr + blockIdx.x);
                     nsp = __ldg(sell.span_ptr + blockIdx.x + 1) - sp0;
                 }
-                if (bytes) {
+                const bool w16 = sell.stage == 2 && sell.lwords16;
+                if (w16 && bytes && nsp) {
+                    // 16-bit local words (half the copy and the buffer) and the spans; a block
+                    // without spans stages nothing and reads its global words
+                    const uint32_t bytes16 = bytes >> 1;
+                    uint16_t* wbuf = reinterpret_cast<uint16_t*>(smem_raw + tb);
+                    R* sbuf = reinterpret_cast<R*>(smem_raw + tb + ((2u * sell.stage_words + 15u) & ~15u));
+                    if (threadIdx.x == 0) mbar_init(&stage_bar, 1);
+                    __syncthreads();
+                    if (threadIdx.x < 32) {
+                        if (threadIdx.x == 0) {
+                            uint32_t tx = bytes16;
+                            for (uint32_t q = 0; q < nsp; q++) tx += 3u * sell.spans[sp0 + q].y * (uint32_t)sizeof(R);
+                            mbar_arrive_expect_tx(&stage_bar, tx);
+                        }
+                        __syncwarp();
+                        for (uint32_t k = threadIdx.x; k < 1 + 3 * nsp; k += 32) {
+                            if (k == 0) {
+                                bulk_copy_stream(wbuf, sell.lwords16 + wbase, bytes16, &stage_bar);
+                            } else {
+                                const uint4 sp = sell.spans[sp0 + (k - 1) / 3];
+                                const uint32_t c = (k - 1) % 3;
+                                bulk_copy(sbuf + c * sell.spin_slots + sp.z, a.src.p[c] + sp.x,
+                                          sp.y * (uint32_t)sizeof(R), &stage_bar);
+                            }
+                        }
+                    }
+                    staged16 = wbuf;
+                    sspin = sbuf;
+                } else if (!w16 && bytes) {
                     uint32_t* wbuf = reinterpret_cast<uint32_t*>(smem_raw + tb);
                     R* sbuf = reinterpret_cast<R*>(smem_raw + tb + 4u * sell.stage_words);
                     if (threadIdx.x == 0) mbar_init(&stage_bar, 1);
@@ -217,15 +247,16 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
         if (a.nz_mode == 1) { a.nz.p[0][i] = lrn[0]; a.nz.p[1][i] = lrn[1]; a.nz.p[2][i] = lrn[2]; }
     }
     bool stage_timeout = false;
-    if (staged && !mbar_wait_bounded(&stage_bar, STAGE_WAIT_POLLS)) {
+    if ((staged || staged16) && !mbar_wait_bounded(&stage_bar, STAGE_WAIT_POLLS)) {
         // the copy did not land in time: record it and read the words from global memory
         atomicOr(sell.err, ERR_STAGE_TIMEOUT);
         staged = nullptr;      // the global words carry global columns
+        staged16 = nullptr;
         sspin = nullptr;
         stage_timeout = true;
     }
     R h[3] = {R(0), R(0), R(0)};
-    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, a.src, tab, h, staged, wbase, sspin);
+    if constexpr (EX == ASD_EXCH_CSR) gather_sell<R, FULL>(sell, i, a.src, tab, h, staged, wbase, sspin, staged16);
     if constexpr (EX == ASD_EXCH_DIA) gather_dia<R, FULL>(dia, c.n, i, a.src, tab, h);
     if (c.q4_ptr) {
         R h4[3];
@@ -396,7 +427,10 @@ cudaError_t launch_stage_k(asd_handle* hd, const StageArgs<R>& a) {
     size_t smem = 0;
     if (EX == ASD_EXCH_CSR && hd->sell.typed) {
         smem = sizeof(R) * table_stride<FULL>() * hd->sell.ntypes;
-        if (hd->sell.stage) smem = ((smem + 15) & ~(size_t)15) + 4 * (size_t)hd->sell.stage_words;
+        if (hd->sell.stage == 2 && hd->sell.lwords16)
+            smem = ((smem + 15) & ~(size_t)15) + ((2 * (size_t)hd->sell.stage_words + 15) & ~(size_t)15);
+        else if (hd->sell.stage)
+            smem = ((smem + 15) & ~(size_t)15) + 4 * (size_t)hd->sell.stage_words;
         if (hd->sell.stage == 2) smem += 3 * sizeof(R) * (size_t)hd->sell.spin_slots;
     }
     if (EX == ASD_EXCH_DIA && hd->dia.dtype) smem = sizeof(R) * table_stride<FULL>() *hd->dia.ntypes;

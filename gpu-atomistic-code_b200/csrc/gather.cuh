@@ -133,9 +133,20 @@ __device__ __forceinline__ void accumulate_typed(const R* tab, uint32_t t, R x, 
 template <typename R, bool FULL>
 __device__ __forceinline__ void gather_sell(const SellDev& m, uint32_t i, const CVec3<R>& s, const R* tab, R h[3],
                                             const uint32_t* staged = nullptr, uint32_t wbase = 0,
-                                            const R* sspin = nullptr) {
+                                            const R* sspin = nullptr, const uint16_t* staged16 = nullptr) {
     const uint32_t sl = i >> 5, lane = i & 31u;
     const uint32_t p0 = __ldg(m.slice_ptr + sl), p1 = __ldg(m.slice_ptr + sl + 1);
+    if (m.typed && staged16 && sspin) {
+        // 16-bit words: slot | id << lbits into the staged neighbour spins [3][spin_slots]
+        const uint32_t mask = (1u << m.lbits) - 1u, cb = m.lbits, ns = m.spin_slots;
+#pragma unroll 4
+        for (uint32_t e = p0 - wbase + lane; e < p1 - wbase; e += 32) {
+            const uint32_t w = staged16[e];
+            const uint32_t j = w & mask, t = w >> cb;
+            accumulate_typed<R, FULL>(tab, t, sspin[j], sspin[ns + j], sspin[2 * ns + j], h);
+        }
+        return;
+    }
     if (m.typed && staged && sspin) {
         // words carry block-local slots into the staged neighbour spins [3][spin_slots]
         const uint32_t mask = (1u << m.colbits) - 1u, cb = m.colbits, ns = m.spin_slots;

@@ -39,6 +39,10 @@ struct SellDev {
     // slot offset off in shared memory ([3][spin_slots] components); lwords are the typed words
     // with the column replaced by the slot (blocks without spans keep global columns)
     uint32_t* lwords = nullptr;
+    // the same local words packed to 16 bits (slot | id << lbits) when the largest block's slots
+    // and the tensor ids fit; blocks without spans then read their global words unstaged
+    uint16_t* lwords16 = nullptr;
+    uint32_t lbits = 0;
     uint32_t* span_ptr = nullptr;
     uint4* spans = nullptr;          // (start, len, off, 0) in elements
     uint32_t spin_slots = 0, spin_block = 0;
