@@ -110,12 +110,17 @@ __global__ void mag_partial_aos(StepConst c, uint32_t nsub, const uint32_t* __re
 
 __global__ void mag_final(uint32_t nrep, uint32_t nsub, uint32_t nchunk, const double* __restrict__ part,
                           const double* __restrict__ inv_count, double* __restrict__ out) {
-    const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+    // one block per (replica, sublattice, component): its threads stride over the chunks, then a
+    // block sum (fixed order, so the result does not depend on timing)
+    __shared__ double sm[32];
+    const uint32_t q = blockIdx.x;
     if (q >= nrep * nsub * 3) return;
     const uint32_t comp = q % 3, s = (q / 3) % nsub, r = q / (3 * nsub);
     double acc = 0.0;
-    for (uint32_t ch = 0; ch < nchunk; ch++) acc += part[(((size_t)r * nchunk + ch) * nsub + s) * 3 + comp];
-    out[q] = acc * inv_count[r * nsub + s];
+    for (uint32_t ch = threadIdx.x; ch < nchunk; ch += blockDim.x)
+        acc += part[(((size_t)r * nchunk + ch) * nsub + s) * 3 + comp];
+    const double t = block_sum(acc, sm);
+    if (threadIdx.x == 0) out[q] = t * inv_count[r * nsub + s];
 }
 
 template <typename R>
@@ -337,7 +342,7 @@ cudaError_t launch_magnetisation(asd_handle* h) {
         mag_partial<double><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sd[0], h->sd[1], h->sd[2],
                                                               nullptr, nullptr, nullptr, grid.x, h->d_magpart);
     }
-    mag_final<<<nb(h->nrep * nsub * 3, 128), 128, 0, h->stream>>>(h->nrep, nsub, grid.x, h->d_magpart, inv_count, h->d_mag);
+    mag_final<<<h->nrep * nsub * 3, 128, 0, h->stream>>>(h->nrep, nsub, grid.x, h->d_magpart, inv_count, h->d_mag);
     h->launches += 2;
     return cudaGetLastError();
 }
