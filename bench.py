@@ -1,10 +1,12 @@
 #!/usr/bin/env python
 """Benchmark of the sLLG step: spin-updates/s on one B200 (or N replicas on N GPUs).
 
-Default workload: the body-centred-tetragonal 2-sublattice antiferromagnet,
-64x64x64 cells (524,288 spins), 26 neighbours/site with full 3x3 tensors in
-CSR (SELL-32 on the device), Heun, T=300 K, FP32 state with FP64
-renormalisation.  Prints one JSON line (rank 0).
+Default workload ("northstar"): the 1M-spin exchange + dipolar lattice, simple cubic
+128x128x64 (1,048,576 spins), open boundaries, nearest-neighbour exchange in CSR (SELL-32 on
+the device) plus the point-dipole field by zero-padded FFT on the 256x256x128 mesh, refreshed
+every step, Heun, T=0, FP32 state with FP64 renormalisation.  Other workloads (--workload):
+bct2_64 (BCT-2 64^3 cells, 26 neighbours, full 3x3 tensors, T=300 K), bct2_64_dia, sc16,
+replicas96, sc128_fft, film_rk4.  Prints one JSON line (rank 0).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 """
@@ -160,16 +162,47 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- reference arm
+# The reference's CPU step cannot evaluate the dipole field here (its FFT path needs FFTW3, which
+# is absent), so the north-star lattice runs on the FP64 restatement with the long-range field by
+# threaded FFT (oracle/fft_oracle.py, pinned against the direct-sum oracle); lattices without a
+# long-range field run the reference's own llgCPU compiled from source.  Neither loads the
+# product library: the north-star CSR comes from a numpy builder that is bit-exact with the
+# reference's exchunitcell, the BCT-2 CSR from the reference's exchunitcell itself.
+NS_DIM = (128, 128, 64)
+REF_STEP_CAP = 60          # at most this many timed CPU steps per run (~1.3 s each at 1M spins, 8 cores)
+
+
+def cpu_port_northstar(steps, warmup, workers=None):
+    """FFT restatement on the north-star lattice: (spin-updates/s, seconds, spins, threads, steps)."""
+    sys.path[:0] = [REPO]
+    from oracle import fft_oracle as F
+    s = F.sc_dipole_system(NS_DIM)
+    o = F.FFTOracle(s, dt=1e-16, update=1, workers=workers)
+    o.set_spins(F.random_spins(s.nspins, 0))
+    o.step(warmup)
+    secs = o.timed_steps(steps)
+    return s.nspins * steps / secs, secs, s.nspins, o.workers, steps
+
+
 def _ref_worker(args):
-    """One process: the reference llgCPU on a BCT-2 sample lattice, timed per step."""
+    """One process: the reference llgCPU on the BCT-2 lattice, CSR from the reference's exchunitcell."""
     cells, steps, warmup, seed = args
     sys.path[:0] = [REPO, PKG]
-    import numpy as np  # noqa: F401
-    import asd_lattice as LT
+    import numpy as np
+    from asd_lattice import _bct2_bonds           # bond list only (numpy); no library call
     from oracle import oracle as O
-    s = LT.bct2_antiferromagnet(cells, layout="csr", T=300.0)
+    ba, bt, bv, bj = _bct2_bonds(np.random.default_rng(2))
+    xadj, adj, val = O.ref_exchunitcell((cells,) * 3, (1, 1, 1), [1.5, 1.5],
+                                        [(a, b, v, np.asarray(j).reshape(3, 3)) for a, b, v, j in zip(ba, bt, bv, bj)])
+    from types import SimpleNamespace as NS
+    mats = [NS(mu=1.5, lam=0.01, gamma=1.0, k1u=-1e-23, k1u_dir=(0.0, 0.0, 1.0), sublattice=q) for q in (0, 1)]
+    s = NS(nspins=2 * cells ** 3, materials=mats, atom=None, exch=2, full=True, xadj=xadj, adjncy=adj, csr_val=val,
+           temperature=300.0, site_field=None)
     r = O.RefLLGCPU(s, seed=(seed, seed + 100))
-    r.set_spins(LT.random_spins(s.nspins, seed))
+    rng = np.random.default_rng(seed)
+    z = rng.uniform(-1, 1, s.nspins)
+    ph = rng.uniform(0, 2 * np.pi, s.nspins)
+    r.set_spins(np.stack([np.sqrt(1 - z * z) * np.cos(ph), np.sqrt(1 - z * z) * np.sin(ph), z], 1))
     r.step(warmup)
     t0 = time.perf_counter()
     r.step(steps)
@@ -189,19 +222,37 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    procs = os.cpu_count() or 1
-    cells = 12
-    rate, res = cpu_reference(cells, args.steps, args.warmup, procs)
-    n = res[0][0]
-    line = {"metric": METRIC, "value": rate, "unit": "spin-updates/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * max(r[2] for r in res) / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "bct2_64 (CPU sample)", "nspins_per_process": n, "processes": procs},
-            "cpu_baseline": {"value": rate, "unit": "spin-updates/s", "cores": procs, "kind": "reference",
-                             "sample": f"reference llgCPU (src/llgCPU.cpp, compiled from source) on BCT-2 {cells}^3 "
-                                       f"cells ({n} spins, 26 nbrs, full 3x3 CSR, T=300 K), one independent "
-                                       f"replica per process x {procs} processes, {args.steps} steps each"},
-            "e2e": {"value": rate, "unit": "spin-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    base = {"metric": METRIC, "unit": "spin-updates/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
+    k = max(1, min(args.steps, REF_STEP_CAP))
+    if args.workload == "northstar":
+        rate, secs, n, thr, k = cpu_port_northstar(k, min(args.warmup, 2))
+        sample = (f"FP64 restatement of the reference's Heun step (oracle/fft_oracle.py: CSR exchange, dipole by "
+                  f"threaded FFT on the 256x256x128 mesh, pinned against the direct-sum oracle) on the same "
+                  f"sc 128x128x64 open lattice and initial spins, {k} timed steps of the whole lattice "
+                  f"({secs:.1f} s), {thr} threads")
+        kind = "port"
+        cfg = {"workload": "northstar", "lattice": "sc 128x128x64 open", "nspins": n,
+               "field": "CSR NN exchange + FFT dipole every step", "T_K": 0.0, "integrator": "heun",
+               "same_config": True}
+    elif args.workload == "bct2_64":
+        procs = os.cpu_count() or 1
+        k = max(1, min(args.steps, 30))
+        rate, res = cpu_reference(64, k, min(args.warmup, 2), procs)
+        secs = max(r[2] for r in res)
+        n, thr = res[0][0], procs
+        sample = (f"reference llgCPU (src/llgCPU.cpp, compiled from source) on the same BCT-2 64^3-cell lattice "
+                  f"({n} spins, 26 nbrs, full 3x3 CSR from the reference's exchunitcell, T=300 K), one "
+                  f"independent replica per process x {procs} processes, {k} timed steps each ({secs:.1f} s)")
+        kind = "reference"
+        cfg = {"workload": "bct2_64", "nspins_per_process": n, "processes": procs, "same_config": True}
+    else:
+        print(json.dumps({"impl": "reference", "unavailable": f"no CPU reference arm for workload {args.workload}"}))
+        return
+    line = dict(base, value=rate, ms_per_step=1e3 * secs / k, config=cfg, steps_run=k,
+                cpu_baseline={"value": rate, "unit": "spin-updates/s", "cores": thr, "kind": kind, "sample": sample},
+                e2e={"value": rate, "unit": "spin-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0})
     print(json.dumps(line), flush=True)
 
 
@@ -340,13 +391,23 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            rate, res = cpu_reference(16, args.cpu_steps, 2, 1)
-            cpu = {"value": rate, "unit": "spin-updates/s", "cores": 1, "kind": "reference",
-                   "sample": f"reference llgCPU (src/llgCPU.cpp compiled from source) on BCT-2 16^3 cells "
-                             f"({res[0][0]} spins, same 26-neighbour full-tensor CSR, T=300 K), {args.cpu_steps} "
-                             f"steps, 1 thread"}
-        except Exception as e:  # the harness library is built by __graft_entry__.build()
-            cpu = {"value": None, "unit": "spin-updates/s", "cores": 1, "kind": "reference",
+            if args.workload == "northstar":
+                rate, secs, nn, thr, k = cpu_port_northstar(args.cpu_steps, 1)
+                cpu = {"value": rate, "unit": "spin-updates/s", "cores": thr, "kind": "port",
+                       "sample": f"FP64 restatement (oracle/fft_oracle.py: CSR exchange, dipole by threaded FFT) on "
+                                 f"the same sc 128x128x64 lattice and spins, {k} whole-lattice steps "
+                                 f"({secs:.1f} s), {thr} threads"}
+            else:
+                k = max(1, min(args.cpu_steps, 60))
+                rate, res = cpu_reference(64, k, 1, 1) if args.workload == "bct2_64" else (None, None)
+                if rate is None:
+                    raise RuntimeError(f"no CPU baseline for workload {args.workload}")
+                cpu = {"value": rate, "unit": "spin-updates/s", "cores": 1, "kind": "reference",
+                       "sample": f"reference llgCPU (src/llgCPU.cpp compiled from source) on the same BCT-2 64^3-cell "
+                                 f"lattice ({res[0][0]} spins, CSR from the reference's exchunitcell, T=300 K), "
+                                 f"{k} steps ({res[0][2]:.1f} s), 1 thread (the reference has no threading)"}
+        except Exception as e:  # the checkers are built by __graft_entry__.build()
+            cpu = {"value": None, "unit": "spin-updates/s", "cores": None, "kind": "port",
                    "sample": f"unavailable: {e}"}
 
     if rank == 0:
@@ -378,10 +439,11 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="bct2_64")
+    ap.add_argument("--workload", default="northstar")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=1500)
+    ap.add_argument("--cpu-steps", type=int, default=8,
+                    help="whole-lattice steps of the CPU baseline (north star: ~1.3 s each on 8 cores)")
     ap.add_argument("--err-steps", type=int, default=100)
     ap.add_argument("--launch-shape", default="",
                     help="block,staging for the fused stage kernel instead of the autotuner's choice "
