@@ -84,7 +84,7 @@ void free_all(asd_handle* h) {
     if (L.c2r) cufftDestroy(L.c2r);
     if (L.z2z) cufftDestroy(L.z2z);
     if (L.c2c) cufftDestroy(L.c2c);
-    F(L.k1); F(L.k2);
+    F(L.k1); F(L.k2); F(L.yk); F(L.nkt);
     F(h->sq.idx); F(h->sq.sub); F(h->sq.uo); F(h->sq.kidx); F(h->sq.grid); F(h->sq.series);
     if (h->sq.plan) cufftDestroy(h->sq.plan);
     F(h->d_magpart); F(h->d_mag); F(h->d_inv_count); F(h->d_sub_of_atom); F(h->d_stats);
@@ -330,7 +330,13 @@ void setup_lr(asd_handle* h, const asd_system& s, bool plain) {
         // pruned transform when the last axis is a power of two: z transforms only for the rows
         // of the spins' box, 2D transforms of the (x, y) planes by cuFFT
         L.pruned = (mz >= 4 && mz <= 2048 && (mz & (mz - 1)) == 0 && h->n > 0) ? 1 : 0;   // z-pass smem <= 45 KB
-        if (L.pruned) {
+        if (L.pruned) for (int a = 0; a < 3; a++) { L.box0[a] = lo[a]; L.box1[a] = hi[a]; }
+        // the library's plane kernels replace cuFFT's (x, y) passes where every axis fits them
+        L.planes = (L.pruned && !(h->p.flags & ASD_FLAG_CUFFT_PLANES) && plane_path_fits(L, false) &&
+                    plane_path_fits(L, true)) ? 1 : 0;
+        if (L.planes) {
+            // buffers are allocated with the tiled N_k (build_nk_f32)
+        } else if (L.pruned) {
             for (int a = 0; a < 3; a++) { L.box0[a] = lo[a]; L.box1[a] = hi[a]; }
             L.k1 = dalloc<float2>(3 * L.Pk);
             L.k2 = dalloc<float2>(3 * L.Pk);
@@ -346,7 +352,7 @@ void setup_lr(asd_handle* h, const asd_system& s, bool plain) {
             CKFFT(cufftSetStream(L.c2r, h->stream));
         }
         e = build_nk_f32(h, d_nr);
-        if (e == cudaSuccess && L.pruned) e = permute_nk_pruned(h);
+        if (e == cudaSuccess && L.pruned && !L.planes) e = permute_nk_pruned(h);
     }
     cudaFree(d_nr);
     CK(e);
@@ -359,7 +365,7 @@ void set_dyn(asd_handle* h, int idx, double v) {
 
 void scatter_if_needed(asd_handle* h) {
     if (h->lr.mode == ASD_LR_NONE || h->p.precision == ASD_FP64_PLAIN || h->lr_scattered) return;
-    CK(launch_lr_scatter_f32(h, h->sf));
+    CK(launch_lr_scatter(h));
     h->lr_scattered = true;
 }
 
@@ -606,7 +612,6 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         if (s0.lr == ASD_LR_FFT) REQUIRE(h->exch == ASD_EXCH_FFT || h->exch == ASD_EXCH_NONE, "FFT field excludes CSR/DIA exchange");
         if (h->exch == ASD_EXCH_FFT) REQUIRE(s0.lr == ASD_LR_FFT, "exchange method fft needs lr = ASD_LR_FFT");
         h->dexch = h->exch;
-        REQUIRE(!(p.precision == ASD_FP64_FUSED && s0.lr != ASD_LR_NONE), "FP64 fused form has no long-range field; use FP64 plain");
         // material constants (src/llg.cpp:591-592, src/geom.cpp:244)
         StepConst& sc = h->sc;
         sc.n = n; sc.nmat = h->nmat; sc.nrep = nsys; sc.flags = p.flags;
@@ -1082,6 +1087,11 @@ int asd_sync(asd_handle* h) {
         CK(cudaStreamSynchronize(h->stream));
         uint32_t e = 0;
         if (h->d_err) CK(cudaMemcpy(&e, h->d_err, sizeof e, cudaMemcpyDeviceToHost));
+        if (e & 2u) {
+            CK(cudaMemset(h->d_err, 0, sizeof(uint32_t)));
+            throw Fail{ASD_ETIMEOUT, "a long-range transform block's bulk-copy wait ran out; the long-range field of "
+                                     "that evaluation is invalid"};
+        }
         if (e & 1u) {
             CK(cudaMemset(h->d_err, 0, sizeof(uint32_t)));
             throw Fail{ASD_ETIMEOUT, "a stage kernel's shared-memory staging wait ran out; those blocks read the "
@@ -1204,7 +1214,11 @@ int asd_get_ttm_temperatures(asd_handle* h, double* Te, double* Tl) {
 
 int asd_tuning(const asd_handle* h, char* out, size_t out_len) {
     if (!h || !out || out_len == 0) return ASD_EINVAL;
-    std::snprintf(out, out_len, "%s", h->tune.c_str());
+    const LongRange& L = h->lr;
+    const char* lr = L.mode == ASD_LR_NONE ? "" : h->p.precision == ASD_FP64_PLAIN ? "; long-range: cuFFT Z2Z 3D"
+                     : L.planes ? "; long-range: plane kernels" : L.pruned ? "; long-range: z-pass + cuFFT 2D planes"
+                                                                       : "; long-range: cuFFT R2C/C2R 3D";
+    std::snprintf(out, out_len, "%s%s", h->tune.c_str(), lr);
     return ASD_OK;
 }
 

@@ -53,16 +53,17 @@ __global__ void kconv9c(size_t Pk, const float2* __restrict__ nk, float2* __rest
     m[i] = o[0]; m[Pk + i] = o[1]; m[2 * Pk + i] = o[2];
 }
 
-__global__ void scatter_k(uint32_t n, size_t P, const float* __restrict__ sx, const float* __restrict__ sy,
-                          const float* __restrict__ sz, const float* __restrict__ w, const uint32_t* __restrict__ idx,
+template <typename R>
+__global__ void scatter_k(uint32_t n, size_t P, const R* __restrict__ sx, const R* __restrict__ sy,
+                          const R* __restrict__ sz, const float* __restrict__ w, const uint32_t* __restrict__ idx,
                           float* __restrict__ mr) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t m = idx[i];
     const float wv = w[i];
-    mr[m] = sx[i] * wv;
-    mr[P + m] = sy[i] * wv;
-    mr[2 * P + m] = sz[i] * wv;
+    mr[m] = (float)sx[i] * wv;
+    mr[P + m] = (float)sy[i] * wv;
+    mr[2 * P + m] = (float)sz[i] * wv;
 }
 
 // Largest |Re| and |Im| of the FP64 half spectrum (non-negative doubles order like their bits):
@@ -427,9 +428,13 @@ cudaError_t permute_nk_pruned(asd_handle* h) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_lr_scatter_f32(asd_handle* h, const float* const s[3]) {
+// The handle's spins (FP32 or fused FP64) times their weight into the padded M_r.
+cudaError_t launch_lr_scatter(asd_handle* h) {
     LongRange& L = h->lr;
-    scatter_k<<<nb(h->n, 256), 256, 0, h->stream>>>(h->n, L.P, s[0], s[1], s[2], L.w, L.mesh_idx, L.r);
+    if (h->p.precision == ASD_FP32)
+        scatter_k<float><<<nb(h->n, 256), 256, 0, h->stream>>>(h->n, L.P, h->sf[0], h->sf[1], h->sf[2], L.w, L.mesh_idx, L.r);
+    else
+        scatter_k<double><<<nb(h->n, 256), 256, 0, h->stream>>>(h->n, L.P, h->sd[0], h->sd[1], h->sd[2], L.w, L.mesh_idx, L.r);
     h->launches += 1;
     return cudaGetLastError();
 }
@@ -437,6 +442,7 @@ cudaError_t launch_lr_scatter_f32(asd_handle* h, const float* const s[3]) {
 // M_r -> (R2C) -> N_k . M_k -> (C2R) -> H_r
 cudaError_t launch_lr_eval_f32(asd_handle* h) {
     LongRange& L = h->lr;
+    if (L.planes) return launch_lr_planes(h);
     if (L.pruned) {
         const ZPass A = zpass_args(L);
         cudaError_t e = zpass_run(h, false);
@@ -494,6 +500,28 @@ cudaError_t build_nk_f32(asd_handle* h, const double* d_nr) {
     double re, im;
     memcpy(&re, &hm[0], 8); memcpy(&im, &hm[1], 8);
     L.nk_real = (im <= 1e-9 * re) ? 1 : 0;
+    if (L.planes) {
+        // the plane kernels read N_k tiled per (kz, ky tile); a general N_k takes 9 complex
+        // components (a symmetric set expanded first)
+        const bool cplx = !(nc == 6 && L.nk_real);
+        double2* z9 = z;
+        if (cplx && nc == 6) {
+            cudaMalloc(&z9, sizeof(double2) * 9 * L.Pk);
+            static const int inv6[9] = {0, 1, 2, 1, 3, 4, 2, 4, 5};
+            for (int q = 0; q < 9; q++)
+                cudaMemcpyAsync(z9 + q * L.Pk, z + inv6[q] * L.Pk, sizeof(double2) * L.Pk, cudaMemcpyDeviceToDevice, h->stream);
+        }
+        if (cplx) L.ncomp = 9;
+        e = build_nk_tiles(h, z9, cplx ? 9 : 6, cplx);
+        cudaError_t e2 = cudaStreamSynchronize(h->stream);
+        if (z9 != z) cudaFree(z9);
+        cufftDestroy(plan);
+        cudaFree(mx); cudaFree(src); cudaFree(z);
+        if (e != cudaSuccess) return e;
+        if (e2 != cudaSuccess) return e2;
+        e = cudaMalloc(&L.yk, sizeof(float2) * plane_spectrum_elems(L));
+        return e == cudaSuccess ? cudaGetLastError() : e;
+    }
     if (nc == 6 && L.nk_real) {
         cudaMalloc(&L.nkr, sizeof(float) * 6 * L.Pk);
         nk_pack_real<<<nb(6 * L.Pk, 256), 256, 0, h->stream>>>(L.Pk, 6, z, nullptr, L.nkr, nullptr);

@@ -1,0 +1,678 @@
+// Long-range field, FP32 form: the zero-padded convolution H = IFFT(N_k FFT(M)) in three kernels
+// of this library, pruned to the spins' bounding box (replaces the reference's zero / copy /
+// cufftExecC2C / CFConv / cufftExecC2C / copy sequence, src/cufields.cu:248-462,
+// src/cuda_util.cu:76,97,245,250, and the two 2D cuFFT passes of the earlier pruned path).
+//
+//  plane_zy_fwd  (one block per box row x and component): real FFT along z of the box rows
+//                (the spectrum kept in shared memory, transposed), then the FFT along y of
+//                every kz: Y[c][kz][ky-tile][x][j], x and y counted from the box origin.
+//  plane_x_conv  (one block per (kz, tile of T ky columns)): its Y tile of all three components
+//                and its N_k tile arrive by bulk copy; FFT along x, the 3x3 product with N_k,
+//                the inverse FFT along x, box rows only, written back in place by bulk copy.
+//  plane_yz_inv  (one block per box row x and component): inverse FFT along y of every kz
+//                (box columns only, into shared memory), then the inverse real FFT along z of
+//                the box rows into H_r.
+//
+// Shifting the box to the origin along x and y does not change the cyclic convolution (it
+// depends on mesh differences only), and lets every pass skip the zero half of its input and
+// the discarded half of its output.  The transforms are unnormalised like cuFFT's: the stage
+// kernels multiply the gathered field by 1/P.
+#include "fft_dev.cuh"
+#include "gather.cuh"
+#include <algorithm>
+#include <cooperative_groups.h>
+#include <cstring>
+
+namespace asd {
+namespace {
+using namespace fftd;
+namespace cg = cooperative_groups;
+
+inline unsigned nbk(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
+
+constexpr uint32_t PT = 8;                 // ky tile width of the spectrum and N_k layouts
+
+struct PlaneArgs {
+    uint32_t m0;                     // mesh x (y and z are compile-time in the kernels)
+    uint32_t bx0, by0;               // box origin (x, y)
+    uint32_t zs, nz;                 // z rows: float2 pairs [zs, zs + nz) hold data, nz <= N/2
+    uint32_t bx, by;                 // box extents along x (<= m0/2) and y (<= m1/2)
+    uint32_t ntile;                  // ky tiles (m1 / PT)
+    // a (component, box row x) is shared by a cluster of CL blocks: block `rank` transforms the
+    // z rows y in [rank hy, rank hy + hy) and the kz in [rank hk, rank hk + hk); the transposed
+    // z spectrum of its rows, Zs[kz][ldz] (ldz odd, >= hy), is read and written across the
+    // cluster in distributed shared memory
+    uint32_t CL, hy, lhy, hk, ldz;
+    uint32_t kzb;                    // kz values per y-pass round (rounds balanced)
+    uint32_t scr;                    // scratch (float2) of the z/y passes
+    uint32_t nkx;                    // kx rows of the N_k tile: m0 (full) or m0/2 + 1 (kx parity used)
+    uint32_t odd;                    // bit q: component q of N_k is odd in kx (N(-kx) = -N(kx))
+    size_t P;                        // padded real points
+    uint32_t* err;                   // device error bits
+};
+
+constexpr uint32_t ERR_FFT_TIMEOUT = 2u;
+
+__device__ __forceinline__ void bulk_store(void* gdst, const void* ssrc, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_addr(ssrc)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit_wait_read() {
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Y element (c, kz, x, ky) in the tiled spectrum layout [c][kz][ky / PT][x][ky % PT].
+__device__ __forceinline__ size_t yk_index(const PlaneArgs& A, uint32_t Kz, uint32_t c, uint32_t kz, uint32_t x,
+                                           uint32_t ky) {
+    return ((((size_t)c * Kz + kz) * A.ntile + (ky / PT)) * A.bx + x) * PT + (ky % PT);
+}
+
+// Compile-time geometry of the z/y kernels: z rows of N = Z1 Z2 complex points (mesh z = 2N),
+// y transforms of M1 = R1 R2 points.
+template <int Z1, int Z2, int R1, int R2>
+struct ZYGeom {
+    static constexpr uint32_t N = Z1 * Z2, KZ = N + 1;
+    static constexpr uint32_t TY = 256 / (Z1 > Z2 ? Z1 : Z2);         // z rows per round
+    static constexpr uint32_t LD = fft2pass_pitch(N, Z1, Z2);          // z row pitch
+    static constexpr uint32_t M1 = R1 * R2;
+};
+
+// ---------------------------------------------------------------- forward: z (R2C) then y
+template <int Z1, int Z2, int R1, int R2>
+__global__ void __launch_bounds__(256, 3) plane_zy_fwd(const float* __restrict__ mr, float2* __restrict__ yk,
+                                                       const PlaneArgs A) {
+    using G = ZYGeom<Z1, Z2, R1, R2>;
+    constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
+    extern __shared__ __align__(16) float2 sm[];
+    cg::cluster_group cl = cg::this_cluster();
+    float2* Zs = sm;                                   // [KZ][ldz]: this block's z rows
+    float2* scr = Zs + (size_t)KZ * A.ldz;             // z rows [TY][LD] | y exchange [kzb][R1][R2+1]
+    float2* twz = scr + A.scr;                         // N + (N + 1) z twiddles
+    float2* twy = twz + 2 * N + 1;                     // M1 y twiddles
+    const uint32_t rank = cl.block_rank();
+    const uint32_t xl = blockIdx.x / A.CL, c = blockIdx.y, x = A.bx0 + xl;
+    load_twiddles(twz, N);
+    load_tw(twy, M1);
+    const float2* row0 = reinterpret_cast<const float2*>(mr + (size_t)c * A.P) + A.zs;
+    const float2* ws = twz + N;
+    const uint32_t ry0 = rank * A.hy, ry1 = min(A.by, ry0 + A.hy);
+    for (uint32_t y0 = ry0; y0 < ry1; y0 += TY) {
+        __syncthreads();
+        // rows shifted to the z pair zs; pairs n >= N/2 are zero and not read by the pruned pass
+        for (uint32_t e = threadIdx.x; e < TY * (N / 2); e += blockDim.x) {
+            const uint32_t r = e / (N / 2), n = e % (N / 2), yl = y0 + r;
+            float2 v = make_float2(0.f, 0.f);
+            if (yl < ry1 && n < A.nz) v = row0[((size_t)x * M1 + A.by0 + yl) * N + n];
+            scr[r * LD + n] = v;
+        }
+        __syncthreads();
+        fft2pass<Z1, Z2, false, true, false>(scr, LD, twz, TY);
+        for (uint32_t e = threadIdx.x; e < KZ * TY; e += blockDim.x) {
+            const uint32_t r = e / KZ, k = e % KZ, yl = y0 + r;
+            if (yl >= ry1) continue;
+            const float2 zk = scr[r * LD + (k & (N - 1))], zm = scr[r * LD + ((N - k) & (N - 1))];
+            Zs[k * A.ldz + (yl - ry0)] = r2c_split(zk, zm, ws[k]);
+        }
+    }
+    cl.sync();                                         // every block's rows are in its Zs
+    const uint32_t kz_lo = rank * A.hk, kz_hi = min(KZ, kz_lo + A.hk);
+    for (uint32_t kz0 = kz_lo; kz0 < kz_hi; kz0 += A.kzb) {
+        {
+            const uint32_t kzl = threadIdx.x / R2, t = threadIdx.x % R2, kz = kz0 + kzl;
+            if (kzl < A.kzb && kz < kz_hi) {
+                float2 v[R1];
+#pragma unroll
+                for (int k = 0; k < R1 / 2; k++) {     // rows y >= M1/2 are zero
+                    const uint32_t yy = t + R2 * k;
+                    v[k] = make_float2(0.f, 0.f);
+                    if (yy < A.by) {
+                        const float2* zp = cl.map_shared_rank(Zs, yy >> A.lhy);
+                        v[k] = zp[kz * A.ldz + (yy & (A.hy - 1))];
+                    }
+                }
+                dftp<R1, false, true, false>(v);
+#pragma unroll
+                for (int m = 1; m < R1; m++) v[m] = cmul(v[m], twy[t * m]);
+#pragma unroll
+                for (int m = 0; m < R1; m++) scr[(kzl * R1 + m) * (R2 + 1) + t] = v[m];
+            }
+        }
+        __syncthreads();
+        {
+            const uint32_t kzl = threadIdx.x / R1, m = threadIdx.x % R1, kz = kz0 + kzl;
+            if (kzl < A.kzb && kz < kz_hi) {
+                float2 u[R2];
+#pragma unroll
+                for (int t = 0; t < R2; t++) u[t] = scr[(kzl * R1 + m) * (R2 + 1) + t];
+                dft<R2, false>(u);
+#pragma unroll
+                for (int q = 0; q < R2; q++) yk[yk_index(A, KZ, c, kz, xl, m + R1 * q)] = u[q];
+            }
+        }
+        __syncthreads();
+    }
+    cl.sync();                                         // no block retires while a peer reads its Zs
+}
+
+// ---------------------------------------------------------------- x, N_k product, inverse x
+// Shared memory: Ys [3][bx][PT] (input and output), Ns (N_k tile: 6 x nkx x PT floats or
+// 9 x M0 x PT float2), E (exchange, R1 x (R2 PT + 8) float2), twx [M0].  A real N_k whose every
+// component is even or odd in kx is stored for kx <= M0/2 only (nkx = M0/2 + 1 rows); the rows
+// kx > M0/2 are read at M0 - kx with the component's sign.
+template <int R1, int R2, bool CPLX>
+__global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __restrict__ yk,
+                                                                      const void* __restrict__ nkt, const uint32_t Kz,
+                                                                      const PlaneArgs A) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ __align__(8) uint64_t bar;
+    constexpr uint32_t T = PT;
+    constexpr uint32_t M0 = R1 * R2;
+    constexpr uint32_t NQ = CPLX ? 9 : 6;
+    constexpr uint32_t NB = CPLX ? 8 : 4;             // bytes per N_k component value
+    constexpr uint32_t EP = R2 * T + 8;               // exchange pitch per m (padded: no bank conflicts)
+    const uint32_t tile = blockIdx.x, kz = blockIdx.y;
+    float2* Ys = reinterpret_cast<float2*>(smraw);
+    const uint32_t ys_bytes = 3u * A.bx * T * 8u;
+    unsigned char* Nsb = smraw + ((ys_bytes + 15u) & ~15u);
+    const uint32_t ns_bytes = NQ * A.nkx * T * NB;
+    float2* E = reinterpret_cast<float2*>(Nsb + ns_bytes);
+    float2* twx = E + R1 * EP;
+    const uint32_t tid = threadIdx.x, j = tid % T, r = tid / T;
+    const uint32_t slab = A.bx * T;                   // float2 per (c, kz, tile) slab
+    float2* gy[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) gy[c] = yk + (((size_t)c * Kz + kz) * A.ntile + tile) * slab;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_arrive_expect_tx(&bar, ys_bytes + ns_bytes);
+        for (int c = 0; c < 3; c++) bulk_copy_stream(Ys + c * slab, gy[c], slab * 8u, &bar);
+        bulk_copy_stream(Nsb, static_cast<const unsigned char*>(nkt) + ((size_t)kz * A.ntile + tile) * ns_bytes,
+                         ns_bytes, &bar);
+    }
+    load_tw(twx, M0);
+    __syncthreads();
+    if (!mbar_wait_bounded(&bar, STAGE_WAIT_POLLS)) {
+        // the copies did not land in time: flag it, leave this tile untransformed, and retire
+        // only after the copies into shared memory have finished (bounded again)
+        if (tid == 0) atomicOr(A.err, ERR_FFT_TIMEOUT);
+        mbar_wait_bounded(&bar, STAGE_WAIT_POLLS);
+        return;
+    }
+    // forward x transform of the three components; thread (j, m) keeps X[c][m + R1 q]
+    float2 X[3][R2];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if (r < R2) {
+            const uint32_t t = r;
+            float2 v[R1];
+#pragma unroll
+            for (int k = 0; k < R1 / 2; k++) {         // rows x >= M0/2 are zero
+                const uint32_t xx = t + R2 * k;
+                v[k] = xx < A.bx ? Ys[(c * A.bx + xx) * T + j] : make_float2(0.f, 0.f);
+            }
+            dftp<R1, false, true, false>(v);
+#pragma unroll
+            for (int m = 1; m < R1; m++) v[m] = cmul(v[m], twx[t * m]);
+#pragma unroll
+            for (int m = 0; m < R1; m++) E[m * EP + t * T + j] = v[m];
+        }
+        __syncthreads();
+        {
+            const uint32_t m = r;
+#pragma unroll
+            for (int t = 0; t < R2; t++) X[c][t] = E[m * EP + t * T + j];
+            dft<R2, false>(X[c]);
+        }
+        __syncthreads();
+    }
+    // H_k = N_k M_k at kx = m + R1 q
+    {
+        const uint32_t m = r;
+#pragma unroll
+        for (int q = 0; q < R2; q++) {
+            const uint32_t kx = m + R1 * q;
+            const float2 a = X[0][q], b = X[1][q], cc = X[2][q];
+            if constexpr (!CPLX) {
+                const float* Ns = reinterpret_cast<const float*>(Nsb);
+                const bool mir = kx >= A.nkx;                  // kx > M0/2 in the half layout
+                const uint32_t row = mir ? M0 - kx : kx, nk = A.nkx;
+                const uint32_t neg = mir ? A.odd : 0u;
+                float n6[6];
+#pragma unroll
+                for (int q6 = 0; q6 < 6; q6++) {
+                    const float v = Ns[(q6 * nk + row) * T + j];
+                    n6[q6] = (neg >> q6) & 1u ? -v : v;
+                }
+                X[0][q] = make_float2(n6[0] * a.x + n6[1] * b.x + n6[2] * cc.x, n6[0] * a.y + n6[1] * b.y + n6[2] * cc.y);
+                X[1][q] = make_float2(n6[1] * a.x + n6[3] * b.x + n6[4] * cc.x, n6[1] * a.y + n6[3] * b.y + n6[4] * cc.y);
+                X[2][q] = make_float2(n6[2] * a.x + n6[4] * b.x + n6[5] * cc.x, n6[2] * a.y + n6[4] * b.y + n6[5] * cc.y);
+            } else {
+                const float2* Ns = reinterpret_cast<const float2*>(Nsb);
+                const float2 v[3] = {a, b, cc};
+#pragma unroll
+                for (int al = 0; al < 3; al++) {
+                    float2 o = make_float2(0.f, 0.f);
+#pragma unroll
+                    for (int be = 0; be < 3; be++) o = cadd(o, cmul(Ns[((3 * al + be) * M0 + kx) * T + j], v[be]));
+                    X[al][q] = o;
+                }
+            }
+        }
+    }
+    // inverse x transform, box rows only, into Ys
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        {
+            const uint32_t m = r;
+            dft<R2, true>(X[c]);
+#pragma unroll
+            for (int t = 0; t < R2; t++) E[m * EP + t * T + j] = t ? cmulc(X[c][t], twx[t * m]) : X[c][t];
+        }
+        __syncthreads();
+        if (r < R2) {
+            const uint32_t t = r;
+            float2 w[R1];
+#pragma unroll
+            for (int m = 0; m < R1; m++) w[m] = E[m * EP + t * T + j];
+            dftp<R1, true, false, true>(w);            // the rows x < M0/2 only
+#pragma unroll
+            for (int k = 0; k < R1 / 2; k++) {
+                const uint32_t xx = t + R2 * k;
+                if (xx < A.bx) Ys[(c * A.bx + xx) * T + j] = w[k];
+            }
+        }
+        __syncthreads();
+    }
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+        for (int c = 0; c < 3; c++) bulk_store(gy[c], Ys + c * slab, slab * 8u);
+        bulk_commit_wait_read();
+    }
+}
+
+// ---------------------------------------------------------------- inverse: y then z (C2R)
+template <int Z1, int Z2, int R1, int R2>
+__global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict__ yk, float* __restrict__ hr,
+                                                       const PlaneArgs A) {
+    using G = ZYGeom<Z1, Z2, R1, R2>;
+    constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
+    extern __shared__ __align__(16) float2 sm[];
+    cg::cluster_group cl = cg::this_cluster();
+    float2* Zs = sm;
+    float2* scr = Zs + (size_t)KZ * A.ldz;
+    float2* twz = scr + A.scr;
+    float2* twy = twz + 2 * N + 1;
+    const uint32_t rank = cl.block_rank();
+    const uint32_t xl = blockIdx.x / A.CL, c = blockIdx.y, x = A.bx0 + xl;
+    load_twiddles(twz, N);
+    load_tw(twy, M1);
+    __syncthreads();
+    // inverse y of this block's kz: every box row's value goes to the Zs of the block owning it
+    const uint32_t kz_lo = rank * A.hk, kz_hi = min(KZ, kz_lo + A.hk);
+    for (uint32_t kz0 = kz_lo; kz0 < kz_hi; kz0 += A.kzb) {
+        {
+            const uint32_t kzl = threadIdx.x / R1, m = threadIdx.x % R1, kz = kz0 + kzl;
+            if (kzl < A.kzb && kz < kz_hi) {
+                float2 u[R2];
+#pragma unroll
+                for (int q = 0; q < R2; q++) u[q] = yk[yk_index(A, KZ, c, kz, xl, m + R1 * q)];
+                dft<R2, true>(u);
+#pragma unroll
+                for (int t = 0; t < R2; t++)
+                    scr[(kzl * R1 + m) * (R2 + 1) + t] = t ? cmulc(u[t], twy[t * m]) : u[t];
+            }
+        }
+        __syncthreads();
+        {
+            const uint32_t kzl = threadIdx.x / R2, t = threadIdx.x % R2, kz = kz0 + kzl;
+            if (kzl < A.kzb && kz < kz_hi) {
+                float2 w[R1];
+#pragma unroll
+                for (int m = 0; m < R1; m++) w[m] = scr[(kzl * R1 + m) * (R2 + 1) + t];
+                dftp<R1, true, false, true>(w);        // the rows y < M1/2 only
+#pragma unroll
+                for (int k = 0; k < R1 / 2; k++) {
+                    const uint32_t yy = t + R2 * k;
+                    if (yy < A.by) {
+                        float2* zp = cl.map_shared_rank(Zs, yy >> A.lhy);
+                        zp[kz * A.ldz + (yy & (A.hy - 1))] = w[k];
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    cl.sync();                                         // every row of every block's Zs is written
+    const float2* ws = twz + N;
+    float2* out0 = reinterpret_cast<float2*>(hr + (size_t)c * A.P) + A.zs;
+    const uint32_t ry0 = rank * A.hy, ry1 = min(A.by, ry0 + A.hy);
+    for (uint32_t y0 = ry0; y0 < ry1; y0 += TY) {
+        for (uint32_t e = threadIdx.x; e < KZ * TY; e += blockDim.x) {
+            const uint32_t r = e / KZ, k = e % KZ, yl = y0 + r;
+            scr[r * LD + k] = yl < ry1 ? Zs[k * A.ldz + (yl - ry0)] : make_float2(0.f, 0.f);
+        }
+        __syncthreads();
+        // pairwise in place: thread (r, k) for k in [0, N/2] writes Z'_k and Z'_{N-k}
+        constexpr uint32_t half = N / 2, nh = half + 1;
+        for (uint32_t e = threadIdx.x; e < TY * nh; e += blockDim.x) {
+            const uint32_t r = e / nh, k = e % nh;
+            const float2 xk = scr[r * LD + k], xm = scr[r * LD + (N - k)];
+            const float2 zk = c2r_pre(xk, xm, ws[k]);
+            if (k != 0 && k != half) scr[r * LD + (N - k)] = c2r_pre(xm, xk, ws[N - k]);
+            scr[r * LD + k] = zk;
+        }
+        __syncthreads();
+        fft2pass<Z1, Z2, true, false, true>(scr, LD, twz, TY);   // pairs n < N/2 only
+        for (uint32_t e = threadIdx.x; e < TY * (N / 2); e += blockDim.x) {
+            const uint32_t r = e / (N / 2), n = e % (N / 2), yl = y0 + r;
+            if (yl >= ry1 || n >= A.nz) continue;
+            out0[((size_t)x * M1 + A.by0 + yl) * N + n] = scr[r * LD + n];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- N_k in the tiled layout
+// From the FP64 half spectrum z[q][x][y][kz] (cuFFT D2Z of N_r) to
+// nkt[kz][tile][q][kx][j] (real: float, kx < nkx; complex: float2, kx < m0), ky = tile T + j.
+__global__ void nk_tile_real(size_t Pk, uint32_t nkx, uint32_t m1, uint32_t Kz, uint32_t T,
+                             const double2* __restrict__ z, float* __restrict__ out, size_t total) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const uint32_t j = (uint32_t)(e % T);
+    size_t rest = e / T;
+    const uint32_t kx = (uint32_t)(rest % nkx); rest /= nkx;
+    const uint32_t q = (uint32_t)(rest % 6); rest /= 6;
+    const uint32_t tile = (uint32_t)(rest % (m1 / T));
+    const uint32_t kz = (uint32_t)(rest / (m1 / T));
+    const uint32_t ky = tile * T + j;
+    out[e] = (float)z[(size_t)q * Pk + ((size_t)kx * m1 + ky) * Kz + kz].x;
+}
+
+__global__ void nk_tile_cplx(size_t Pk, uint32_t m0, uint32_t m1, uint32_t Kz, uint32_t T,
+                             const double2* __restrict__ z, float2* __restrict__ out) {
+    const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= Pk * 9) return;
+    const uint32_t j = (uint32_t)(e % T);
+    size_t rest = e / T;
+    const uint32_t kx = (uint32_t)(rest % m0); rest /= m0;
+    const uint32_t q = (uint32_t)(rest % 9); rest /= 9;
+    const uint32_t tile = (uint32_t)(rest % (m1 / T));
+    const uint32_t kz = (uint32_t)(rest / (m1 / T));
+    const uint32_t ky = tile * T + j;
+    const double2 v = z[(size_t)q * Pk + ((size_t)kx * m1 + ky) * Kz + kz];
+    out[e] = make_float2((float)v.x, (float)v.y);
+}
+
+// Largest |N(kx) - N(m0-kx)| and |N(kx) + N(m0-kx)| (real parts) of each of the 6 components:
+// dev[2q] (even test), dev[2q+1] (odd test); non-negative doubles compare like their bits.
+__global__ void nk_parity_x(size_t Pk, uint32_t m0, uint32_t m1, uint32_t Kz, const double2* __restrict__ z,
+                            unsigned long long* dev) {
+    double de[6] = {0, 0, 0, 0, 0, 0}, dodd[6] = {0, 0, 0, 0, 0, 0};
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < Pk; i += (size_t)gridDim.x * blockDim.x) {
+        const uint32_t kx = (uint32_t)(i / ((size_t)m1 * Kz));
+        const size_t rest = i % ((size_t)m1 * Kz);
+        const size_t mi = (size_t)((m0 - kx) % m0) * m1 * Kz + rest;
+#pragma unroll
+        for (int q = 0; q < 6; q++) {
+            const double a = z[(size_t)q * Pk + i].x, b = z[(size_t)q * Pk + mi].x;
+            de[q] = fmax(de[q], fabs(a - b));
+            dodd[q] = fmax(dodd[q], fabs(a + b));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+        for (int o = 16; o > 0; o >>= 1) {
+            de[q] = fmax(de[q], __shfl_xor_sync(0xffffffffu, de[q], o));
+            dodd[q] = fmax(dodd[q], __shfl_xor_sync(0xffffffffu, dodd[q], o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMax(dev + 2 * q, (unsigned long long)__double_as_longlong(de[q]));
+            atomicMax(dev + 2 * q + 1, (unsigned long long)__double_as_longlong(dodd[q]));
+        }
+    }
+}
+
+uint32_t ilog2(uint32_t v) {
+    uint32_t l = 0;
+    while ((1u << l) < v) l++;
+    return l;
+}
+
+PlaneArgs plane_args(const LongRange& L) {
+    PlaneArgs A{};
+    const uint32_t m1 = L.mesh[1], N = L.mesh[2] / 2, Kz = N + 1;
+    const int z1 = split_r1((int)N), z2 = split_r2((int)N);
+    const uint32_t TY = 256 / (uint32_t)std::max(z1, z2);
+    const uint32_t LD = fft2pass_pitch(N, (uint32_t)z1, (uint32_t)z2);
+    A.m0 = L.mesh[0];
+    A.bx0 = L.box0[0]; A.by0 = L.box0[1];
+    A.zs = L.box0[2] / 2;
+    A.nz = L.box1[2] / 2 - A.zs + 1;
+    A.bx = L.box1[0] - L.box0[0] + 1;
+    A.by = L.box1[1] - L.box0[1] + 1;
+    A.ntile = m1 / PT;
+    A.CL = A.by >= 64 ? 4 : A.by >= 16 ? 2 : 1;
+    A.hy = 1u << ilog2((A.by + A.CL - 1) / A.CL);
+    A.lhy = ilog2(A.hy);
+    A.hk = (Kz + A.CL - 1) / A.CL;
+    A.ldz = A.hy | 1u;
+    const int r1 = split_r1((int)m1), r2 = split_r2((int)m1);
+    const uint32_t kzmax = 256 / (uint32_t)std::max(r1, r2);
+    const uint32_t rounds = (A.hk + kzmax - 1) / kzmax;
+    A.kzb = (A.hk + rounds - 1) / rounds;              // equal rounds of at most kzmax kz
+    A.scr = std::max<uint32_t>(TY * LD, A.kzb * (uint32_t)r1 * (uint32_t)(r2 + 1));
+    A.nkx = L.nk_nkx ? L.nk_nkx : A.m0;
+    A.odd = L.nk_odd;
+    A.P = L.P;
+    return A;
+}
+
+size_t zy_smem(const LongRange& L, const PlaneArgs& A) {
+    const uint32_t N = L.mesh[2] / 2;
+    return sizeof(float2) * ((size_t)(N + 1) * A.ldz + A.scr + 2 * N + 1 + L.mesh[1]);
+}
+
+size_t xconv_smem(const PlaneArgs& A, bool cplx) {
+    const size_t ys = ((3u * A.bx * PT * 8u) + 15u) & ~(size_t)15u;
+    const size_t ns = cplx ? (size_t)9 * A.m0 * PT * 8 : (size_t)6 * A.nkx * PT * 4;
+    const uint32_t r1 = (uint32_t)split_r1((int)A.m0), r2 = (uint32_t)split_r2((int)A.m0);
+    return ys + ns + sizeof(float2) * ((size_t)r1 * (r2 * PT + 8) + A.m0);
+}
+
+// Raise a kernel's dynamic shared-memory limit once per instantiation (and again only when a
+// larger size is asked for); the device is the one of the process's first plane launch.
+template <typename K>
+cudaError_t set_smem(K kern, size_t bytes) {
+    static size_t opted = 48 * 1024;
+    if (bytes <= opted) return cudaSuccess;
+    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) opted = bytes;
+    return e;
+}
+
+// A launch with thread-block clusters of `cl` blocks along x.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_clusters(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, uint32_t cl,
+                            Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
+// z split x y split instantiations: z N in {4..256}, y mesh in {8..256}
+#define ASD_ZY_CASES(M, Z1, Z2)                                                                           \
+    switch (M) {                                                                                          \
+    case 8: ASD_ZY_CALL(Z1, Z2, 4, 2) break;                                                              \
+    case 16: ASD_ZY_CALL(Z1, Z2, 4, 4) break;                                                             \
+    case 32: ASD_ZY_CALL(Z1, Z2, 8, 4) break;                                                             \
+    case 64: ASD_ZY_CALL(Z1, Z2, 8, 8) break;                                                             \
+    case 128: ASD_ZY_CALL(Z1, Z2, 16, 8) break;                                                           \
+    case 256: ASD_ZY_CALL(Z1, Z2, 16, 16) break;                                                          \
+    default: return cudaErrorInvalidValue;                                                                \
+    }
+
+#define ASD_Z_CASES(N, M)                                                                                 \
+    switch (N) {                                                                                          \
+    case 4: ASD_ZY_CASES(M, 2, 2) break;                                                                  \
+    case 8: ASD_ZY_CASES(M, 4, 2) break;                                                                  \
+    case 16: ASD_ZY_CASES(M, 4, 4) break;                                                                 \
+    case 32: ASD_ZY_CASES(M, 8, 4) break;                                                                 \
+    case 64: ASD_ZY_CASES(M, 8, 8) break;                                                                 \
+    case 128: ASD_ZY_CASES(M, 16, 8) break;                                                               \
+    case 256: ASD_ZY_CASES(M, 16, 16) break;                                                              \
+    default: return cudaErrorInvalidValue;                                                                \
+    }
+
+cudaError_t run_zy(const LongRange& L, const PlaneArgs& A, bool inverse, cudaStream_t st) {
+    const size_t sm = zy_smem(L, A);
+    const dim3 grid(A.bx * A.CL, 3);
+    const float* mr = L.r;
+    float* hr = L.r + 3 * L.P;
+    float2* yk = L.yk;
+    const float2* ykc = L.yk;
+    cudaError_t e = cudaSuccess;
+#define ASD_ZY_CALL(Z1, Z2, R1, R2)                                                                       \
+    if (inverse) {                                                                                        \
+        if ((e = set_smem(plane_yz_inv<Z1, Z2, R1, R2>, sm)) != cudaSuccess) return e;                    \
+        e = launch_clusters(plane_yz_inv<Z1, Z2, R1, R2>, grid, dim3(256), sm, st, A.CL, ykc, hr, A);     \
+    } else {                                                                                              \
+        if ((e = set_smem(plane_zy_fwd<Z1, Z2, R1, R2>, sm)) != cudaSuccess) return e;                    \
+        e = launch_clusters(plane_zy_fwd<Z1, Z2, R1, R2>, grid, dim3(256), sm, st, A.CL, mr, yk, A);      \
+    }
+    ASD_Z_CASES(L.mesh[2] / 2, L.mesh[1])
+#undef ASD_ZY_CALL
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+template <int R1, int R2>
+cudaError_t run_xconv_t(const LongRange& L, const PlaneArgs& A, bool cplx, cudaStream_t st) {
+    const uint32_t Kz = L.mesh[2] / 2 + 1;
+    const dim3 grid(A.ntile, Kz);
+    const size_t sm = xconv_smem(A, cplx);
+    cudaError_t e;
+    if (cplx) {
+        if ((e = set_smem(plane_x_conv<R1, R2, true>, sm)) != cudaSuccess) return e;
+        plane_x_conv<R1, R2, true><<<grid, PT * R1, sm, st>>>(L.yk, L.nkt, Kz, A);
+    } else {
+        if ((e = set_smem(plane_x_conv<R1, R2, false>, sm)) != cudaSuccess) return e;
+        plane_x_conv<R1, R2, false><<<grid, PT * R1, sm, st>>>(L.yk, L.nkt, Kz, A);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t run_xconv(const LongRange& L, const PlaneArgs& A, bool cplx, cudaStream_t st) {
+    switch (A.m0) {
+    case 4: return run_xconv_t<2, 2>(L, A, cplx, st);
+    case 8: return run_xconv_t<4, 2>(L, A, cplx, st);
+    case 16: return run_xconv_t<4, 4>(L, A, cplx, st);
+    case 32: return run_xconv_t<8, 4>(L, A, cplx, st);
+    case 64: return run_xconv_t<8, 8>(L, A, cplx, st);
+    case 128: return run_xconv_t<16, 8>(L, A, cplx, st);
+    case 256: return run_xconv_t<16, 16>(L, A, cplx, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace
+
+// The plane path applies when every mesh axis is a power of two (x 4..256, y 8..256, z 8..512:
+// the register transforms' sizes), the spins' box spans at most half the mesh along x and y and
+// its z pairs fit in half a row (so every forward pass skips the zero half of its input and
+// every inverse pass forms only the box half of its output), and the shared memory fits.
+bool plane_path_fits(const LongRange& L, bool cplx) {
+    auto p2 = [](uint32_t v) { return v >= 2 && (v & (v - 1)) == 0; };
+    if (!p2(L.mesh[0]) || !p2(L.mesh[1]) || !p2(L.mesh[2])) return false;
+    if (L.mesh[0] < 4 || L.mesh[0] > 256 || L.mesh[1] < 8 || L.mesh[1] > 256 || L.mesh[2] < 8 || L.mesh[2] > 512)
+        return false;
+    LongRange t = L;
+    t.nk_nkx = L.mesh[0];                              // the larger N_k tile bounds the shared memory
+    const PlaneArgs A = plane_args(t);
+    const uint32_t N = L.mesh[2] / 2;
+    if (2 * A.bx > L.mesh[0] || 2 * A.by > L.mesh[1] || 2 * A.nz > N) return false;
+    return zy_smem(L, A) <= 200 * 1024 && xconv_smem(A, cplx) <= 220 * 1024;
+}
+
+size_t plane_spectrum_elems(const LongRange& L) {
+    const PlaneArgs A = plane_args(L);
+    return 3 * (size_t)(L.mesh[2] / 2 + 1) * A.ntile * A.bx * PT;
+}
+
+// Tiled N_k from the FP64 half spectrum z[ncomp][m0][m1][Kz] (device); allocates L.nkt.  A real
+// N_k whose 6 components are each even or odd in kx (the point dipole and symmetric exchange on
+// a lattice with mirror symmetry in x) keeps only kx <= m0/2.
+cudaError_t build_nk_tiles(asd_handle* h, const double2* z, uint32_t ncomp, bool cplx) {
+    LongRange& L = h->lr;
+    const uint32_t Kz = L.mesh[2] / 2 + 1;
+    const size_t Pk = (size_t)L.mesh[0] * L.mesh[1] * Kz;
+    cudaError_t e;
+    if (!cplx) {
+        unsigned long long* dev = nullptr;
+        if ((e = cudaMalloc(&dev, 12 * sizeof(unsigned long long))) != cudaSuccess) return e;
+        cudaMemsetAsync(dev, 0, 12 * sizeof(unsigned long long), h->stream);
+        nk_parity_x<<<std::min<unsigned>(nbk(Pk, 256), 148 * 8), 256, 0, h->stream>>>(Pk, L.mesh[0], L.mesh[1], Kz,
+                                                                                         z, dev);
+        unsigned long long hb[12];
+        cudaMemcpyAsync(hb, dev, sizeof(hb), cudaMemcpyDeviceToHost, h->stream);
+        e = cudaStreamSynchronize(h->stream);
+        cudaFree(dev);
+        if (e != cudaSuccess) return e;
+        double d[12], big = 0.0;
+        for (int q = 0; q < 12; q++) { memcpy(&d[q], &hb[q], 8); big = std::max(big, d[q]); }
+        // tolerance: FP64 transform rounding relative to the spectrum's scale (big >= max |N_k|)
+        const double tol = 1e-11 * big;
+        uint32_t odd = 0;
+        bool ok = L.mesh[0] >= 2;
+        for (int q = 0; q < 6 && ok; q++) {
+            if (d[2 * q] <= tol) continue;                 // even
+            if (d[2 * q + 1] <= tol) { odd |= 1u << q; continue; }
+            ok = false;
+        }
+        L.nk_nkx = ok ? L.mesh[0] / 2 + 1 : L.mesh[0];
+        L.nk_odd = ok ? odd : 0;
+        const size_t total = (size_t)6 * L.nk_nkx * L.mesh[1] * Kz;
+        float* t = nullptr;
+        if ((e = cudaMalloc(&t, sizeof(float) * total)) != cudaSuccess) return e;
+        nk_tile_real<<<nbk(total, 256), 256, 0, h->stream>>>(Pk, L.nk_nkx, L.mesh[1], Kz, PT, z, t, total);
+        L.nkt = t;
+    } else {
+        float2* t = nullptr;
+        if ((e = cudaMalloc(&t, sizeof(float2) * 9 * Pk)) != cudaSuccess) return e;
+        (void)ncomp;
+        L.nk_nkx = L.mesh[0];
+        L.nk_odd = 0;
+        nk_tile_cplx<<<nbk(9 * Pk, 256), 256, 0, h->stream>>>(Pk, L.mesh[0], L.mesh[1], Kz, PT, z, t);
+        L.nkt = t;
+    }
+    return cudaGetLastError();
+}
+
+// M_r -> H_r through the three plane kernels.
+cudaError_t launch_lr_planes(asd_handle* h) {
+    LongRange& L = h->lr;
+    PlaneArgs A = plane_args(L);
+    A.err = h->d_err;
+    const bool cplx = !(L.ncomp == 6 && L.nk_real);
+    cudaError_t e;
+    if ((e = run_zy(L, A, false, h->stream)) != cudaSuccess) return e;
+    if ((e = run_xconv(L, A, cplx, h->stream)) != cudaSuccess) return e;
+    if ((e = run_zy(L, A, true, h->stream)) != cudaSuccess) return e;
+    h->launches += 3;
+    return cudaSuccess;
+}
+
+}  // namespace asd

@@ -98,6 +98,13 @@ struct LongRange {
     float2* k1 = nullptr;
     float2* k2 = nullptr;
     cufftHandle c2c = 0;
+    // plane path (every axis a power of two, x and y <= 256): the library's own three kernels
+    // (z+y forward, x + N_k product + inverse x, inverse y+z); the spectrum yk is
+    // [c][kz][ky tile][box x][8] and N_k is tiled to match ([kz][tile][comp][kx][8])
+    int planes = 0;
+    uint32_t nk_nkx = 0, nk_odd = 0;   // kx rows of the tiled N_k and its odd components (bits)
+    float2* yk = nullptr;
+    void* nkt = nullptr;
     // FP64 plain: complex padded arrays [3][P] and full complex N_k [9][P]
     double2 *zr = nullptr, *zk = nullptr, *zh = nullptr, *znk = nullptr;
     cufftHandle z2z = 0;
@@ -213,7 +220,11 @@ cudaError_t launch_plain_step(asd_handle* h, uint64_t t);
 cudaError_t launch_fused_step(asd_handle* h, uint32_t rel, bool in_capture);
 cudaError_t launch_step_advance(asd_handle* h, uint32_t nsteps);
 cudaError_t launch_lr_eval_f32(asd_handle* h);
-cudaError_t launch_lr_scatter_f32(asd_handle* h, const float* const s[3]);
+cudaError_t launch_lr_scatter(asd_handle* h);
+cudaError_t launch_lr_planes(asd_handle* h);
+bool plane_path_fits(const LongRange& L, bool cplx);
+size_t plane_spectrum_elems(const LongRange& L);
+cudaError_t build_nk_tiles(asd_handle* h, const double2* z, uint32_t ncomp, bool cplx);
 cudaError_t launch_lr_eval_plain(asd_handle* h, const double* s, double* out, bool overwrite_with_demag);
 cudaError_t launch_field_only(asd_handle* h, double* d_out);
 cudaError_t launch_plain_field(asd_handle* h, double* d_out);

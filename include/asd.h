@@ -68,6 +68,9 @@ extern "C" {
 #define ASD_FLAG_AUTOTUNE            (1u << 17) /* FP32 form: time block shapes at create */
 #define ASD_FLAG_STREAMED_EXCHANGE   (1u << 18) /* fused forms: keep every tensor in the matrix stream
                                                    instead of the typed (column, tensor-id) layout */
+#define ASD_FLAG_CUFFT_PLANES        (1u << 19) /* fused forms: run the (x, y) passes of the long-range
+                                                   transform through cuFFT instead of the library's
+                                                   plane kernels (comparison aid) */
 
 #define ASD_ALL_REPLICAS 0xFFFFFFFFu
 
@@ -275,7 +278,8 @@ int asd_time_steps_cold(asd_handle* h, uint64_t nsteps, uint64_t flush_bytes, do
 int asd_kernel_stats(const asd_handle* h, char* name, size_t name_len, double* avg_ms, uint64_t* count,
                      double* bytes_per_launch);
 /* Launch shape of the fused stage kernel chosen at create (block size, shared-memory staging of
- * the typed exchange words) and, with ASD_FLAG_AUTOTUNE, the autotuner's timings. */
+ * the typed exchange words), with ASD_FLAG_AUTOTUNE the autotuner's timings, and the transform
+ * path of the long-range field. */
 int asd_tuning(const asd_handle* h, char* out, size_t out_len);
 /* Set the fused stage kernel's launch shape by hand: block in {64, 128, 256}; staging 1 stages
  * each block's typed exchange words in shared memory by bulk copy, staging 2 also the spans of
