@@ -38,16 +38,13 @@ struct PlaneArgs {
     uint32_t zs, nz;                 // z rows: float2 pairs [zs, zs + nz) hold data, nz <= N/2
     uint32_t bx, by;                 // box extents along x (<= m0/2) and y (<= m1/2)
     uint32_t ntile;                  // ky tiles (m1 / PT)
-    // a (component, box row x) is shared by a cluster of CL blocks: block `rank` transforms the
-    // z rows y in [rank hy, rank hy + hy) and the kz in [rank hk, rank hk + hk); the transposed
-    // z spectrum of its rows, Zs[kz][ldz] (ldz odd, >= hy), is read and written across the
-    // cluster in distributed shared memory
-    uint32_t CL, hy, lhy, hk, ldz;
     uint32_t kzb;                    // kz values per y-pass round (rounds balanced)
     uint32_t scr;                    // scratch (float2) of the z/y passes
     uint32_t nkx;                    // kx rows of the N_k tile: m0 (full) or m0/2 + 1 (kx parity used)
     uint32_t odd;                    // bit q: component q of N_k is odd in kx (N(-kx) = -N(kx))
     size_t P;                        // padded real points
+    const float2* twt;               // twiddles: z (N), z split (N + 1), y (m1), x (m0)
+    uint32_t twx_off;                // offset of the x twiddles in twt (2N + 1 + m1)
     uint32_t* err;                   // device error bits
 };
 
@@ -71,34 +68,53 @@ __device__ __forceinline__ size_t yk_index(const PlaneArgs& A, uint32_t Kz, uint
 }
 
 // Compile-time geometry of the z/y kernels: z rows of N = Z1 Z2 complex points (mesh z = 2N),
-// y transforms of M1 = R1 R2 points.
+// y transforms of M1 = R1 R2 points.  A (component, box row x) is shared by a cluster of CL
+// blocks: block `rank` transforms the z rows y in [rank HY, rank HY + HY) (the box's y extent
+// is at most M1/2 = CL HY) and the kz in [rank HK, rank HK + HK); the transposed z spectrum of
+// its rows, Zs[KZ][LDZ], is read and written across the cluster in distributed shared memory.
+// HY is a multiple of R2, so the block owning row t + R2 k of a y pass is k / (HY / R2).
 template <int Z1, int Z2, int R1, int R2>
 struct ZYGeom {
     static constexpr uint32_t N = Z1 * Z2, KZ = N + 1;
     static constexpr uint32_t TY = 256 / (Z1 > Z2 ? Z1 : Z2);         // z rows per round
     static constexpr uint32_t LD = fft2pass_pitch(N, Z1, Z2);          // z row pitch
     static constexpr uint32_t M1 = R1 * R2;
+    static constexpr uint32_t CL = M1 >= 32 ? 4 : 1;
+    static constexpr uint32_t HY = M1 >= 32 ? M1 / 8 : M1 / 2;
+    static constexpr uint32_t KPB = HY / R2;                           // k values per owner block
+    static constexpr uint32_t LDZ = HY | 1u;
+    // the real kz = 0 and kz = N planes share one complex y transform (slot 0): N slots in all
+    static constexpr uint32_t HK = N / CL;
+    static_assert(CL == 1 || HY % R2 == 0, "cluster rows must be whole y-pass columns");
+    static_assert(N % CL == 0, "y-pass slots split evenly over the cluster");
 };
+__host__ __device__ constexpr uint32_t zy_cl(uint32_t m1) { return m1 >= 32 ? 4 : 1; }
+__host__ __device__ constexpr uint32_t zy_hy(uint32_t m1) { return m1 >= 32 ? m1 / 8 : m1 / 2; }
+
+// z and y twiddles from the table into shared memory (they are contiguous in both)
+__device__ __forceinline__ void copy_tw(float2* dst, const float2* __restrict__ src, uint32_t n) {
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) dst[j] = __ldg(src + j);
+}
 
 // ---------------------------------------------------------------- forward: z (R2C) then y
 template <int Z1, int Z2, int R1, int R2>
-__global__ void __launch_bounds__(256, 3) plane_zy_fwd(const float* __restrict__ mr, float2* __restrict__ yk,
+__global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const float* __restrict__ mr, float2* __restrict__ yk,
                                                        const PlaneArgs A) {
     using G = ZYGeom<Z1, Z2, R1, R2>;
     constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
+    constexpr uint32_t CL = G::CL, HY = G::HY, LDZ = G::LDZ, HK = G::HK, KPB = G::KPB;
     extern __shared__ __align__(16) float2 sm[];
     cg::cluster_group cl = cg::this_cluster();
-    float2* Zs = sm;                                   // [KZ][ldz]: this block's z rows
-    float2* scr = Zs + (size_t)KZ * A.ldz;             // z rows [TY][LD] | y exchange [kzb][R1][R2+1]
+    float2* Zs = sm;                                   // [KZ][LDZ]: this block's z rows
+    float2* scr = Zs + (size_t)KZ * LDZ;               // z rows [TY][LD] | y exchange [kzb][R1][R2+1]
     float2* twz = scr + A.scr;                         // N + (N + 1) z twiddles
     float2* twy = twz + 2 * N + 1;                     // M1 y twiddles
     const uint32_t rank = cl.block_rank();
-    const uint32_t xl = blockIdx.x / A.CL, c = blockIdx.y, x = A.bx0 + xl;
-    load_twiddles(twz, N);
-    load_tw(twy, M1);
+    const uint32_t xl = blockIdx.x / CL, c = blockIdx.y, x = A.bx0 + xl;
+    copy_tw(twz, A.twt, 2 * N + 1 + M1);
     const float2* row0 = reinterpret_cast<const float2*>(mr + (size_t)c * A.P) + A.zs;
     const float2* ws = twz + N;
-    const uint32_t ry0 = rank * A.hy, ry1 = min(A.by, ry0 + A.hy);
+    const uint32_t ry0 = rank * HY, ry1 = min(A.by, ry0 + HY);
     for (uint32_t y0 = ry0; y0 < ry1; y0 += TY) {
         __syncthreads();
         // rows shifted to the z pair zs; pairs n >= N/2 are zero and not read by the pruned pass
@@ -110,27 +126,40 @@ __global__ void __launch_bounds__(256, 3) plane_zy_fwd(const float* __restrict__
         }
         __syncthreads();
         fft2pass<Z1, Z2, false, true, false>(scr, LD, twz, TY);
-        for (uint32_t e = threadIdx.x; e < KZ * TY; e += blockDim.x) {
-            const uint32_t r = e / KZ, k = e % KZ, yl = y0 + r;
+        // X_k and X_{N-k} from the same two values Z_k, Z_{N-k}
+        constexpr uint32_t NH = N / 2 + 1;
+        for (uint32_t e = threadIdx.x; e < NH * TY; e += blockDim.x) {
+            const uint32_t r = e / NH, k = e % NH, yl = y0 + r;
             if (yl >= ry1) continue;
             const float2 zk = scr[r * LD + (k & (N - 1))], zm = scr[r * LD + ((N - k) & (N - 1))];
-            Zs[k * A.ldz + (yl - ry0)] = r2c_split(zk, zm, ws[k]);
+            float2* zc = Zs + (yl - ry0);
+            zc[k * LDZ] = r2c_split(zk, zm, ws[k]);
+            if (k != N / 2) zc[(N - k) * LDZ] = r2c_split(zm, zk, ws[N - k]);
         }
     }
     cl.sync();                                         // every block's rows are in its Zs
-    const uint32_t kz_lo = rank * A.hk, kz_hi = min(KZ, kz_lo + A.hk);
-    for (uint32_t kz0 = kz_lo; kz0 < kz_hi; kz0 += A.kzb) {
+    const float2* zb[CL];
+#pragma unroll
+    for (uint32_t o = 0; o < CL; o++) zb[o] = cl.map_shared_rank(Zs, o);
+    // y transforms of this block's slots: slot s >= 1 is the plane kz = s; slot 0 carries the two
+    // real planes kz = 0 and kz = N as P = X_0 + i X_N, whose transform C gives
+    // F_0(ky) = (C(ky) + conj C(-ky)) / 2 and F_N(ky) = (C(ky) - conj C(-ky)) / 2i
+    float2* cpk = scr + A.kzb * R1 * (R2 + 1);         // [M1]: C of slot 0
+    const uint32_t s_lo = rank * HK, s_hi = s_lo + HK;
+    for (uint32_t s0 = s_lo; s0 < s_hi; s0 += A.kzb) {
         {
-            const uint32_t kzl = threadIdx.x / R2, t = threadIdx.x % R2, kz = kz0 + kzl;
-            if (kzl < A.kzb && kz < kz_hi) {
+            const uint32_t kzl = threadIdx.x / R2, t = threadIdx.x % R2, sl = s0 + kzl;
+            if (kzl < A.kzb && sl < s_hi) {
                 float2 v[R1];
 #pragma unroll
                 for (int k = 0; k < R1 / 2; k++) {     // rows y >= M1/2 are zero
                     const uint32_t yy = t + R2 * k;
+                    constexpr uint32_t kpb = CL == 1 ? R1 : KPB;
+                    const uint32_t off = t + R2 * (k % kpb);
                     v[k] = make_float2(0.f, 0.f);
                     if (yy < A.by) {
-                        const float2* zp = cl.map_shared_rank(Zs, yy >> A.lhy);
-                        v[k] = zp[kz * A.ldz + (yy & (A.hy - 1))];
+                        if (sl) v[k] = zb[k / kpb][sl * LDZ + off];
+                        else v[k] = make_float2(zb[k / kpb][off].x, zb[k / kpb][N * LDZ + off].x);
                     }
                 }
                 dftp<R1, false, true, false>(v);
@@ -141,15 +170,29 @@ __global__ void __launch_bounds__(256, 3) plane_zy_fwd(const float* __restrict__
             }
         }
         __syncthreads();
+        const bool packed = s0 == 0;                   // block-uniform: slot 0 is in this round
         {
-            const uint32_t kzl = threadIdx.x / R1, m = threadIdx.x % R1, kz = kz0 + kzl;
-            if (kzl < A.kzb && kz < kz_hi) {
+            const uint32_t kzl = threadIdx.x / R1, m = threadIdx.x % R1, sl = s0 + kzl;
+            if (kzl < A.kzb && sl < s_hi) {
                 float2 u[R2];
 #pragma unroll
                 for (int t = 0; t < R2; t++) u[t] = scr[(kzl * R1 + m) * (R2 + 1) + t];
                 dft<R2, false>(u);
+                if (sl) {
 #pragma unroll
-                for (int q = 0; q < R2; q++) yk[yk_index(A, KZ, c, kz, xl, m + R1 * q)] = u[q];
+                    for (int q = 0; q < R2; q++) yk[yk_index(A, KZ, c, sl, xl, m + R1 * q)] = u[q];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < R2; q++) cpk[m + R1 * q] = u[q];
+                }
+            }
+        }
+        if (packed) {
+            __syncthreads();
+            for (uint32_t ky = threadIdx.x; ky < M1; ky += blockDim.x) {
+                const float2 a = cpk[ky], b = cpk[(M1 - ky) & (M1 - 1)];
+                yk[yk_index(A, KZ, c, 0, xl, ky)] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+                yk[yk_index(A, KZ, c, N, xl, ky)] = make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x));
             }
         }
         __syncthreads();
@@ -192,7 +235,7 @@ __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __
         bulk_copy_stream(Nsb, static_cast<const unsigned char*>(nkt) + ((size_t)kz * A.ntile + tile) * ns_bytes,
                          ns_bytes, &bar);
     }
-    load_tw(twx, M0);
+    copy_tw(twx, A.twt + A.twx_off, M0);
     __syncthreads();
     if (!mbar_wait_bounded(&bar, STAGE_WAIT_POLLS)) {
         // the copies did not land in time: flag it, leave this tile untransformed, and retire
@@ -300,26 +343,39 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
                                                        const PlaneArgs A) {
     using G = ZYGeom<Z1, Z2, R1, R2>;
     constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
+    constexpr uint32_t CL = G::CL, HY = G::HY, LDZ = G::LDZ, HK = G::HK, KPB = G::KPB;
     extern __shared__ __align__(16) float2 sm[];
     cg::cluster_group cl = cg::this_cluster();
     float2* Zs = sm;
-    float2* scr = Zs + (size_t)KZ * A.ldz;
+    float2* scr = Zs + (size_t)KZ * LDZ;
     float2* twz = scr + A.scr;
     float2* twy = twz + 2 * N + 1;
     const uint32_t rank = cl.block_rank();
-    const uint32_t xl = blockIdx.x / A.CL, c = blockIdx.y, x = A.bx0 + xl;
-    load_twiddles(twz, N);
-    load_tw(twy, M1);
-    __syncthreads();
-    // inverse y of this block's kz: every box row's value goes to the Zs of the block owning it
-    const uint32_t kz_lo = rank * A.hk, kz_hi = min(KZ, kz_lo + A.hk);
-    for (uint32_t kz0 = kz_lo; kz0 < kz_hi; kz0 += A.kzb) {
-        {
-            const uint32_t kzl = threadIdx.x / R1, m = threadIdx.x % R1, kz = kz0 + kzl;
-            if (kzl < A.kzb && kz < kz_hi) {
-                float2 u[R2];
+    const uint32_t xl = blockIdx.x / CL, c = blockIdx.y, x = A.bx0 + xl;
+    copy_tw(twz, A.twt, 2 * N + 1 + M1);
+    float2* zb[CL];
 #pragma unroll
-                for (int q = 0; q < R2; q++) u[q] = yk[yk_index(A, KZ, c, kz, xl, m + R1 * q)];
+    for (uint32_t o = 0; o < CL; o++) zb[o] = cl.map_shared_rank(Zs, o);
+    __syncthreads();
+    // inverse y of this block's slots (slot 0: D = G_0 + i G_N of the real planes kz = 0 and N,
+    // whose inverse is g_0 + i g_N); every box row's value goes to the Zs of the block owning it
+    const uint32_t s_lo = rank * HK, s_hi = s_lo + HK;
+    for (uint32_t s0 = s_lo; s0 < s_hi; s0 += A.kzb) {
+        {
+            const uint32_t kzl = threadIdx.x / R1, m = threadIdx.x % R1, sl = s0 + kzl;
+            if (kzl < A.kzb && sl < s_hi) {
+                float2 u[R2];
+                if (sl) {
+#pragma unroll
+                    for (int q = 0; q < R2; q++) u[q] = yk[yk_index(A, KZ, c, sl, xl, m + R1 * q)];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < R2; q++) {
+                        const float2 g0 = yk[yk_index(A, KZ, c, 0, xl, m + R1 * q)];
+                        const float2 gn = yk[yk_index(A, KZ, c, N, xl, m + R1 * q)];
+                        u[q] = make_float2(g0.x - gn.y, g0.y + gn.x);
+                    }
+                }
                 dft<R2, true>(u);
 #pragma unroll
                 for (int t = 0; t < R2; t++)
@@ -328,8 +384,8 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
         }
         __syncthreads();
         {
-            const uint32_t kzl = threadIdx.x / R2, t = threadIdx.x % R2, kz = kz0 + kzl;
-            if (kzl < A.kzb && kz < kz_hi) {
+            const uint32_t kzl = threadIdx.x / R2, t = threadIdx.x % R2, sl = s0 + kzl;
+            if (kzl < A.kzb && sl < s_hi) {
                 float2 w[R1];
 #pragma unroll
                 for (int m = 0; m < R1; m++) w[m] = scr[(kzl * R1 + m) * (R2 + 1) + t];
@@ -337,9 +393,15 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
 #pragma unroll
                 for (int k = 0; k < R1 / 2; k++) {
                     const uint32_t yy = t + R2 * k;
+                    constexpr uint32_t kpb = CL == 1 ? R1 : KPB;
+                    const uint32_t off = t + R2 * (k % kpb);
                     if (yy < A.by) {
-                        float2* zp = cl.map_shared_rank(Zs, yy >> A.lhy);
-                        zp[kz * A.ldz + (yy & (A.hy - 1))] = w[k];
+                        if (sl) {
+                            zb[k / kpb][sl * LDZ + off] = w[k];
+                        } else {
+                            zb[k / kpb][off] = make_float2(w[k].x, 0.f);
+                            zb[k / kpb][N * LDZ + off] = make_float2(w[k].y, 0.f);
+                        }
                     }
                 }
             }
@@ -349,11 +411,11 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
     cl.sync();                                         // every row of every block's Zs is written
     const float2* ws = twz + N;
     float2* out0 = reinterpret_cast<float2*>(hr + (size_t)c * A.P) + A.zs;
-    const uint32_t ry0 = rank * A.hy, ry1 = min(A.by, ry0 + A.hy);
+    const uint32_t ry0 = rank * HY, ry1 = min(A.by, ry0 + HY);
     for (uint32_t y0 = ry0; y0 < ry1; y0 += TY) {
         for (uint32_t e = threadIdx.x; e < KZ * TY; e += blockDim.x) {
             const uint32_t r = e / KZ, k = e % KZ, yl = y0 + r;
-            scr[r * LD + k] = yl < ry1 ? Zs[k * A.ldz + (yl - ry0)] : make_float2(0.f, 0.f);
+            scr[r * LD + k] = yl < ry1 ? Zs[k * LDZ + (yl - ry0)] : make_float2(0.f, 0.f);
         }
         __syncthreads();
         // pairwise in place: thread (r, k) for k in [0, N/2] writes Z'_k and Z'_{N-k}
@@ -437,6 +499,22 @@ __global__ void nk_parity_x(size_t Pk, uint32_t m0, uint32_t m1, uint32_t Kz, co
     }
 }
 
+// Twiddle table of the plane kernels, rounded from double precision: exp(-2 pi i j / N) (j < N),
+// exp(-i pi k / N) (k <= N), exp(-2 pi i j / m1) (j < m1), exp(-2 pi i j / m0) (j < m0).
+__global__ void tw_table_k(uint32_t N, uint32_t m1, uint32_t m0, float2* __restrict__ t) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n1 = 2 * N + 1, n2 = n1 + m1, n3 = n2 + m0;
+    if (i >= n3) return;
+    double a;
+    if (i < N) a = -2.0 * (double)i / (double)N;
+    else if (i < n1) a = -(double)(i - N) / (double)N;
+    else if (i < n2) a = -2.0 * (double)(i - n1) / (double)m1;
+    else a = -2.0 * (double)(i - n2) / (double)m0;
+    double sn, cs;
+    sincospi(a, &sn, &cs);
+    t[i] = make_float2((float)cs, (float)sn);
+}
+
 uint32_t ilog2(uint32_t v) {
     uint32_t l = 0;
     while ((1u << l) < v) l++;
@@ -456,25 +534,23 @@ PlaneArgs plane_args(const LongRange& L) {
     A.bx = L.box1[0] - L.box0[0] + 1;
     A.by = L.box1[1] - L.box0[1] + 1;
     A.ntile = m1 / PT;
-    A.CL = A.by >= 64 ? 4 : A.by >= 16 ? 2 : 1;
-    A.hy = 1u << ilog2((A.by + A.CL - 1) / A.CL);
-    A.lhy = ilog2(A.hy);
-    A.hk = (Kz + A.CL - 1) / A.CL;
-    A.ldz = A.hy | 1u;
+    const uint32_t CL = zy_cl(m1), hk = N / CL;       // y-pass slots per block
     const int r1 = split_r1((int)m1), r2 = split_r2((int)m1);
     const uint32_t kzmax = 256 / (uint32_t)std::max(r1, r2);
-    const uint32_t rounds = (A.hk + kzmax - 1) / kzmax;
-    A.kzb = (A.hk + rounds - 1) / rounds;              // equal rounds of at most kzmax kz
-    A.scr = std::max<uint32_t>(TY * LD, A.kzb * (uint32_t)r1 * (uint32_t)(r2 + 1));
+    const uint32_t rounds = (hk + kzmax - 1) / kzmax;
+    A.kzb = (hk + rounds - 1) / rounds;                // equal rounds of at most kzmax kz
+    A.scr = std::max<uint32_t>(TY * LD, A.kzb * (uint32_t)r1 * (uint32_t)(r2 + 1) + m1);
     A.nkx = L.nk_nkx ? L.nk_nkx : A.m0;
     A.odd = L.nk_odd;
     A.P = L.P;
+    A.twt = L.twt;
+    A.twx_off = 2 * N + 1 + m1;
     return A;
 }
 
 size_t zy_smem(const LongRange& L, const PlaneArgs& A) {
-    const uint32_t N = L.mesh[2] / 2;
-    return sizeof(float2) * ((size_t)(N + 1) * A.ldz + A.scr + 2 * N + 1 + L.mesh[1]);
+    const uint32_t N = L.mesh[2] / 2, ldz = zy_hy(L.mesh[1]) | 1u;
+    return sizeof(float2) * ((size_t)(N + 1) * ldz + A.scr + 2 * N + 1 + L.mesh[1]);
 }
 
 size_t xconv_smem(const PlaneArgs& A, bool cplx) {
@@ -540,7 +616,8 @@ cudaError_t launch_clusters(void (*kern)(KArgs...), dim3 grid, dim3 block, size_
 
 cudaError_t run_zy(const LongRange& L, const PlaneArgs& A, bool inverse, cudaStream_t st) {
     const size_t sm = zy_smem(L, A);
-    const dim3 grid(A.bx * A.CL, 3);
+    const uint32_t CL = zy_cl(L.mesh[1]);
+    const dim3 grid(A.bx * CL, 3);
     const float* mr = L.r;
     float* hr = L.r + 3 * L.P;
     float2* yk = L.yk;
@@ -549,10 +626,10 @@ cudaError_t run_zy(const LongRange& L, const PlaneArgs& A, bool inverse, cudaStr
 #define ASD_ZY_CALL(Z1, Z2, R1, R2)                                                                       \
     if (inverse) {                                                                                        \
         if ((e = set_smem(plane_yz_inv<Z1, Z2, R1, R2>, sm)) != cudaSuccess) return e;                    \
-        e = launch_clusters(plane_yz_inv<Z1, Z2, R1, R2>, grid, dim3(256), sm, st, A.CL, ykc, hr, A);     \
+        e = launch_clusters(plane_yz_inv<Z1, Z2, R1, R2>, grid, dim3(256), sm, st, CL, ykc, hr, A);       \
     } else {                                                                                              \
         if ((e = set_smem(plane_zy_fwd<Z1, Z2, R1, R2>, sm)) != cudaSuccess) return e;                    \
-        e = launch_clusters(plane_zy_fwd<Z1, Z2, R1, R2>, grid, dim3(256), sm, st, A.CL, mr, yk, A);      \
+        e = launch_clusters(plane_zy_fwd<Z1, Z2, R1, R2>, grid, dim3(256), sm, st, CL, mr, yk, A);         \
     }
     ASD_Z_CASES(L.mesh[2] / 2, L.mesh[1])
 #undef ASD_ZY_CALL
@@ -658,6 +735,16 @@ cudaError_t build_nk_tiles(asd_handle* h, const double2* z, uint32_t ncomp, bool
         nk_tile_cplx<<<nbk(9 * Pk, 256), 256, 0, h->stream>>>(Pk, L.mesh[0], L.mesh[1], Kz, PT, z, t);
         L.nkt = t;
     }
+    return cudaGetLastError();
+}
+
+// Twiddle table of the plane kernels (allocates L.twt).
+cudaError_t build_plane_twiddles(asd_handle* h) {
+    LongRange& L = h->lr;
+    const uint32_t N = L.mesh[2] / 2, n = 2 * N + 1 + L.mesh[1] + L.mesh[0];
+    cudaError_t e = cudaMalloc(&L.twt, sizeof(float2) * n);
+    if (e != cudaSuccess) return e;
+    tw_table_k<<<nbk(n, 256), 256, 0, h->stream>>>(N, L.mesh[1], L.mesh[0], L.twt);
     return cudaGetLastError();
 }
 

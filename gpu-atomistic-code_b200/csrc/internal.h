@@ -105,6 +105,7 @@ struct LongRange {
     uint32_t nk_nkx = 0, nk_odd = 0;   // kx rows of the tiled N_k and its odd components (bits)
     float2* yk = nullptr;
     void* nkt = nullptr;
+    float2* twt = nullptr;          // twiddle table of the plane kernels
     // FP64 plain: complex padded arrays [3][P] and full complex N_k [9][P]
     double2 *zr = nullptr, *zk = nullptr, *zh = nullptr, *znk = nullptr;
     cufftHandle z2z = 0;
@@ -222,6 +223,7 @@ cudaError_t launch_step_advance(asd_handle* h, uint32_t nsteps);
 cudaError_t launch_lr_eval_f32(asd_handle* h);
 cudaError_t launch_lr_scatter(asd_handle* h);
 cudaError_t launch_lr_planes(asd_handle* h);
+cudaError_t build_plane_twiddles(asd_handle* h);
 bool plane_path_fits(const LongRange& L, bool cplx);
 size_t plane_spectrum_elems(const LongRange& L);
 cudaError_t build_nk_tiles(asd_handle* h, const double2* z, uint32_t ncomp, bool cplx);
