@@ -54,18 +54,18 @@ def pinned(n):
     return arr, (rt, p)
 
 
-def ncu_traffic(workload):
-    """Per-launch DRAM bytes of the stage kernel from the committed ncu summary, if any."""
-    d = os.path.join(REPO, "profiles")
-    if not os.path.isdir(d):
+def ncu_traffic(workload, kernel):
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of `kernel` on
+    `workload` from the committed ncu table profiles/dram_traffic.csv (columns workload, kernel
+    prefix, bytes, source capture), or None."""
+    path = os.path.join(REPO, "profiles", "dram_traffic.csv")
+    if not os.path.exists(path):
         return None
-    for fn in sorted(os.listdir(d)):
-        if not fn.endswith(".md"):
-            continue
-        for line in open(os.path.join(d, fn)):
-            m = re.match(r"\s*bench-traffic\s+(\S+)\s+([0-9.eE+]+)", line)
-            if m and m.group(1) == workload:
-                return float(m.group(2))
+    import csv
+    with open(path) as f:
+        for row in csv.DictReader(f):
+            if row["workload"] == workload and kernel.startswith(row["kernel"]):
+                return float(row["bytes"])
     return None
 
 
@@ -323,10 +323,16 @@ def run_ours(args):
     ms_warm = allmax(ms_warm)
 
     # dominant kernel: per-launch CUDA-event time of the fused stage kernel, cold L2 per launch
+    # every kernel of the step timed launch by launch with a cold L2; the dominant one (largest
+    # summed time) carries the roofline, the others are listed beside it
     ks = h.time_kernels(max(4, min(args.steps, 20)), FLUSH_BYTES)
     peak, peak_kind = hbm_peak()
     achieved = ks["bytes"] / (ks["avg_ms"] * 1e-3) / 1e9 if ks["avg_ms"] > 0 else None
-    traffic = ncu_traffic(args.workload)
+    traffic = ncu_traffic(args.workload, ks["name"])
+    kernels = [{"kernel": k["name"], "avg_ms": k["avg_ms"], "launches": k["count"], "alg_bytes_per_launch": k["bytes"],
+                "achieved_gbs": k["bytes"] / (k["avg_ms"] * 1e-3) / 1e9 if k["avg_ms"] > 0 else None,
+                "frac": (k["bytes"] / (k["avg_ms"] * 1e-3) / 1e9 / peak) if k["avg_ms"] > 0 else None,
+                "traffic": ncu_traffic(args.workload, k["name"])} for k in ks["kernels"]]
 
     # end to end through the C ABI with host buffers: upload spins, per step set the
     # applied field (H2D) + step + magnetisation read-back (D2H), download spins
@@ -362,9 +368,11 @@ def run_ours(args):
            "d2h_bytes_per_step": (24 * n + 8 * nsub_out * args.steps) / args.steps,
            "calls_per_step": "asd_set_applied + asd_step(1) + asd_magnetisation", "host_buffers": "pinned"}
 
-    # FP64 plain form on the same input, and the FP32 error against it on the same noise
+    # FP64 plain form on the same input; the FP32 and fused FP64 forms' errors against it on the
+    # same noise, and the fused FP64 form's throughput
     plain = None
     err = None
+    fused64 = None
     if not args.no_plain:
         pp = A.RunParams(precision=A.FP64_PLAIN, seed=1 + rank, **kw)
         hp = A.Handle(pp, systems)
@@ -376,17 +384,28 @@ def run_ours(args):
         msp = allmax(msp)
         plain = {"value": n * world * kp / (msp * 1e-3), "ms_per_step": msp / kp, "steps": kp, "gpu_launches": lp}
         hp.close()
+        p64 = A.RunParams(precision=A.FP64_FUSED, seed=1 + rank, flags=A.FLAG_AUTOTUNE, **kw)
+        hf = A.Handle(p64, systems)
+        hf.set_spins(S0)
+        hf.step(3)
+        hf.sync()
+        msf, lf = hf.time_steps_cold(kp, FLUSH_BYTES)
+        msf = allmax(msf)
+        hf.close()
         ne = args.err_steps
-        ha = A.Handle(p32, systems)
-        hb = A.Handle(pp, systems)
-        ha.set_spins(S0)
-        hb.set_spins(S0)
-        ha.step(ne)
-        hb.step(ne)
-        err = {"max_abs_dS": float(np.abs(ha.get_spins() - hb.get_spins()).max()), "steps": ne,
-               "vs": "FP64 plain form, same initial spins and same Philox noise"}
-        ha.close()
-        hb.close()
+        hs = {k: A.Handle(pr, systems) for k, pr in (("fp32", p32), ("fp64_fused", p64), ("plain", pp))}
+        for hh in hs.values():
+            hh.set_spins(S0)
+            hh.step(ne)
+        ref = hs["plain"].get_spins()
+        e32 = float(np.abs(hs["fp32"].get_spins() - ref).max())
+        e64 = float(np.abs(hs["fp64_fused"].get_spins() - ref).max())
+        for hh in hs.values():
+            hh.close()
+        err = {"max_abs_dS": e32, "steps": ne, "vs": "FP64 plain form, same initial spins and same Philox noise"}
+        fused64 = {"value": n * world * kp / (msf * 1e-3), "ms_per_step": msf / kp, "steps": kp, "gpu_launches": lf,
+                   "max_abs_dS_vs_fp64_plain": e64, "err_steps": ne,
+                   "speedup_vs_fp64_plain": (msp / msf)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -424,8 +443,9 @@ def run_ours(args):
                              "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                              "kernel": ks["name"], "kernel_avg_ms": ks["avg_ms"],
                              "alg_bytes_per_launch": ks["bytes"], "peak_source": peak_kind},
+                "kernels": kernels,
                 "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
-                "fp64_plain": plain, "error_vs_fp64": err,
+                "fp64_plain": plain, "error_vs_fp64": err, "fp64_fused": fused64,
                 "speedup_vs_fp64_plain": (value / plain["value"]) if plain else None}
         print(json.dumps(line), flush=True)
     h.close()

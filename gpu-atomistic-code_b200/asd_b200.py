@@ -47,6 +47,7 @@ EXPORTED = [
     "asd_time_kernels_cold", "asd_time_steps_cold", "asd_read_ucf", "asd_read_exch", "asd_read_csr_exch",
     "asd_write_csr_exch", "asd_plan_spin_spans", "asd_set_device_layout", "asd_set_ttm",
     "asd_get_ttm_temperatures", "asd_set_four_spin", "asd_spins_random", "asd_spins_pattern",
+    "asd_kernel_table",
 ]
 
 
@@ -133,6 +134,7 @@ def load_library(path: str = LIB_PATH):
         "asd_time_steps": ([P, C.c_uint64, dp, C.POINTER(C.c_uint64)], C.c_int),
         "asd_time_kernels": ([P, C.c_uint64], C.c_int),
         "asd_kernel_stats": ([P, C.c_char_p, C.c_size_t, dp, C.POINTER(C.c_uint64), dp], C.c_int),
+        "asd_kernel_table": ([P, C.c_char_p, C.c_size_t], C.c_int),
         "asd_thermal_normals": ([C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, dp], C.c_int),
         "asd_magnetisation_noalloc": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p],
                                       C.c_int),
@@ -501,7 +503,14 @@ class Handle:
         name = C.create_string_buffer(128)
         avg, cnt, b = C.c_double(), C.c_uint64(), C.c_double()
         _check(lib.asd_kernel_stats(self.h, name, 128, C.byref(avg), C.byref(cnt), C.byref(b)), self.h)
-        return {"name": name.value.decode(), "avg_ms": avg.value, "count": cnt.value, "bytes": b.value}
+        tab = C.create_string_buffer(8192)
+        _check(lib.asd_kernel_table(self.h, tab, len(tab)), self.h)
+        kernels = []
+        for line in tab.value.decode().splitlines():
+            nm, ms, c, by = line.split("|")
+            kernels.append({"name": nm, "avg_ms": float(ms), "count": int(c), "bytes": float(by)})
+        return {"name": name.value.decode(), "avg_ms": avg.value, "count": cnt.value, "bytes": b.value,
+                "kernels": kernels}
 
 
 def _read_check(rc: int, err):

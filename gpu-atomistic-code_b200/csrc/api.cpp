@@ -89,6 +89,7 @@ void free_all(asd_handle* h) {
     if (h->sq.plan) cufftDestroy(h->sq.plan);
     F(h->d_magpart); F(h->d_mag); F(h->d_inv_count); F(h->d_sub_of_atom); F(h->d_stats);
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->graph1) cudaGraphExecDestroy(h->graph1);
     if (h->kev[0]) cudaEventDestroy(h->kev[0]);
     if (h->kev[1]) cudaEventDestroy(h->kev[1]);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -364,6 +365,7 @@ void set_dyn(asd_handle* h, int idx, double v) {
     if (idx != DYN_DET_STEP) CK(launch_set_scalar_f(h, h->d_dynf + idx, (float)v));
 }
 
+// The long-range input from the current spins (after new spins).
 void scatter_if_needed(asd_handle* h) {
     if (h->lr.mode == ASD_LR_NONE || h->p.precision == ASD_FP64_PLAIN || h->lr_scattered) return;
     CK(launch_lr_scatter(h));
@@ -497,9 +499,11 @@ void autotune(asd_handle* h) {
 
 void destroy_graph(asd_handle* h) {
     if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_steps = 0; }
+    if (h->graph1) { cudaGraphExecDestroy(h->graph1); h->graph1 = nullptr; }
 }
 
-// Capture `steps` fused steps + the counter advance into one graph.
+// Capture `steps` fused steps + the counter advance into one graph, and a one-step graph for
+// single-step calls: the det-field step taken from the device counter, the step, the advance.
 void build_graph(asd_handle* h, uint32_t steps) {
     destroy_graph(h);
     cudaGraph_t g;
@@ -521,6 +525,22 @@ void build_graph(asd_handle* h, uint32_t steps) {
     CK(cudaGraphInstantiate(&h->graph, g, 0));
     cudaGraphDestroy(g);
     h->graph_steps = steps;
+    // one step: valid whatever the phase when the long-range refresh pattern does not depend on it
+    const uint32_t upd = h->p.update ? h->p.update : 1;
+    if (h->lr.mode == ASD_LR_DIPOLE && upd != 1) return;
+    h->step = 0;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    e = launch_det_here(h);
+    if (e == cudaSuccess) e = launch_fused_step(h, 0, true);
+    if (e == cudaSuccess) e = launch_step_advance(h, 1);
+    e2 = cudaStreamEndCapture(h->stream, &g);
+    h->step = saved;
+    h->graph1_launches = h->launches - before;
+    h->launches = before;
+    CK(e);
+    CK(e2);
+    CK(cudaGraphInstantiate(&h->graph1, g, 0));
+    cudaGraphDestroy(g);
 }
 
 void run_steps(asd_handle* h, uint64_t nsteps) {
@@ -531,6 +551,13 @@ void run_steps(asd_handle* h, uint64_t nsteps) {
         return;
     }
     scatter_if_needed(h);
+    if (nsteps == 1 && h->graph1 && !h->timing) {
+        // one launch: the graph sets the det-field step to the step it runs
+        CK(cudaGraphLaunch(h->graph1, h->stream));
+        h->launches += h->graph1_launches;
+        h->step += 1;
+        return;
+    }
     set_dyn(h, DYN_DET_STEP, (double)(h->step + nsteps - 1));
     const uint32_t upd = h->p.update ? h->p.update : 1;
     const uint32_t G = h->graph_steps;
@@ -1499,7 +1526,7 @@ int asd_time_kernels_cold(asd_handle* h, uint64_t nsteps, uint64_t flush_bytes) 
     try {
         CK(cudaSetDevice(h->device));
         CK(cudaStreamSynchronize(h->stream));
-        h->ktimer = KernelTimer{};
+        h->ktab.clear();
         if (flush_bytes) {
             CK(cudaMalloc(&h->flush_buf, flush_bytes));
             h->flush_bytes = flush_bytes;
@@ -1560,15 +1587,34 @@ int asd_time_steps_cold(asd_handle* h, uint64_t nsteps, uint64_t flush_bytes, do
     return ASD_OK;
 }
 
+// The dominant kernel of the last asd_time_kernels: the largest device time summed over its
+// launches.
 int asd_kernel_stats(const asd_handle* h, char* name, size_t name_len, double* avg_ms, uint64_t* count,
                      double* bytes_per_launch) {
     if (!h) return ASD_EINVAL;
-    if (name && name_len) {
-        snprintf(name, name_len, "%s", h->ktimer.name.c_str());
+    const KernelTimer* kt = nullptr;
+    for (const auto& k : h->ktab)
+        if (!kt || k.total_ms > kt->total_ms) kt = &k;
+    const KernelTimer none{};
+    if (!kt) kt = &none;
+    if (name && name_len) snprintf(name, name_len, "%s", kt->name.c_str());
+    if (avg_ms) *avg_ms = kt->count ? kt->total_ms / kt->count : 0.0;
+    if (count) *count = kt->count;
+    if (bytes_per_launch) *bytes_per_launch = kt->bytes;
+    return ASD_OK;
+}
+
+int asd_kernel_table(const asd_handle* h, char* out, size_t out_len) {
+    if (!h || !out || out_len == 0) return ASD_EINVAL;
+    std::string t;
+    char line[512];
+    for (const auto& k : h->ktab) {
+        snprintf(line, sizeof line, "%s|%.6f|%llu|%.0f\n", k.name.c_str(), k.count ? k.total_ms / k.count : 0.0,
+                 (unsigned long long)k.count, k.bytes);
+        t += line;
     }
-    if (avg_ms) *avg_ms = h->ktimer.count ? h->ktimer.total_ms / h->ktimer.count : 0.0;
-    if (count) *count = h->ktimer.count;
-    if (bytes_per_launch) *bytes_per_launch = h->ktimer.bytes;
+    if (t.size() + 1 > out_len) return ASD_EINVAL;
+    snprintf(out, out_len, "%s", t.c_str());
     return ASD_OK;
 }
 

@@ -749,15 +749,27 @@ cudaError_t build_plane_twiddles(asd_handle* h) {
 }
 
 // M_r -> H_r through the three plane kernels.
+// Algorithmic bytes per launch: the box rows of M_r or H_r (3 components, the z pairs that hold
+// data), the spectrum (3 x (N+1) x m1 x box x float2) read and/or written once, N_k read once.
 cudaError_t launch_lr_planes(asd_handle* h) {
     LongRange& L = h->lr;
     PlaneArgs A = plane_args(L);
     A.err = h->d_err;
     const bool cplx = !(L.ncomp == 6 && L.nk_real);
+    const double rows = 3.0 * A.bx * A.by * 2.0 * A.nz * 4.0;
+    const double spec = 8.0 * (double)plane_spectrum_elems(L);
+    const double nkb = cplx ? 9.0 * 8.0 * L.mesh[0] * L.mesh[1] * (L.mesh[2] / 2 + 1)
+                            : 6.0 * 4.0 * A.nkx * L.mesh[1] * (L.mesh[2] / 2 + 1);
     cudaError_t e;
+    timer_begin(h);
     if ((e = run_zy(L, A, false, h->stream)) != cudaSuccess) return e;
+    timer_end(h, "plane_zy_fwd (z R2C + y FFT)", rows + spec);
+    timer_begin(h);
     if ((e = run_xconv(L, A, cplx, h->stream)) != cudaSuccess) return e;
+    timer_end(h, "plane_x_conv (x FFT, N_k product, inverse x FFT)", 2.0 * spec + nkb);
+    timer_begin(h);
     if ((e = run_zy(L, A, true, h->stream)) != cudaSuccess) return e;
+    timer_end(h, "plane_yz_inv (inverse y FFT + z C2R)", spec + rows);
     h->launches += 3;
     return cudaSuccess;
 }

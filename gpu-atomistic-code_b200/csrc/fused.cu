@@ -382,6 +382,8 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
 }
 
 __global__ void advance_k(uint64_t* step, uint32_t n) { *step += n; }
+// The det field is written at the step the device counter holds (the one-step graph's step).
+__global__ void det_here_k(const uint64_t* step, double* dyn) { dyn[DYN_DET_STEP] = (double)*step; }
 
 template <typename R>
 Vec3<R> v3(R* const p[3]) { return Vec3<R>{{p[0], p[1], p[2]}}; }
@@ -443,26 +445,16 @@ cudaError_t launch_stage_k(asd_handle* hd, const StageArgs<R>& a) {
             opted = smem;
         }
     }
-    if (hd->timing) {
-        if (hd->flush_buf) cudaMemsetAsync(hd->flush_buf, 0, hd->flush_bytes, hd->stream);
-        cudaEventRecord(hd->kev[0], hd->stream);
-    }
+    timer_begin(hd);
     stage_kernel<R, EX, FULL, COMP, K><<<grid, B, smem, hd->stream>>>(hd->sc, hd->sell, hd->dia, a);
     hd->launches += 1;
     if (hd->timing) {
-        cudaEventRecord(hd->kev[1], hd->stream);
-        cudaEventSynchronize(hd->kev[1]);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, hd->kev[0], hd->kev[1]);
-        KernelTimer& kt = hd->ktimer;
-        const double b = stage_bytes<R>(hd, a, COMP);
-        kt.bytes = (kt.bytes * kt.count + b) / (double)(kt.count + 1);
-        kt.total_ms += ms;
-        kt.count += 1;
         const bool typed = (EX == ASD_EXCH_CSR && hd->sell.typed) || (EX == ASD_EXCH_DIA && hd->dia.dtype);
-        kt.name = std::string("stage_kernel<") + (sizeof(R) == 4 ? "float" : "double") + "," +
-                  (EX == ASD_EXCH_CSR ? "SELL32" : EX == ASD_EXCH_DIA ? "DIA" : "NONE") + (typed ? "-typed" : "") +
-                  (FULL ? ",full" : ",diag") + (COMP ? ",comp>" : ">");
+        const std::string name = std::string("stage_kernel<") + (sizeof(R) == 4 ? "float" : "double") + "," +
+                                 (EX == ASD_EXCH_CSR ? "SELL32" : EX == ASD_EXCH_DIA ? "DIA" : "NONE") +
+                                 (typed ? "-typed" : "") + (FULL ? ",full" : ",diag") + (COMP ? ",comp" : "") +
+                                 (K == 1 ? ",predictor>" : K == 2 ? ",corrector>" : K == 3 ? ",rk-stage>" : ",rk-last>");
+        timer_end(hd, name, stage_bytes<R>(hd, a, COMP));
     }
     return cudaGetLastError();
 }
@@ -646,6 +638,12 @@ cudaError_t time_first_stage(asd_handle* h, int warm, int reps, float* ms) {
 cudaError_t launch_fused_step(asd_handle* h, uint32_t rel, bool) {
     if (h->p.precision == ASD_FP32) return fused_step_t<float>(h, rel);
     return fused_step_t<double>(h, rel);
+}
+
+cudaError_t launch_det_here(asd_handle* h) {
+    det_here_k<<<1, 1, 0, h->stream>>>(h->d_step, h->d_dyn);
+    h->launches += 1;
+    return cudaGetLastError();
 }
 
 cudaError_t launch_step_advance(asd_handle* h, uint32_t nsteps) {

@@ -206,20 +206,51 @@ struct asd_handle {
     // CUDA graph of a chunk of FP32 steps
     cudaGraphExec_t graph = nullptr;
     uint32_t graph_steps = 0;
+    cudaGraphExec_t graph1 = nullptr;    // one step (single-step calls)
+    uint64_t graph1_launches = 0;
     int block = 256;
     // timing of the dominant kernel
     bool timing = false;
     void* flush_buf = nullptr;           // written before each timed stage launch (cold L2)
     size_t flush_bytes = 0;
-    asd::KernelTimer ktimer;
+    std::vector<asd::KernelTimer> ktab;  // per kernel (name) of the last asd_time_kernels
     cudaEvent_t kev[2] = {nullptr, nullptr};
 };
+
+namespace asd {
+// Timed launches (asd_time_kernels): before the launch, an optional L2 flush and an event on the
+// handle's stream; after it, the event pair's device time accumulated under `name` with the
+// launch's algorithmic bytes.
+inline void timer_begin(asd_handle* h) {
+    if (!h->timing) return;
+    if (h->flush_buf) cudaMemsetAsync(h->flush_buf, 0, h->flush_bytes, h->stream);
+    cudaEventRecord(h->kev[0], h->stream);
+}
+inline void timer_end(asd_handle* h, const std::string& name, double bytes) {
+    if (!h->timing) return;
+    cudaEventRecord(h->kev[1], h->stream);
+    cudaEventSynchronize(h->kev[1]);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h->kev[0], h->kev[1]);
+    KernelTimer* kt = nullptr;
+    for (auto& k : h->ktab)
+        if (k.name == name) kt = &k;
+    if (!kt) {
+        h->ktab.push_back(KernelTimer{name, 0.0, 0, 0.0});
+        kt = &h->ktab.back();
+    }
+    kt->bytes = (kt->bytes * kt->count + bytes) / (double)(kt->count + 1);
+    kt->total_ms += ms;
+    kt->count += 1;
+}
+}  // namespace asd
 
 namespace asd {
 // launchers implemented in the .cu files; all return cudaError_t of the launch
 cudaError_t launch_plain_step(asd_handle* h, uint64_t t);
 cudaError_t launch_fused_step(asd_handle* h, uint32_t rel, bool in_capture);
 cudaError_t launch_step_advance(asd_handle* h, uint32_t nsteps);
+cudaError_t launch_det_here(asd_handle* h);
 cudaError_t launch_lr_eval_f32(asd_handle* h);
 cudaError_t launch_lr_scatter(asd_handle* h);
 cudaError_t launch_lr_planes(asd_handle* h);

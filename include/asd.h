@@ -263,8 +263,9 @@ int asd_num_sublattices(const asd_handle* h, uint32_t* nsub);
 /* Time nsteps asd_step calls on the device with CUDA events on the handle's stream;
  * *ms = elapsed milliseconds, *launches = kernels this library launched. */
 int asd_time_steps(asd_handle* h, uint64_t nsteps, double* ms, uint64_t* launches);
-/* Advance nsteps with direct (un-graphed) launches, bracketing every fused stage-kernel
- * launch with CUDA events on the handle's stream; results via asd_kernel_stats.
+/* Advance nsteps with direct (un-graphed) launches, bracketing every fused stage-kernel and
+ * long-range plane-kernel launch with CUDA events on the handle's stream; results via
+ * asd_kernel_stats / asd_kernel_table.
  * Measurement aid with no reference counterpart. */
 int asd_time_kernels(asd_handle* h, uint64_t nsteps);
 /* As asd_time_kernels, with a device buffer of flush_bytes written before every timed launch so
@@ -273,10 +274,14 @@ int asd_time_kernels_cold(asd_handle* h, uint64_t nsteps, uint64_t flush_bytes);
 /* Device time of nsteps steps, each preceded by an untimed write of flush_bytes (> L2 size) and
  * bracketed by its own CUDA events; *ms = sum over the steps.  Measurement aid. */
 int asd_time_steps_cold(asd_handle* h, uint64_t nsteps, uint64_t flush_bytes, double* ms, uint64_t* launches);
-/* Per-kernel device time of the fused stage kernel in the last asd_time_kernels:
- * average ms per launch, launch count and algorithmic bytes per launch. */
+/* Device time of the dominant kernel of the last asd_time_kernels (the one with the largest
+ * summed time over its launches): average ms per launch, launch count and algorithmic bytes per
+ * launch.  Measurement aid. */
 int asd_kernel_stats(const asd_handle* h, char* name, size_t name_len, double* avg_ms, uint64_t* count,
                      double* bytes_per_launch);
+/* Every kernel timed in the last asd_time_kernels, one line each: "name|avg_ms|count|bytes\n";
+ * ASD_EINVAL when out_len is too small.  Measurement aid. */
+int asd_kernel_table(const asd_handle* h, char* out, size_t out_len);
 /* Launch shape of the fused stage kernel chosen at create (block size, shared-memory staging of
  * the typed exchange words), with ASD_FLAG_AUTOTUNE the autotuner's timings, and the transform
  * path of the long-range field. */

@@ -1,0 +1,109 @@
+"""Long runs at the sizes and lengths the benchmark configurations state.
+
+* Configuration 0 exactly: simple cubic 16^3 (4,096 spins), periodic, NN exchange in CSR, K1u along
+  z, lambda = 0.1, dt = 1e-16 s, Heun, T = 0, 10^4 steps from uniformly random spins.  The FP64
+  plain form must equal the FP64 oracle bit for bit and stay within 1e-10 of the reference's own
+  CUDA kernels (src/cuint.cu, src/cufields.cu launched in the order of src/cuda.cu:43-258); the
+  fused FP64 form within 1e-8 of the oracle; the FP32 form within 1e-5 after 3,000 steps and
+  1e-4 after 10^4 (its per-step rounding, ~1e-10, grows with the trajectory's sensitivity).
+* The north-star lattice (sc 128x128x64, open, CSR NN exchange + FFT dipole every step), T = 0,
+  against the FP64 plain form: the FP32 form within 1e-5 up to 3,000 steps; after 10^4 steps the
+  fused FP64 form (FP64 state and fields, FP32 dipole transform) within 2e-5 (measured 1.1e-5:
+  the FP32 rounding of N_k and of the transform) and the FP32 form within 1e-3 (measured 2.0e-4).
+  Beside them, the FP64 plain form started from spins perturbed by 1e-15 measures how far the
+  trajectory itself amplifies a difference: it stays below 1e-9 (measured 2.7e-11), so the FP32
+  form's 2e-4 is its own arithmetic (FP32 neighbour spins, fields and torque; the fused FP64
+  form removes 95 % of it), not the dynamics.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import asd_b200 as A
+import asd_lattice as LT
+from helpers import maxdiff
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def run(s, steps, precision, S0, **kw):
+    flags = A.FLAG_COMPENSATED if precision == A.FP32 else 0
+    with A.Handle(A.RunParams(precision=precision, flags=flags, **kw), s) as h:
+        h.set_spins(S0)
+        h.step(steps)
+        return h.get_spins()
+
+
+def test_config0_full_length(gpu):
+    s = LT.sc_ferromagnet(16)
+    S0 = LT.random_spins(s.nspins, 0)
+    o = O.Oracle(s, dt=1e-16)
+    o.set_spins(S0)
+    hs = {k: A.Handle(A.RunParams(precision=p, dt=1e-16, flags=A.FLAG_COMPENSATED if p == A.FP32 else 0), s)
+          for k, p in (("plain", A.FP64_PLAIN), ("fused", A.FP64_FUSED), ("fp32", A.FP32))}
+    rc = O.RefCUDA(s, dt=1e-16) if os.path.exists(O.REF_CUDA_SO) else None
+    try:
+        for h in hs.values():
+            h.set_spins(S0)
+        if rc:
+            rc.set_spins(S0)
+        done = 0
+        for cp in (3000, 10_000):
+            o.step(cp - done)
+            for h in hs.values():
+                h.step(cp - done)
+            if rc:
+                rc.step(cp - done)
+            done = cp
+            ref = o.spins()
+            plain = hs["plain"].get_spins()
+            assert np.array_equal(plain, ref), (cp, maxdiff(plain, ref))
+            ef = maxdiff(hs["fused"].get_spins(), ref)
+            e32 = maxdiff(hs["fp32"].get_spins(), ref)
+            er = maxdiff(plain, rc.spins()) if rc else 0.0
+            print(f"config 0, {cp} steps: fused FP64 {ef:.3e}, FP32 {e32:.3e}, reference CUDA kernels {er:.3e}")
+            assert er <= 1e-10, (cp, er)
+            assert ef <= 1e-8, (cp, ef)
+            if cp == 3000:
+                assert e32 <= 1e-5, (cp, e32)
+            else:
+                assert e32 <= 1e-4, (cp, e32)
+    finally:
+        for h in hs.values():
+            h.close()
+        if rc:
+            rc.close()
+
+
+def test_north_star_accuracy_1e4(gpu):
+    s = LT.sc_ferromagnet((128, 128, 64), pbc=(0, 0, 0), dipole=True)
+    S0 = LT.random_spins(s.nspins, 0)
+    S1 = S0.copy()
+    S1[:, 0] *= 1.0 + 1e-15
+    kw = dict(integrator=A.HEUN, dt=1e-16, update=1)
+    hs = {k: A.Handle(A.RunParams(precision=p, flags=A.FLAG_COMPENSATED if p == A.FP32 else 0, **kw), s)
+          for k, p in (("plain", A.FP64_PLAIN), ("ctrl", A.FP64_PLAIN), ("fused", A.FP64_FUSED), ("fp32", A.FP32))}
+    try:
+        for k, h in hs.items():
+            h.set_spins(S1 if k == "ctrl" else S0)
+        for h in hs.values():
+            h.step(3000)
+        ref = hs["plain"].get_spins()
+        e32 = maxdiff(hs["fp32"].get_spins(), ref)
+        assert e32 <= 1e-5, e32
+        for h in hs.values():
+            h.step(7000)
+        ref = hs["plain"].get_spins()
+        ectrl = maxdiff(hs["ctrl"].get_spins(), ref)
+        efused = maxdiff(hs["fused"].get_spins(), ref)
+        e32b = maxdiff(hs["fp32"].get_spins(), ref)
+        print(f"north star, 10^4 steps: fused FP64 {efused:.3e}, FP32 {e32b:.3e} (3000 steps: {e32:.3e}), "
+              f"FP64 control {ectrl:.3e}")
+        assert ectrl <= 1e-9, ectrl
+        assert efused <= 2e-5, efused
+        assert e32b <= 1e-3, e32b
+    finally:
+        for h in hs.values():
+            h.close()
