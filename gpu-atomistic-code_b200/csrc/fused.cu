@@ -247,7 +247,8 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
         if (a.nz_mode == 1) { a.nz.p[0][i] = lrn[0]; a.nz.p[1][i] = lrn[1]; a.nz.p[2][i] = lrn[2]; }
     }
     bool stage_timeout = false;
-    if ((staged || staged16) && !mbar_wait_bounded(&stage_bar, STAGE_WAIT_POLLS)) {
+    const uint32_t polls = (c.flags & ASD_FLAG_WAIT_TIMEOUT) ? 0u : STAGE_WAIT_POLLS;
+    if ((staged || staged16) && !mbar_wait_bounded(&stage_bar, polls)) {
         // the copy did not land in time: record it and read the words from global memory
         atomicOr(sell.err, ERR_STAGE_TIMEOUT);
         staged = nullptr;      // the global words carry global columns

@@ -71,6 +71,12 @@ extern "C" {
 #define ASD_FLAG_CUFFT_PLANES        (1u << 19) /* fused forms: run the (x, y) passes of the long-range
                                                    transform through cuFFT instead of the library's
                                                    plane kernels (comparison aid) */
+#define ASD_FLAG_WAIT_TIMEOUT           (1u << 20) /* test aid: the device-side waits for bulk copies give
+                                                   up at once and take their time-out path (the stage
+                                                   kernels then read global memory, results unchanged;
+                                                   the x transform leaves its tile, an invalid field);
+                                                   the wait before a block retires keeps its bound;
+                                                   asd_sync reports ASD_ETIMEOUT */
 
 #define ASD_ALL_REPLICAS 0xFFFFFFFFu
 
