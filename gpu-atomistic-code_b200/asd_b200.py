@@ -48,7 +48,7 @@ EXPORTED = [
     "asd_time_kernels_cold", "asd_time_steps_cold", "asd_read_ucf", "asd_read_exch", "asd_read_csr_exch",
     "asd_write_csr_exch", "asd_plan_spin_spans", "asd_set_device_layout", "asd_set_ttm",
     "asd_get_ttm_temperatures", "asd_set_four_spin", "asd_spins_random", "asd_spins_pattern",
-    "asd_kernel_table",
+    "asd_kernel_table", "asd_get_state", "asd_set_state",
 ]
 
 
@@ -136,6 +136,8 @@ def load_library(path: str = LIB_PATH):
         "asd_time_kernels": ([P, C.c_uint64], C.c_int),
         "asd_kernel_stats": ([P, C.c_char_p, C.c_size_t, dp, C.POINTER(C.c_uint64), dp], C.c_int),
         "asd_kernel_table": ([P, C.c_char_p, C.c_size_t], C.c_int),
+        "asd_get_state": ([P, C.c_void_p, C.POINTER(C.c_size_t)], C.c_int),
+        "asd_set_state": ([P, C.c_void_p, C.c_size_t], C.c_int),
         "asd_thermal_normals": ([C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, dp], C.c_int),
         "asd_magnetisation_noalloc": ([C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p],
                                       C.c_int),
@@ -369,6 +371,24 @@ class Handle:
 
     def sync(self):
         _check(load_library().asd_sync(self.h), self.h)
+
+    def get_step(self) -> int:
+        t = C.c_uint64()
+        _check(load_library().asd_get_step(self.h, C.byref(t)), self.h)
+        return t.value
+
+    def get_state(self) -> bytes:
+        """Exact state (spins in the form's storage, step, bath temperatures, TTM) for restart."""
+        lib = load_library()
+        n = C.c_size_t()
+        _check(lib.asd_get_state(self.h, None, C.byref(n)), self.h)
+        buf = C.create_string_buffer(n.value)
+        _check(lib.asd_get_state(self.h, buf, C.byref(n)), self.h)
+        return buf.raw[: n.value]
+
+    def set_state(self, state: bytes):
+        buf = C.create_string_buffer(bytes(state), len(state))
+        _check(load_library().asd_set_state(self.h, buf, len(state)), self.h)
 
     def set_temperature(self, T: float, replica: int = ALL_REPLICAS):
         _check(load_library().asd_set_temperature(self.h, replica, T), self.h)

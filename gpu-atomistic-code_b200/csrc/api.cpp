@@ -1108,6 +1108,113 @@ int asd_set_step(asd_handle* h, uint64_t t) {
     return ASD_OK;
 }
 
+// ---- exact state (checkpoint and restart)
+namespace {
+struct StateHeader {
+    char magic[4];          // "ASDS"
+    uint32_t version;       // 1
+    uint32_t precision, flags_comp, n, nrep, has_ttm, reserved;
+    uint64_t step;
+};
+
+size_t state_bytes(const asd_handle* h) {
+    size_t b = sizeof(StateHeader);
+    const size_t n3 = 3 * (size_t)h->n;
+    if (h->p.precision == ASD_FP32) b += n3 * sizeof(float) * ((h->p.flags & ASD_FLAG_COMPENSATED) ? 2 : 1);
+    else b += n3 * sizeof(double);
+    b += (size_t)h->nrep * (sizeof(double) + sizeof(float));
+    if (h->d_ttm) b += sizeof(TtmDev);
+    return b;
+}
+}  // namespace
+
+int asd_get_state(asd_handle* h, void* buf, size_t* len) {
+    if (!h || !len) return ASD_EINVAL;
+    try {
+        const size_t need = state_bytes(h);
+        if (!buf) { *len = need; return ASD_OK; }
+        REQUIRE(*len >= need, "state buffer too small (asd_get_state with buf = NULL gives the size)");
+        CK(cudaSetDevice(h->device));
+        StateHeader hd{};
+        memcpy(hd.magic, "ASDS", 4);
+        hd.version = 1;
+        hd.precision = h->p.precision;
+        hd.flags_comp = (h->p.flags & ASD_FLAG_COMPENSATED) ? 1 : 0;
+        hd.n = h->n; hd.nrep = h->nrep; hd.has_ttm = h->d_ttm ? 1 : 0;
+        hd.step = h->step;
+        unsigned char* o = static_cast<unsigned char*>(buf);
+        memcpy(o, &hd, sizeof hd);
+        o += sizeof hd;
+        const size_t n = h->n;
+        auto get = [&](const void* d, size_t bytes) {
+            CK(cudaMemcpyAsync(o, d, bytes, cudaMemcpyDeviceToHost, h->stream));
+            o += bytes;
+        };
+        if (h->p.precision == ASD_FP32) {
+            for (int c = 0; c < 3; c++) get(h->sf[c], n * sizeof(float));
+            if (hd.flags_comp)
+                for (int c = 0; c < 3; c++) get(h->sl[c], n * sizeof(float));
+        } else if (h->p.precision == ASD_FP64_FUSED) {
+            for (int c = 0; c < 3; c++) get(h->sd[c], n * sizeof(double));
+        } else {
+            get(h->p_s, 3 * n * sizeof(double));
+        }
+        get(h->d_rep_sqrtT, h->nrep * sizeof(double));
+        get(h->d_rep_sqrtT_f, h->nrep * sizeof(float));
+        if (h->d_ttm) get(h->d_ttm, sizeof(TtmDev));
+        CK(cudaStreamSynchronize(h->stream));
+        *len = need;
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
+int asd_set_state(asd_handle* h, const void* buf, size_t len) {
+    if (!h || !buf) return ASD_EINVAL;
+    try {
+        StateHeader hd{};
+        REQUIRE(len >= sizeof hd, "state too short");
+        memcpy(&hd, buf, sizeof hd);
+        REQUIRE(memcmp(hd.magic, "ASDS", 4) == 0 && hd.version == 1, "not a state of this library");
+        REQUIRE(hd.precision == h->p.precision && hd.n == h->n && hd.nrep == h->nrep &&
+                    hd.flags_comp == ((h->p.flags & ASD_FLAG_COMPENSATED) ? 1u : 0u),
+                "state taken from a handle of another form or lattice");
+        REQUIRE(len == state_bytes(h) + (hd.has_ttm && !h->d_ttm ? sizeof(TtmDev) : 0) -
+                           (!hd.has_ttm && h->d_ttm ? sizeof(TtmDev) : 0),
+                "state size does not match the handle");
+        REQUIRE(!hd.has_ttm || h->d_ttm, "the state carries a two-temperature model: start it (asd_set_ttm) first");
+        CK(cudaSetDevice(h->device));
+        const unsigned char* in = static_cast<const unsigned char*>(buf) + sizeof hd;
+        const size_t n = h->n;
+        auto put = [&](void* d, size_t bytes) {
+            CK(cudaMemcpyAsync(d, in, bytes, cudaMemcpyHostToDevice, h->stream));
+            in += bytes;
+        };
+        if (h->p.precision == ASD_FP32) {
+            for (int c = 0; c < 3; c++) put(h->sf[c], n * sizeof(float));
+            if (hd.flags_comp)
+                for (int c = 0; c < 3; c++) put(h->sl[c], n * sizeof(float));
+        } else if (h->p.precision == ASD_FP64_FUSED) {
+            for (int c = 0; c < 3; c++) put(h->sd[c], n * sizeof(double));
+        } else {
+            put(h->p_s, 3 * n * sizeof(double));
+        }
+        put(h->d_rep_sqrtT, h->nrep * sizeof(double));
+        put(h->d_rep_sqrtT_f, h->nrep * sizeof(float));
+        if (hd.has_ttm) put(h->d_ttm, sizeof(TtmDev));
+        CK(cudaMemcpyAsync(h->d_step, &hd.step, sizeof hd.step, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        h->step = hd.step;
+        // host copies of the bath temperatures follow the device
+        std::vector<double> sq(h->nrep);
+        memcpy(sq.data(), static_cast<const unsigned char*>(buf) + len - (hd.has_ttm ? sizeof(TtmDev) : 0) -
+                              h->nrep * (sizeof(double) + sizeof(float)),
+               h->nrep * sizeof(double));
+        for (uint32_t r = 0; r < h->nrep; r++) h->h_rep_T[r] = sq[r] * sq[r];
+        h->lr_scattered = false;    // the long-range input is formed again from these spins
+    } catch (const Fail& f) { return fail(h, f); }
+    return ASD_OK;
+}
+
 int asd_sync(asd_handle* h) {
     if (!h) return ASD_EINVAL;
     try {

@@ -160,6 +160,17 @@ int asd_get_step(const asd_handle* h, uint64_t* t);
 int asd_set_step(asd_handle* h, uint64_t t);
 int asd_sync(asd_handle* h);
 
+/* Exact state for checkpoint and restart, the binary counterpart of the reference's restart
+ * files (spins::restart_text, src/spins.cpp:342-398, which print the spins as text): the spins in
+ * the form's own storage (FP32 hi+lo pairs, or FP64), the step counter, the replicas' bath
+ * temperatures and the two-temperature model's state.  buf == NULL: *len = the size needed.
+ * Parameters (applied field, site-field ramp, flags) are the caller's and are not included. */
+int asd_get_state(asd_handle* h, void* buf, size_t* len);
+/* Restore a state taken from a handle created with the same parameters and lattice (and the
+ * two-temperature model started when the state carries one): no renormalisation, so the next
+ * steps are bit-identical to those of the run the state was taken from. */
+int asd_set_state(asd_handle* h, const void* buf, size_t len);
+
 /* llg::T (passed per launch, src/cuda.cu:159); replica ASD_ALL_REPLICAS sets all. */
 int asd_set_temperature(asd_handle* h, uint32_t replica, double T);
 /* llg::applied (src/cuda.cu:159). */
