@@ -2,12 +2,11 @@
 // allocation at all: the partial sums live in a fixed file-scope device array.
 //
 // Who needs this: code that cannot call cudaMalloc/cudaFree at the point it
-// wants a magnetisation - a step loop being recorded into a CUDA graph
-// (allocation is not allowed during global-mode stream capture), a host that
-// hands all device memory to its own pool allocator and runs at its limit, or a
-// time-critical loop that must not hit cudaFree's implicit device-wide
-// synchronisation.  asd_magnetisation() on a handle allocates its scratch once
-// at asd_create; this entry point needs neither a handle nor an allocation.
+// wants a magnetisation - a host that hands all device memory to its own pool
+// allocator and runs at its limit, or a time-critical loop that must not hit
+// cudaFree's implicit device-wide synchronisation.  asd_magnetisation() on a
+// handle allocates its scratch once at asd_create; this entry point needs
+// neither a handle nor an allocation.
 #include "../../include/asd.h"
 #include <cuda_runtime.h>
 #include <mutex>
@@ -40,26 +39,36 @@ __device__ __forceinline__ double na_block_sum(double v, double* sm) {
     return r;
 }
 
-// Block b sums the spins of [b*chunk, (b+1)*chunk) per sublattice and writes every
-// slot (b, s) it owns, so nothing left from an earlier call is ever read.
+// Block b sums the spins of [b*chunk, (b+1)*chunk) per sublattice in one pass (register
+// accumulators for NS >= nsub sublattices, each thread in a fixed order) and writes every slot
+// (b, s) it owns, so nothing left from an earlier call is ever read.  Spins whose sublattice
+// id is nsub or more are left out of every sum.
+template <uint32_t NS>
 __global__ void na_partial(const double* __restrict__ s3, uint32_t n, const uint32_t* __restrict__ sub,
                            uint32_t nsub, uint32_t chunk, double* __restrict__ part) {
     __shared__ double sm[32];
     const uint32_t b = blockIdx.x;
     const size_t beg = (size_t)b * chunk;
     const size_t end = beg + chunk < n ? beg + chunk : n;
-    for (uint32_t s = 0; s < nsub; s++) {
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0, cnt = 0.0;
-        for (size_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
-            if ((sub ? sub[i] : 0u) != s) continue;
-            a0 += s3[3 * i]; a1 += s3[3 * i + 1]; a2 += s3[3 * i + 2];
-            cnt += 1.0;
-        }
-        const double t0 = na_block_sum(a0, sm), t1 = na_block_sum(a1, sm), t2 = na_block_sum(a2, sm),
-                     t3 = na_block_sum(cnt, sm);
+    double acc[NS][4];
+#pragma unroll
+    for (uint32_t q = 0; q < NS; q++) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.0;
+    for (size_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+        const uint32_t s = sub ? sub[i] : 0u;
+        const double x = s3[3 * i], y = s3[3 * i + 1], z = s3[3 * i + 2];
+#pragma unroll
+        for (uint32_t q = 0; q < NS; q++)
+            if (q == s) { acc[q][0] += x; acc[q][1] += y; acc[q][2] += z; acc[q][3] += 1.0; }
+    }
+#pragma unroll
+    for (uint32_t q = 0; q < NS; q++) {
+        if (q >= nsub) break;
+        double t[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) t[k] = na_block_sum(acc[q][k], sm);
         if (threadIdx.x == 0) {
-            double* o = part + ((size_t)b * nsub + s) * 4;
-            o[0] = t0; o[1] = t1; o[2] = t2; o[3] = t3;
+            double* o = part + ((size_t)b * nsub + q) * 4;
+            o[0] = t[0]; o[1] = t[1]; o[2] = t[2]; o[3] = t[3];
         }
     }
 }
@@ -102,7 +111,12 @@ extern "C" int asd_magnetisation_noalloc(const double* d_spins, uint32_t nspins,
     const uint32_t chunk = (nspins + nblocks - 1) / nblocks;
     nblocks = (nspins + chunk - 1) / chunk;
     cudaStream_t st = (cudaStream_t)stream;
-    na_partial<<<nblocks, NA_BLOCK, 0, st>>>(d_spins, nspins, d_sublattice, nsub, chunk, (double*)part);
+    double* pp = (double*)part;
+    if (nsub == 1) na_partial<1><<<nblocks, NA_BLOCK, 0, st>>>(d_spins, nspins, d_sublattice, nsub, chunk, pp);
+    else if (nsub == 2) na_partial<2><<<nblocks, NA_BLOCK, 0, st>>>(d_spins, nspins, d_sublattice, nsub, chunk, pp);
+    else if (nsub <= 4) na_partial<4><<<nblocks, NA_BLOCK, 0, st>>>(d_spins, nspins, d_sublattice, nsub, chunk, pp);
+    else if (nsub <= 8) na_partial<8><<<nblocks, NA_BLOCK, 0, st>>>(d_spins, nspins, d_sublattice, nsub, chunk, pp);
+    else na_partial<16><<<nblocks, NA_BLOCK, 0, st>>>(d_spins, nspins, d_sublattice, nsub, chunk, pp);
     na_final<<<1, 64, 0, st>>>(nblocks, nsub, (const double*)part, d_out);
     return cudaGetLastError() == cudaSuccess ? ASD_OK : ASD_ECUDA;
 }

@@ -188,19 +188,22 @@ int asd_set_site_field_pulse(asd_handle* h, double amp, double t0, double sigma)
 /* util::calc_mag method 0 (src/util_mag.cpp:44-65) per replica: out[(r*nsub+s)*3+c], FP64 sums. */
 int asd_magnetisation(asd_handle* h, double* out, size_t out_len);
 /* Sublattice-mean magnetisation of spins that already sit in device memory, without any
- * device allocation.  No counterpart in the reference: it exists for callers that cannot
- * call cudaMalloc/cudaFree where they need the result - inside a CUDA-graph capture, under
- * a pool allocator that owns all device memory, or in a loop that must avoid cudaFree's
- * device-wide synchronisation.
+ * device allocation.  No counterpart in the reference: it exists for callers that cannot call
+ * cudaMalloc/cudaFree where they need the result - a host that hands all device memory to its
+ * own pool allocator and runs at its limit, or a loop that must avoid cudaFree's device-wide
+ * synchronisation.
  *   d_spins: 3*nspins doubles [3i+c] on the current device; d_sublattice: nspins sublattice
- *   indices (< nsub) on the device, or NULL for one sublattice; d_out: nsub*3 doubles on the
- *   device; stream: a cudaStream_t (NULL = legacy default stream).  Work is enqueued on the
- *   stream; the call returns without waiting.
+ *   indices on the device, or NULL for one sublattice (spins whose index is nsub or more are
+ *   left out of every sum); d_out: nsub*3 doubles on the device; stream: a cudaStream_t
+ *   (NULL = legacy default stream).  Work is enqueued on the stream; the call returns without
+ *   waiting.
  * Scratch is a static device array of ASD_NOALLOC_MAX_BLOCKS x ASD_NOALLOC_MAX_SUBLATTICES x 4
  * doubles (1 MiB) that every GPU loading the library keeps until exit; nsub above
  * ASD_NOALLOC_MAX_SUBLATTICES is rejected with ASD_EINVAL.  The first call on a device looks
- * up the array's device address and should come before any stream capture.  All calls share
- * the array: calls that overlap on the GPU (different streams, no ordering) race. */
+ * up the array's device address (kept for the process; a device reset invalidates it, so do
+ * not call this on a device after cudaDeviceReset) and should come before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (different streams, no ordering)
+ * race. */
 #define ASD_NOALLOC_MAX_BLOCKS 2048
 #define ASD_NOALLOC_MAX_SUBLATTICES 16
 int asd_magnetisation_noalloc(const double* d_spins, uint32_t nspins, const uint32_t* d_sublattice, uint32_t nsub,
