@@ -40,12 +40,26 @@ u32p = C.POINTER(C.c_uint32)
 i32p = C.POINTER(C.c_int32)
 
 
+def reference_dir():
+    """The reference tree the checkers compile from: $ASD_REFERENCE_DIR, else the REF default of
+    oracle/Makefile (the build recipe names its location)."""
+    d = os.environ.get("ASD_REFERENCE_DIR")
+    if d:
+        return d
+    with open(os.path.join(HERE, "Makefile")) as f:
+        for line in f:
+            if line.startswith("REF ?="):
+                return line.split("?=", 1)[1].strip()
+    return ""
+
+
 def build():
     """Compile the checkers (the reference targets only where the reference tree exists)."""
     targets = ["liboracle.so"]
-    if os.path.isdir("/root/reference/src"):
+    ref = reference_dir()
+    if ref and os.path.isdir(os.path.join(ref, "src")):
         targets.append("ref")
-    subprocess.run(["make", "-C", HERE] + targets, check=True, capture_output=True)
+    subprocess.run(["make", "-C", HERE, f"REF={ref}"] + targets, check=True, capture_output=True)
 
 
 def _ptr(a, ct):

@@ -10,7 +10,7 @@ import asd_b200 as A
 import asd_lattice as LT
 from oracle import oracle as O
 
-HAVE_REF_BUILDERS = os.path.exists(O.REF_BUILDERS_SO) or os.path.isdir("/root/reference/src")
+HAVE_REF_BUILDERS = os.path.exists(O.REF_BUILDERS_SO) or os.path.isdir(os.path.join(O.reference_dir(), "src"))
 needs_ref = pytest.mark.skipif(not HAVE_REF_BUILDERS, reason="reference builders not built")
 
 
@@ -185,7 +185,7 @@ def test_csr_exch_file_round_trip(tmp_path):
         A.read_csr_exch(p, s.nspins + 1)             # first check of src/exch.cpp:77-81
 
 
-REF_EXAMPLES = "/root/reference/Examples"
+REF_EXAMPLES = os.path.join(O.reference_dir(), "Examples")
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not present")
