@@ -491,7 +491,7 @@ class Handle:
                                                 int(divide_by_3)), self.h)
 
     def set_device_layout(self, layout: int):
-        """EXCH_DIA or EXCH_CSR (SELL-32) for a DIA matrix."""
+        """EXCH_DIA or EXCH_CSR (SELL-32): for a DIA matrix, or a CSR matrix on at most 32 diagonals."""
         _check(load_library().asd_set_device_layout(self.h, layout), self.h)
 
     def set_launch_shape(self, block: int, staging: int):

@@ -252,6 +252,76 @@ void build_sell(asd_handle* h, const std::vector<uint32_t>& xadj, const std::vec
     }
 }
 
+// A CSR matrix whose entries lie on few diagonals (col - row takes at most 32 values, as on a
+// regular lattice) is also held in the typed DIA layout, whose gather forms each column from the
+// row and the diagonal (one id byte per entry instead of a 4-byte word, every load of a warp
+// contiguous); the autotuner picks the faster layout.  Entries of one row on one diagonal are
+// summed.  Builds nothing (returns false) for other matrices, several replicas or the streamed
+// layout.
+bool build_dia_alt(asd_handle* h, const std::vector<uint32_t>& xadj, const std::vector<uint32_t>& adj,
+                   const std::vector<double>& val9) {
+    if (h->nrep != 1 || (h->p.flags & ASD_FLAG_STREAMED_EXCHANGE) || h->p.precision == ASD_FP64_PLAIN) return false;
+    const uint32_t n = h->n;
+    constexpr uint32_t MAXD = 32;
+    std::map<int64_t, uint32_t> offs;
+    for (uint32_t i = 0; i < n; i++)
+        for (uint32_t k = xadj[i]; k < xadj[i + 1]; k++) {
+            offs.emplace((int64_t)adj[k] - (int64_t)i, 0u);
+            if (offs.size() > MAXD) return false;
+        }
+    if (offs.empty()) return false;
+    std::vector<int32_t> off;
+    for (auto& kv : offs) { kv.second = (uint32_t)off.size(); off.push_back((int32_t)kv.first); }
+    const uint32_t nd = (uint32_t)off.size();
+    const bool full = h->full != 0, zz_yy = (h->p.flags & ASD_FLAG_GPU_DZZ_FROM_DYY) != 0;
+    const int nc = full ? 9 : 3;
+    const int qmap[3] = {0, 4, zz_yy ? 4 : 8};
+    TensorTable tt(nc);
+    std::vector<uint8_t> ids((size_t)nd * n, 0);
+    std::array<std::array<double, 9>, MAXD> loc;
+    std::array<bool, MAXD> used;
+    for (uint32_t i = 0; i < n; i++) {
+        used.fill(false);
+        for (uint32_t k = xadj[i]; k < xadj[i + 1]; k++) {
+            const uint32_t d = offs[(int64_t)adj[k] - (int64_t)i];
+            if (!used[d]) { loc[d].fill(0.0); used[d] = true; }
+            for (int q = 0; q < nc; q++) {
+                int src = full ? q : qmap[q];
+                if (full && q == 8 && zz_yy) src = 4;
+                loc[d][q] += val9[9 * (size_t)k + src];
+            }
+        }
+        for (uint32_t d = 0; d < nd; d++) {
+            if (!used[d]) continue;
+            const int64_t t = tt.id(loc[d]);
+            if (t < 0 || t > 255) return false;
+            ids[(size_t)d * n + i] = (uint8_t)t;
+        }
+    }
+    const uint32_t nt = (n + 31) / 32;
+    std::vector<uint32_t> tp(nt + 1, 0), td;
+    for (uint32_t w = 0; w < nt; w++) {
+        const uint32_t r0 = 32 * w, r1 = std::min(n, r0 + 32);
+        for (uint32_t d = 0; d < nd; d++) {
+            bool any = false;
+            for (uint32_t r = r0; r < r1 && !any; r++) any = ids[(size_t)d * n + r] != 0;
+            if (any) td.push_back(d);
+        }
+        tp[w + 1] = (uint32_t)td.size();
+    }
+    DiaDev& m = h->dia;
+    m.ndiag = nd;
+    m.off = dupload(off.data(), off.size());
+    m.dtype = dupload(ids.data(), ids.size());
+    m.ntypes = tt.size();
+    if (h->p.precision == ASD_FP32) { std::vector<float> tf = tt.table<float>(); m.tab_f = dupload(tf.data(), tf.size()); }
+    else { std::vector<double> tdd = tt.table<double>(); m.tab_d = dupload(tdd.data(), tdd.size()); }
+    m.tile_ptr = dupload(tp.data(), tp.size());
+    m.tile_diag = dupload(td.data(), std::max<size_t>(td.size(), 1));
+    h->dia_alt = true;
+    return true;
+}
+
 void setup_lr(asd_handle* h, const asd_system& s, bool plain) {
     LongRange& L = h->lr;
     L.mode = (int)s.lr;
@@ -466,9 +536,11 @@ void autotune(asd_handle* h) {
     struct Cand { uint32_t layout; int B; int mode; };
     static const char* names[3] = {"direct", "words", "words+spins"};
     std::vector<Cand> cs;
-    // DIA input also exists as SELL-32: both device layouts are candidates
+    // DIA input also exists as SELL-32, and a CSR matrix on few diagonals as DIA: both device
+    // layouts are candidates
     std::vector<uint32_t> layouts{h->dexch};
-    if (h->exch == ASD_EXCH_DIA && h->sell.slice_ptr) layouts = {ASD_EXCH_CSR, ASD_EXCH_DIA};
+    if ((h->exch == ASD_EXCH_DIA && h->sell.slice_ptr) || (h->exch == ASD_EXCH_CSR && h->dia_alt))
+        layouts = {ASD_EXCH_CSR, ASD_EXCH_DIA};
     for (uint32_t lay : layouts)
         for (int B : {64, 128, 256}) {
             cs.push_back({lay, B, 0});
@@ -826,8 +898,10 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
                         for (int q = 0; q < (p.integrator == ASD_RK4 ? 3 : 5); q++) h->kd[q][c] = dalloc<double>(n);
                 }
             }
-            if (h->exch == ASD_EXCH_CSR) build_sell(h, xadj, adj, val9);
-            else if (h->exch == ASD_EXCH_DIA) {
+            if (h->exch == ASD_EXCH_CSR) {
+                build_sell(h, xadj, adj, val9);
+                build_dia_alt(h, xadj, adj, val9);
+            } else if (h->exch == ASD_EXCH_DIA) {
                 h->dia.ndiag = s0.ndiag;
                 h->dia.off = dupload(doff.data(), doff.size());
                 const size_t m = (size_t)s0.ndiag * n;
@@ -1259,8 +1333,9 @@ int asd_set_device_layout(asd_handle* h, uint32_t layout) {
     try {
         REQUIRE(layout == ASD_EXCH_CSR || layout == ASD_EXCH_DIA, "layout must be ASD_EXCH_CSR or ASD_EXCH_DIA");
         if (h->p.precision == ASD_FP64_PLAIN) return ASD_OK;
-        REQUIRE(layout == h->exch || (h->exch == ASD_EXCH_DIA && h->sell.slice_ptr),
-                "a CSR matrix has no DIA device layout");
+        REQUIRE(layout == h->exch || (h->exch == ASD_EXCH_DIA && h->sell.slice_ptr) ||
+                    (h->exch == ASD_EXCH_CSR && h->dia_alt),
+                "this CSR matrix has no DIA device layout (more than 32 diagonals, several replicas or streamed)");
         CK(cudaSetDevice(h->device));
         CK(cudaStreamSynchronize(h->stream));
         h->dexch = layout;

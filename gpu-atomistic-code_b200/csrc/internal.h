@@ -151,6 +151,7 @@ struct asd_handle {
     uint32_t n = 0, nrep = 0, nmat = 0, nsub = 1;
     uint32_t exch = ASD_EXCH_NONE, full = 0;
     uint32_t dexch = ASD_EXCH_NONE;      // device layout of the fused kernels (DIA input may run as SELL)
+    bool dia_alt = false;                // a CSR matrix also held as typed DIA (few diagonals)
     uint64_t step = 0;
     uint64_t launches = 0;
     asd::StepConst sc{};

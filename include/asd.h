@@ -311,9 +311,11 @@ int asd_tuning(const asd_handle* h, char* out, size_t out_len);
  * neighbour spins its rows read (each falls back to the lower mode where the layout is not
  * typed SELL or the data do not fit).  Results do not depend on the shape. */
 int asd_set_launch_shape(asd_handle* h, uint32_t block, uint32_t staging);
-/* Device layout of the fused kernels for a DIA matrix: ASD_EXCH_DIA (row-aligned diagonals,
- * the reference's layout) or ASD_EXCH_CSR (the same entries as SELL-32, summed in the same
- * order); the autotuner chooses between them.  Measurement and tuning aid. */
+/* Device layout of the fused kernels: for a DIA matrix ASD_EXCH_DIA (row-aligned diagonals, the
+ * reference's layout) or ASD_EXCH_CSR (the same entries as SELL-32, summed in the same order);
+ * for a CSR matrix of one replica whose entries lie on at most 32 diagonals (a regular lattice)
+ * ASD_EXCH_CSR (SELL-32) or ASD_EXCH_DIA (typed diagonals, summed in ascending diagonal order).
+ * The autotuner chooses between them.  Measurement and tuning aid. */
 int asd_set_device_layout(asd_handle* h, uint32_t layout);
 
 /* The thermal normals the step uses for (seed, stream, step): 3 per spin for spins
