@@ -291,6 +291,8 @@ def run_ours(args):
     if args.launch_shape:
         blk, stg = (int(x) for x in args.launch_shape.split(","))
         h.set_launch_shape(blk, stg)
+    if args.layout:
+        h.set_device_layout(A.EXCH_DIA if args.layout == "dia" else A.EXCH_CSR)
     h.set_spins(S0)
     h.step(args.warmup)
     h.sync()
@@ -465,6 +467,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=8,
                     help="whole-lattice steps of the CPU baseline (north star: ~1.3 s each on 8 cores)")
     ap.add_argument("--err-steps", type=int, default=100)
+    ap.add_argument("--layout", default="", choices=["", "sell", "dia"],
+                    help="device layout of the exchange matrix instead of the autotuner's choice")
     ap.add_argument("--launch-shape", default="",
                     help="block,staging for the fused stage kernel instead of the autotuner's choice "
                          "(staging 0 none, 1 words, 2 words+spins)")
