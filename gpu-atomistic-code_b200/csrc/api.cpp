@@ -67,7 +67,7 @@ void free_all(asd_handle* h) {
         F(h->nzf[c]); F(h->nzd[c]);
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
-    F(h->d_err); F(h->d_aos); F(h->d_rep_of_tile); F(h->d_ttm); F(h->d_q4ptr); F(h->d_q4jkl);
+    F(h->d_err); F(h->d_aos); F(h->d_check); F(h->d_rep_of_tile); F(h->d_ttm); F(h->d_q4ptr); F(h->d_q4jkl);
     F(h->sell.lwords); F(h->sell.span_ptr); F(h->sell.spans);
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
     F(h->sell.typed); F(h->sell.tab_f); F(h->sell.tab_d);
@@ -1095,34 +1095,30 @@ static double* aos_buffer(asd_handle* h) {
     return h->d_aos;
 }
 
+// The spins are uploaded to the staging buffer and checked there (every component finite, every
+// squared length above 1e-24: the first offender is reported, as a host scan would); only a
+// valid array is converted into the state, so a rejected call leaves the state unchanged.
 int asd_set_spins(asd_handle* h, const double* s, size_t n_spins) {
     if (!h) return ASD_EINVAL;
     try {
         REQUIRE(s && n_spins == h->n, "spin array must hold 3*nspins doubles");
-        for (size_t q = 0; q < 3 * n_spins; q++)
-            if (!std::isfinite(s[q])) throw Fail{ASD_ENOTFINITE, "non-finite spin component at index " + std::to_string(q)};
-        for (size_t i = 0; i < n_spins; i++) {
-            const double m = s[3 * i] * s[3 * i] + s[3 * i + 1] * s[3 * i + 1] + s[3 * i + 2] * s[3 * i + 2];
-            REQUIRE(m > 1e-24, "zero-length spin at index " + std::to_string(i));
-        }
         CK(cudaSetDevice(h->device));
-        if (h->p.precision == ASD_FP64_PLAIN) {
-            std::vector<double> v(s, s + 3 * n_spins);
-            for (size_t i = 0; i < n_spins; i++) {
-                const double m = sqrt(v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
-                v[3 * i] /= m; v[3 * i + 1] /= m; v[3 * i + 2] /= m;
-            }
-            CK(cudaMemcpyAsync(h->p_s, v.data(), v.size() * 8, cudaMemcpyHostToDevice, h->stream));
-            CK(cudaStreamSynchronize(h->stream));
-        } else {
-            double* d = aos_buffer(h);
-            cudaError_t e = cudaMemcpyAsync(d, s, 3 * n_spins * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-            if (e == cudaSuccess) e = launch_convert_spins_in(h, d);
-            cudaError_t e2 = cudaStreamSynchronize(h->stream);
-            CK(e);
-            CK(e2);
-            h->lr_scattered = false;
-        }
+        double* d = aos_buffer(h);
+        if (!h->d_check) h->d_check = dalloc<unsigned long long>(2);
+        unsigned long long bad[2] = {0, 0};
+        cudaError_t e = cudaMemcpyAsync(d, s, 3 * n_spins * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+        if (e == cudaSuccess) e = launch_check_spins(h, d, h->d_check);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(bad, h->d_check, sizeof(bad), cudaMemcpyDeviceToHost, h->stream);
+        cudaError_t e2 = cudaStreamSynchronize(h->stream);
+        CK(e);
+        CK(e2);
+        if (bad[0] != ~0ull) throw Fail{ASD_ENOTFINITE, "non-finite spin component at index " + std::to_string(bad[0])};
+        REQUIRE(bad[1] == ~0ull, "zero-length spin at index " + std::to_string(bad[1]));
+        e = launch_convert_spins_in(h, d);
+        e2 = cudaStreamSynchronize(h->stream);
+        CK(e);
+        CK(e2);
+        h->lr_scattered = false;
     } catch (const Fail& f) { return fail(h, f); }
     return ASD_OK;
 }

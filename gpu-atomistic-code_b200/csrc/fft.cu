@@ -467,7 +467,6 @@ cudaError_t launch_lr_eval_f32(asd_handle* h) {
 // Build the FP32 half-spectrum N_k from the FP64 real-space matrix d_nr[9][P] (device).
 cudaError_t build_nk_f32(asd_handle* h, const double* d_nr) {
     LongRange& L = h->lr;
-    const int* n = nullptr; (void)n;
     int dims[3] = {(int)L.mesh[0], (int)L.mesh[1], (int)L.mesh[2]};
     const uint32_t nc = L.ncomp;
     static const int map6[6] = {0, 1, 2, 4, 5, 8};

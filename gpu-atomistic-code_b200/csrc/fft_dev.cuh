@@ -219,14 +219,29 @@ __device__ __forceinline__ void load_twiddles(float2* tw, uint32_t N) {
     }
 }
 
+// Barrier of a group of threads that shares rows of shared memory: the warp when every row's
+// threads lie in one warp (WL), else the block.
+template <bool WL>
+__device__ __forceinline__ void group_sync() {
+    if constexpr (WL) __syncwarp(); else __syncthreads();
+}
+
+// True when fft2pass<N1, N2> keeps every row inside one warp: both passes give row r the
+// threads [r N2, (r + 1) N2), so warp w owns the rows [w 32 / N2, (w + 1) 32 / N2).
+template <int N1, int N2>
+__host__ __device__ constexpr bool rows_warp_local() { return N1 == N2 && 32 % N2 == 0; }
+
 // N = N1 * N2 point DFT of TY rows of shared memory (row pitch ld, natural order in and out, in
 // place), TY * max(N1, N2) <= blockDim.x; N1, N2 <= 16.  The intermediate between the passes is
 // stored with pitch N2 + 1 per m, so ld >= N1 (N2 + 1); with ld = N2 (mod 16) the accesses of
-// both passes are free of bank conflicts.  Ends with a barrier.
+// both passes are free of bank conflicts.  Ends with a barrier: the warp's when
+// rows_warp_local<N1, N2>() (the caller then writes and reads each row from the warp owning
+// it), else the block's.
 template <int N1, int N2, bool INV, bool HIN = false, bool HOUT = false>
 __device__ __forceinline__ void fft2pass(float2* s, uint32_t ld, const float2* tw, uint32_t TY) {
     // HIN: the row's inputs N/2..N are zero (pass 1 reads k < N1/2 only); HOUT: only the outputs
     // 0..N/2 are formed (pass 2 writes q < N2/2 only)
+    constexpr bool WL = rows_warp_local<N1, N2>();
     {
         const uint32_t it = threadIdx.x, r = it / N2, t = it % N2;
         const bool act = it < TY * N2;
@@ -238,12 +253,12 @@ __device__ __forceinline__ void fft2pass(float2* s, uint32_t ld, const float2* t
 #pragma unroll
             for (int m = 1; m < N1; m++) v[m] = INV ? cmulc(v[m], tw[t * m]) : cmul(v[m], tw[t * m]);
         }
-        __syncthreads();
+        group_sync<WL>();
         if (act) {
 #pragma unroll
             for (int m = 0; m < N1; m++) s[r * ld + m * (N2 + 1) + t] = v[m];
         }
-        __syncthreads();
+        group_sync<WL>();
     }
     {
         const uint32_t it = threadIdx.x, r = it / N1, m = it % N1;
@@ -254,12 +269,12 @@ __device__ __forceinline__ void fft2pass(float2* s, uint32_t ld, const float2* t
             for (int t = 0; t < N2; t++) u[t] = s[r * ld + m * (N2 + 1) + t];
             dftp<N2, INV, false, HOUT>(u);
         }
-        __syncthreads();
+        group_sync<WL>();
         if (act) {
 #pragma unroll
             for (int q = 0; q < (HOUT ? N2 / 2 : N2); q++) s[r * ld + m + N1 * q] = u[q];
         }
-        __syncthreads();
+        group_sync<WL>();
     }
 }
 

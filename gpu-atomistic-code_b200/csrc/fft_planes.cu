@@ -97,6 +97,25 @@ __device__ __forceinline__ void copy_tw(float2* dst, const float2* __restrict__ 
     for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) dst[j] = __ldg(src + j);
 }
 
+// Split cluster barrier: arrive (release: this thread's earlier shared-memory accesses, local
+// and remote, are ordered before it) and wait (acquire).  A block that only has to outlive its
+// peers' reads of its shared memory arrives as soon as its own remote reads are done and waits
+// at its end, so the wait does not hold its global stores behind a fence.
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+
+// The threads that handle a set of z rows: with warp-local rows (rows_warp_local<Z1, Z2>) warp w
+// loads, transforms and stores its own RW = 32 / Z2 rows of the TY, else the whole block
+// handles all TY rows.
+template <bool WL, uint32_t TY, uint32_t RW>
+struct RowGroup {
+    uint32_t r0, nr, t, nt;        // first row, rows, thread index in the group, group size
+    __device__ __forceinline__ RowGroup() {
+        if constexpr (WL) { r0 = (threadIdx.x >> 5) * RW; nr = RW; t = threadIdx.x & 31u; nt = 32; }
+        else { r0 = 0; nr = TY; t = threadIdx.x; nt = blockDim.x; }
+    }
+};
+
 // ---------------------------------------------------------------- forward: z (R2C) then y
 template <int Z1, int Z2, int R1, int R2>
 __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const float* __restrict__ mr, float2* __restrict__ yk,
@@ -104,6 +123,8 @@ __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const floa
     using G = ZYGeom<Z1, Z2, R1, R2>;
     constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
     constexpr uint32_t CL = G::CL, HY = G::HY, LDZ = G::LDZ, HK = G::HK, KPB = G::KPB;
+    constexpr bool WLZ = rows_warp_local<Z1, Z2>();    // z rows warp-local
+    constexpr bool WLY = R1 == R2 && 32 % R1 == 0;     // a kz slot's y passes inside one warp
     extern __shared__ __align__(16) float2 sm[];
     cg::cluster_group cl = cg::this_cluster();
     float2* Zs = sm;                                   // [KZ][LDZ]: this block's z rows
@@ -113,24 +134,26 @@ __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const floa
     const uint32_t rank = cl.block_rank();
     const uint32_t xl = blockIdx.x / CL, c = blockIdx.y, x = A.bx0 + xl;
     copy_tw(twz, A.twt, 2 * N + 1 + M1);
+    __syncthreads();
     const float2* row0 = reinterpret_cast<const float2*>(mr + (size_t)c * A.P) + A.zs;
     const float2* ws = twz + N;
     const uint32_t ry0 = rank * HY, ry1 = min(A.by, ry0 + HY);
+    const RowGroup<WLZ, TY, 32 / Z2> g;
     for (uint32_t y0 = ry0; y0 < ry1; y0 += TY) {
-        __syncthreads();
+        group_sync<WLZ>();
         // rows shifted to the z pair zs; pairs n >= N/2 are zero and not read by the pruned pass
-        for (uint32_t e = threadIdx.x; e < TY * (N / 2); e += blockDim.x) {
-            const uint32_t r = e / (N / 2), n = e % (N / 2), yl = y0 + r;
+        for (uint32_t e = g.t; e < g.nr * (N / 2); e += g.nt) {
+            const uint32_t r = g.r0 + e / (N / 2), n = e % (N / 2), yl = y0 + r;
             float2 v = make_float2(0.f, 0.f);
             if (yl < ry1 && n < A.nz) v = row0[((size_t)x * M1 + A.by0 + yl) * N + n];
             scr[r * LD + n] = v;
         }
-        __syncthreads();
+        group_sync<WLZ>();
         fft2pass<Z1, Z2, false, true, false>(scr, LD, twz, TY);
         // X_k and X_{N-k} from the same two values Z_k, Z_{N-k}
         constexpr uint32_t NH = N / 2 + 1;
-        for (uint32_t e = threadIdx.x; e < NH * TY; e += blockDim.x) {
-            const uint32_t r = e / NH, k = e % NH, yl = y0 + r;
+        for (uint32_t e = g.t; e < NH * g.nr; e += g.nt) {
+            const uint32_t r = g.r0 + e / NH, k = e % NH, yl = y0 + r;
             if (yl >= ry1) continue;
             const float2 zk = scr[r * LD + (k & (N - 1))], zm = scr[r * LD + ((N - k) & (N - 1))];
             float2* zc = Zs + (yl - ry0);
@@ -170,7 +193,10 @@ __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const floa
                 for (int m = 0; m < R1; m++) scr[(kzl * R1 + m) * (R2 + 1) + t] = v[m];
             }
         }
-        __syncthreads();
+        // the last round has read every peer row this block needs: arrive on the cluster
+        // barrier whose wait ends the kernel
+        if (s0 + A.kzb >= s_hi) cluster_arrive();
+        group_sync<WLY>();
         const bool packed = s0 == 0;                   // block-uniform: slot 0 is in this round
         {
             const uint32_t kzl = threadIdx.x / R1, m = threadIdx.x % R1, sl = s0 + kzl;
@@ -189,16 +215,18 @@ __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const floa
             }
         }
         if (packed) {
-            __syncthreads();
-            for (uint32_t ky = threadIdx.x; ky < M1; ky += blockDim.x) {
-                const float2 a = cpk[ky], b = cpk[(M1 - ky) & (M1 - 1)];
-                yk[yk_index(A, KZ, c, 0, xl, ky)] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
-                yk[yk_index(A, KZ, c, N, xl, ky)] = make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x));
-            }
+            // slot 0's pass-2 threads are the first R1 of the block: warp 0 (WLY) splits C
+            group_sync<WLY>();
+            if (!WLY || threadIdx.x < 32)
+                for (uint32_t ky = threadIdx.x; ky < M1; ky += WLY ? 32u : blockDim.x) {
+                    const float2 a = cpk[ky], b = cpk[(M1 - ky) & (M1 - 1)];
+                    yk[yk_index(A, KZ, c, 0, xl, ky)] = make_float2(0.5f * (a.x + b.x), 0.5f * (a.y - b.y));
+                    yk[yk_index(A, KZ, c, N, xl, ky)] = make_float2(0.5f * (a.y + b.y), -0.5f * (a.x - b.x));
+                }
         }
-        __syncthreads();
+        group_sync<WLY>();
     }
-    cl.sync();                                         // no block retires while a peer reads its Zs
+    cluster_wait();                                    // no block retires while a peer reads its Zs
 }
 
 // ---------------------------------------------------------------- x, N_k product, inverse x
@@ -238,9 +266,10 @@ __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __
     }
     copy_tw(twx, A.twt + A.twx_off, M0);
     __syncthreads();
-    if (!mbar_wait_bounded(&bar, A.wait_once ? 0u : STAGE_WAIT_POLLS)) {
-        // the copies did not land in time: flag it, leave this tile untransformed, and retire
-        // only after the copies into shared memory have finished (bounded again)
+    if (__syncthreads_or(!mbar_wait_bounded(&bar, A.wait_once ? 0u : STAGE_WAIT_POLLS))) {
+        // the copies did not land in time for some thread: the whole block flags it, leaves this
+        // tile untransformed, and retires only after the copies into shared memory have finished
+        // (bounded again)
         if (tid == 0) atomicOr(A.err, ERR_FFT_TIMEOUT);
         mbar_wait_bounded(&bar, STAGE_WAIT_POLLS);
         return;
@@ -345,6 +374,8 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
     using G = ZYGeom<Z1, Z2, R1, R2>;
     constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
     constexpr uint32_t CL = G::CL, HY = G::HY, LDZ = G::LDZ, HK = G::HK, KPB = G::KPB;
+    constexpr bool WLZ = rows_warp_local<Z1, Z2>();
+    constexpr bool WLY = R1 == R2 && 32 % R1 == 0;
     extern __shared__ __align__(16) float2 sm[];
     cg::cluster_group cl = cg::this_cluster();
     float2* Zs = sm;
@@ -383,7 +414,7 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
                     scr[(kzl * R1 + m) * (R2 + 1) + t] = t ? cmulc(u[t], twy[t * m]) : u[t];
             }
         }
-        __syncthreads();
+        group_sync<WLY>();
         {
             const uint32_t kzl = threadIdx.x / R2, t = threadIdx.x % R2, sl = s0 + kzl;
             if (kzl < A.kzb && sl < s_hi) {
@@ -407,35 +438,36 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
                 }
             }
         }
-        __syncthreads();
+        group_sync<WLY>();
     }
     cl.sync();                                         // every row of every block's Zs is written
     const float2* ws = twz + N;
     float2* out0 = reinterpret_cast<float2*>(hr + (size_t)c * A.P) + A.zs;
     const uint32_t ry0 = rank * HY, ry1 = min(A.by, ry0 + HY);
+    const RowGroup<WLZ, TY, 32 / Z2> g;
     for (uint32_t y0 = ry0; y0 < ry1; y0 += TY) {
-        for (uint32_t e = threadIdx.x; e < KZ * TY; e += blockDim.x) {
-            const uint32_t r = e / KZ, k = e % KZ, yl = y0 + r;
+        for (uint32_t e = g.t; e < KZ * g.nr; e += g.nt) {
+            const uint32_t r = g.r0 + e / KZ, k = e % KZ, yl = y0 + r;
             scr[r * LD + k] = yl < ry1 ? Zs[k * LDZ + (yl - ry0)] : make_float2(0.f, 0.f);
         }
-        __syncthreads();
+        group_sync<WLZ>();
         // pairwise in place: thread (r, k) for k in [0, N/2] writes Z'_k and Z'_{N-k}
         constexpr uint32_t half = N / 2, nh = half + 1;
-        for (uint32_t e = threadIdx.x; e < TY * nh; e += blockDim.x) {
-            const uint32_t r = e / nh, k = e % nh;
+        for (uint32_t e = g.t; e < g.nr * nh; e += g.nt) {
+            const uint32_t r = g.r0 + e / nh, k = e % nh;
             const float2 xk = scr[r * LD + k], xm = scr[r * LD + (N - k)];
             const float2 zk = c2r_pre(xk, xm, ws[k]);
             if (k != 0 && k != half) scr[r * LD + (N - k)] = c2r_pre(xm, xk, ws[N - k]);
             scr[r * LD + k] = zk;
         }
-        __syncthreads();
+        group_sync<WLZ>();
         fft2pass<Z1, Z2, true, false, true>(scr, LD, twz, TY);   // pairs n < N/2 only
-        for (uint32_t e = threadIdx.x; e < TY * (N / 2); e += blockDim.x) {
-            const uint32_t r = e / (N / 2), n = e % (N / 2), yl = y0 + r;
+        for (uint32_t e = g.t; e < g.nr * (N / 2); e += g.nt) {
+            const uint32_t r = g.r0 + e / (N / 2), n = e % (N / 2), yl = y0 + r;
             if (yl >= ry1 || n >= A.nz) continue;
             out0[((size_t)x * M1 + A.by0 + yl) * N + n] = scr[r * LD + n];
         }
-        __syncthreads();
+        group_sync<WLZ>();
     }
 }
 
@@ -561,15 +593,9 @@ size_t xconv_smem(const PlaneArgs& A, bool cplx) {
     return ys + ns + sizeof(float2) * ((size_t)r1 * (r2 * PT + 8) + A.m0);
 }
 
-// Raise a kernel's dynamic shared-memory limit once per instantiation (and again only when a
-// larger size is asked for); the device is the one of the process's first plane launch.
 template <typename K>
 cudaError_t set_smem(K kern, size_t bytes) {
-    static size_t opted = 48 * 1024;
-    if (bytes <= opted) return cudaSuccess;
-    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    if (e == cudaSuccess) opted = bytes;
-    return e;
+    return raise_smem_limit(reinterpret_cast<const void*>(kern), bytes);
 }
 
 // A launch with thread-block clusters of `cl` blocks along x.

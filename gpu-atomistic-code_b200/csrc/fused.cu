@@ -437,14 +437,9 @@ cudaError_t launch_stage_k(asd_handle* hd, const StageArgs<R>& a) {
         if (hd->sell.stage == 2) smem += 3 * sizeof(R) * (size_t)hd->sell.spin_slots;
     }
     if (EX == ASD_EXCH_DIA && hd->dia.dtype) smem = sizeof(R) * table_stride<FULL>() *hd->dia.ntypes;
-    if (smem > 48 * 1024) {
-        static size_t opted = 48 * 1024;   // per instantiation: raise the dynamic shared-memory cap once
-        if (smem > opted) {
-            const cudaError_t e = cudaFuncSetAttribute(stage_kernel<R, EX, FULL, COMP, K>,
-                                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
-            opted = smem;
-        }
+    {
+        const cudaError_t e = raise_smem_limit(reinterpret_cast<const void*>(stage_kernel<R, EX, FULL, COMP, K>), smem);
+        if (e != cudaSuccess) return e;
     }
     timer_begin(hd);
     stage_kernel<R, EX, FULL, COMP, K><<<grid, B, smem, hd->stream>>>(hd->sc, hd->sell, hd->dia, a);

@@ -191,6 +191,7 @@ struct asd_handle {
     std::vector<uint32_t> h_words;       // typed SELL words (host copy, for the local words)
     uint32_t* d_err = nullptr;           // device error bits (staging wait timeouts)
     double* d_aos = nullptr;             // [3N] staging buffer of the spin / field transfers
+    unsigned long long* d_check = nullptr; // [2] first non-finite component, first zero-length spin
     uint32_t* d_rep_of_tile = nullptr;   // replica of each 32-spin tile's first spin
     asd::TtmDev* d_ttm = nullptr;        // two-temperature model (null: off)
     uint32_t* d_q4ptr = nullptr;         // four-spin quartet offsets [N+1]
@@ -280,6 +281,10 @@ cudaError_t launch_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step
 cudaError_t launch_thermal_normals_f(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, float* d_out,
                                      cudaStream_t st);
 cudaError_t launch_convert_spins_in(asd_handle* h, const double* d_aos);
+// Raise a kernel's dynamic shared-memory limit on the current device to at least `bytes`,
+// calling cudaFuncSetAttribute only when this (device, kernel) has not been raised that far.
+cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
+cudaError_t launch_check_spins(asd_handle* h, const double* d_aos, unsigned long long* d_check);
 cudaError_t launch_convert_out(asd_handle* h, int what, double* d_aos);
 cudaError_t build_nk_f32(asd_handle* h, const double* d_nr);
 cudaError_t permute_nk_pruned(asd_handle* h);

@@ -2,6 +2,8 @@
 // field-only evaluation behind asd_get_field.
 #include "gather.cuh"
 #include <algorithm>
+#include <map>
+#include <mutex>
 
 namespace asd {
 namespace {
@@ -134,6 +136,33 @@ __global__ void spins_in_k(uint32_t n, const double* __restrict__ aos, R* __rest
     const R hx = (R)v[0], hy = (R)v[1], hz = (R)v[2];
     x[i] = hx; y[i] = hy; z[i] = hz;
     if (lx) { lx[i] = (float)(v[0] - (double)hx); ly[i] = (float)(v[1] - (double)hy); lz[i] = (float)(v[2] - (double)hz); }
+}
+
+// Input checks of a spin array (AoS doubles), as the host-side checks they replace: bad[0] =
+// the first non-finite component, bad[1] = the first spin of squared length <= 1e-24 (both
+// ~0 when none; the caller sets them to ~0 first).  The squared length is formed without
+// contraction, as the host's scalar code forms it.
+__global__ void spins_check_k(uint32_t n, const double* __restrict__ aos, unsigned long long* bad) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = aos[3 * (size_t)i], y = aos[3 * (size_t)i + 1], z = aos[3 * (size_t)i + 2];
+    const double v[3] = {x, y, z};
+    for (int c = 0; c < 3; c++)
+        if (!isfinite(v[c])) { atomicMin(bad, 3ull * i + c); break; }
+    const double m = __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+    if (!(m > 1e-24)) atomicMin(bad + 1, (unsigned long long)i);
+}
+
+// FP64 plain form: S / |S| with the host's operations in the host's order (IEEE square root and
+// division, no contraction), into the plain form's AoS state.
+__global__ void spins_in_plain_k(uint32_t n, const double* __restrict__ aos, double* __restrict__ s) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = aos[3 * (size_t)i], y = aos[3 * (size_t)i + 1], z = aos[3 * (size_t)i + 2];
+    const double m = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z)));
+    s[3 * (size_t)i] = __ddiv_rn(x, m);
+    s[3 * (size_t)i + 1] = __ddiv_rn(y, m);
+    s[3 * (size_t)i + 2] = __ddiv_rn(z, m);
 }
 
 template <typename R>
@@ -347,9 +376,34 @@ cudaError_t launch_magnetisation(asd_handle* h) {
     return cudaGetLastError();
 }
 
+cudaError_t raise_smem_limit(const void* kernel, size_t bytes) {
+    if (bytes <= 48 * 1024) return cudaSuccess;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> raised;
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& have = raised[{dev, kernel}];
+    if (bytes <= have) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess) have = bytes;
+    return e;
+}
+
+cudaError_t launch_check_spins(asd_handle* h, const double* d_aos, unsigned long long* d_check) {
+    cudaError_t e = cudaMemsetAsync(d_check, 0xff, 2 * sizeof(unsigned long long), h->stream);
+    if (e != cudaSuccess) return e;
+    spins_check_k<<<nb(h->n, 256), 256, 0, h->stream>>>(h->n, d_aos, d_check);
+    h->launches += 1;
+    return cudaGetLastError();
+}
+
 cudaError_t launch_convert_spins_in(asd_handle* h, const double* d_aos) {
     const unsigned g = nb(h->n, 256);
-    if (h->p.precision == ASD_FP32) {
+    if (h->p.precision == ASD_FP64_PLAIN) {
+        spins_in_plain_k<<<g, 256, 0, h->stream>>>(h->n, d_aos, h->p_s);
+    } else if (h->p.precision == ASD_FP32) {
         const bool comp = (h->p.flags & ASD_FLAG_COMPENSATED) != 0;
         spins_in_k<float><<<g, 256, 0, h->stream>>>(h->n, d_aos, h->sf[0], h->sf[1], h->sf[2], comp ? h->sl[0] : nullptr,
                                                      comp ? h->sl[1] : nullptr, comp ? h->sl[2] : nullptr);

@@ -134,3 +134,17 @@ def test_planes_north_star_lattice_against_fft_restatement(gpu):
     assert maxdiff(d, ref) <= 1e-8, maxdiff(d, ref)
     p, _ = run(s, 10, A.FP64_PLAIN, S0=S0)
     assert maxdiff(p, ref) <= 1e-10, maxdiff(p, ref)
+
+
+def test_planes_shared_memory_limit_per_kernel(gpu):
+    """Two x-pass kernels of one signature in one process, the larger first: a general N_k on
+    mesh x 256 (191 KB of shared memory per block), then on mesh x 128 (96 KB).  Each kernel
+    gets its own raised shared-memory limit, whatever the order of the handles."""
+    rng = np.random.default_rng(7)
+    for L in ((128, 4, 4), (64, 4, 4)):
+        s = LT.sc_ferromagnet(L, pbc=(0, 0, 0), dipole=True)
+        s.nr = s.nr + rng.uniform(-0.05, 0.05, s.nr.shape) * np.abs(s.nr).max()
+        o = oracle(s, 10)
+        g, tune = run(s, 10, A.FP32, A.FLAG_COMPENSATED)
+        assert PLANES in tune, tune
+        assert maxdiff(g, o) <= 1e-5, (L, maxdiff(g, o))
