@@ -110,17 +110,19 @@ __constant__ double FRK5C[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0,
 __constant__ double FRK4C[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
 
 // Register caps of the FP32 kernels, chosen from ptxas reports so that none spills: 6 blocks
-// of 256 per SM (40 registers) for the full-tensor SELL and field-only kernels, 5 (48) for the
-// rest; the FP64 kernels keep the default cap.
-template <typename R, int EX, bool FULL>
+// of 256 per SM (40 registers) for the full-tensor SELL kernels but their RK stages before the
+// last, and for the field-only kernels; 5 (48) for the rest; the FP64 kernels keep the default
+// cap.
+template <typename R, int EX, bool FULL, int K>
 struct MinBlocks {
-    static constexpr int value = sizeof(R) != 4 ? 1 : ((EX == ASD_EXCH_CSR && FULL) || EX == ASD_EXCH_NONE) ? 6 : 5;
+    static constexpr int value =
+        sizeof(R) != 4 ? 1 : ((EX == ASD_EXCH_CSR && FULL && K != 3) || EX == ASD_EXCH_NONE) ? 6 : 5;
 };
 
 // K: the stage kind at compile time (1 Heun predictor, 2 Heun corrector, 3 RK stage before the
 // last, 4 last RK stage); a.kind still carries the RK stage index.
 template <typename R, int EX, bool FULL, bool COMP, int K>
-__global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
+__global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL, K>::value)
     stage_kernel(const StepConst c, const SellDev sell, const DiaDev dia, const StageArgs<R> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t stage_bar;
@@ -142,11 +144,15 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
     uint32_t wbase = 0;
     if constexpr (EX == ASD_EXCH_CSR) {
         if (sell.typed) {
+            // the tensor table: with staging, one more bulk copy on the staging barrier; else a
+            // block-wide load
+            bool tab_staged = false;
+            const uint32_t tab_bytes = (uint32_t)sizeof(R) * table_stride<FULL>() * sell.ntypes;
             if (sell.stage) {
                 // this block's slices are contiguous in the SELL stream: one bulk copy into
                 // shared memory behind the tensor table; with stage 2 also one copy per
                 // (neighbour-spin span, component); all overlap the noise draw below
-                const uint32_t tb = (uint32_t)(sizeof(R) * table_stride<FULL>() * sell.ntypes + 15u) & ~15u;
+                const uint32_t tb = (tab_bytes + 15u) & ~15u;
                 const uint32_t spb = blockDim.x >> 5;
                 const uint32_t s0 = blockIdx.x * spb, s1 = min(s0 + spb, sell.nslices);
                 wbase = __ldg(sell.slice_ptr + s0);
@@ -167,17 +173,19 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
                     __syncthreads();
                     if (threadIdx.x < 32) {
                         if (threadIdx.x == 0) {
-                            uint32_t tx = bytes16;
+                            uint32_t tx = bytes16 + tab_bytes;
                             for (uint32_t q = 0; q < nsp; q++) tx += 3u * sell.spans[sp0 + q].y * (uint32_t)sizeof(R);
                             mbar_arrive_expect_tx(&stage_bar, tx);
                         }
                         __syncwarp();
-                        for (uint32_t k = threadIdx.x; k < 1 + 3 * nsp; k += 32) {
+                        for (uint32_t k = threadIdx.x; k < 2 + 3 * nsp; k += 32) {
                             if (k == 0) {
                                 bulk_copy_stream(wbuf, sell.lwords16 + wbase, bytes16, &stage_bar);
+                            } else if (k == 1) {
+                                bulk_copy(tab, table_of<R>(sell), tab_bytes, &stage_bar);
                             } else {
-                                const uint4 sp = sell.spans[sp0 + (k - 1) / 3];
-                                const uint32_t c = (k - 1) % 3;
+                                const uint4 sp = sell.spans[sp0 + (k - 2) / 3];
+                                const uint32_t c = (k - 2) % 3;
                                 bulk_copy(sbuf + c * sell.spin_slots + sp.z, a.src.p[c] + sp.x,
                                           sp.y * (uint32_t)sizeof(R), &stage_bar);
                             }
@@ -185,6 +193,7 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
                     }
                     staged16 = wbuf;
                     sspin = sbuf;
+                    tab_staged = true;
                 } else if (!w16 && bytes) {
                     uint32_t* wbuf = reinterpret_cast<uint32_t*>(smem_raw + tb);
                     R* sbuf = reinterpret_cast<R*>(smem_raw + tb + 4u * sell.stage_words);
@@ -192,17 +201,19 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
                     __syncthreads();
                     if (threadIdx.x < 32) {
                         if (threadIdx.x == 0) {
-                            uint32_t tx = bytes;
+                            uint32_t tx = bytes + tab_bytes;
                             for (uint32_t q = 0; q < nsp; q++) tx += 3u * sell.spans[sp0 + q].y * (uint32_t)sizeof(R);
                             mbar_arrive_expect_tx(&stage_bar, tx);
                         }
                         __syncwarp();
-                        for (uint32_t k = threadIdx.x; k < 1 + 3 * nsp; k += 32) {
+                        for (uint32_t k = threadIdx.x; k < 2 + 3 * nsp; k += 32) {
                             if (k == 0) {
                                 bulk_copy_stream(wbuf, (nsp ? sell.lwords : sell.typed) + wbase, bytes, &stage_bar);
+                            } else if (k == 1) {
+                                bulk_copy(tab, table_of<R>(sell), tab_bytes, &stage_bar);
                             } else {
-                                const uint4 sp = sell.spans[sp0 + (k - 1) / 3];
-                                const uint32_t c = (k - 1) % 3;
+                                const uint4 sp = sell.spans[sp0 + (k - 2) / 3];
+                                const uint32_t c = (k - 2) % 3;
                                 bulk_copy(sbuf + c * sell.spin_slots + sp.z, a.src.p[c] + sp.x,
                                           sp.y * (uint32_t)sizeof(R), &stage_bar);
                             }
@@ -210,9 +221,10 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
                     }
                     staged = wbuf;
                     if (nsp) sspin = sbuf;
+                    tab_staged = true;
                 }
             }
-            load_table<R>(table_of<R>(sell), table_stride<FULL>() * sell.ntypes, tab);
+            if (!tab_staged) load_table<R>(table_of<R>(sell), table_stride<FULL>() * sell.ntypes, tab);
         }
     }
     if constexpr (EX == ASD_EXCH_DIA) {
@@ -246,14 +258,30 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
         }
         if (a.nz_mode == 1) { a.nz.p[0][i] = lrn[0]; a.nz.p[1][i] = lrn[1]; a.nz.p[2][i] = lrn[2]; }
     }
+    // the long-range field at this site: with diagonal tensors it is loaded before the staging
+    // wait, so that its two dependent loads (mesh index, field) overlap the copies and the
+    // gather; the full-tensor kernels have no registers to spare and load it after the gather
+    uint32_t midx = 0;
+    float hl[3] = {0.f, 0.f, 0.f};
+    auto load_lr = [&]() {
+        if (a.lr.hr || a.lr.mr) midx = __ldg(a.lr.idx + i);
+        if (a.lr.hr) {
+            hl[0] = __ldg(a.lr.hr + midx);
+            hl[1] = __ldg(a.lr.hr + a.lr.P + midx);
+            hl[2] = __ldg(a.lr.hr + 2 * a.lr.P + midx);
+        }
+    };
+    if constexpr (!FULL) load_lr();
     bool stage_timeout = false;
     const uint32_t polls = (c.flags & ASD_FLAG_WAIT_TIMEOUT) ? 0u : STAGE_WAIT_POLLS;
     if ((staged || staged16) && !mbar_wait_bounded(&stage_bar, polls)) {
-        // the copy did not land in time: record it and read the words from global memory
+        // the copy did not land in time: record it and read the words and the table from
+        // global memory
         atomicOr(sell.err, ERR_STAGE_TIMEOUT);
         staged = nullptr;      // the global words carry global columns
         staged16 = nullptr;
         sspin = nullptr;
+        tab = const_cast<R*>(table_of<R>(sell));
         stage_timeout = true;
     }
     R h[3] = {R(0), R(0), R(0)};
@@ -264,12 +292,11 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL>::value)
         four_spin<R>(c, i, [&](uint32_t j, R v[3]) { v[0] = a.src.p[0][j]; v[1] = a.src.p[1][j]; v[2] = a.src.p[2][j]; }, h4);
         h[0] += h4[0]; h[1] += h4[1]; h[2] += h4[2];
     }
-    uint32_t midx = 0;
-    if (a.lr.hr || a.lr.mr) midx = __ldg(a.lr.idx + i);
+    if constexpr (FULL) load_lr();
     if (a.lr.hr) {
-        h[0] += (R)(__ldg(a.lr.hr + midx) * a.lr.inv_p);
-        h[1] += (R)(__ldg(a.lr.hr + a.lr.P + midx) * a.lr.inv_p);
-        h[2] += (R)(__ldg(a.lr.hr + 2 * a.lr.P + midx) * a.lr.inv_p);
+        h[0] += (R)(hl[0] * a.lr.inv_p);
+        h[1] += (R)(hl[1] * a.lr.inv_p);
+        h[2] += (R)(hl[2] * a.lr.inv_p);
     }
     const double* dyn = c.dyn;
     const R* dynr;
