@@ -32,6 +32,7 @@ FLAG_AUTOTUNE = 1 << 17
 FLAG_STREAMED_EXCHANGE = 1 << 18
 FLAG_CUFFT_PLANES = 1 << 19
 FLAG_WAIT_TIMEOUT = 1 << 20
+FLAG_SERIAL_LAUNCH = 1 << 21
 ALL_REPLICAS = 0xFFFFFFFF
 
 MUB, KB, GYRO = 9.27e-24, 1.38e-23, 1.76e11  # reference constants (src/llg.cpp:25)

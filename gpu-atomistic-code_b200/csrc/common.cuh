@@ -81,6 +81,14 @@ __device__ __forceinline__ double site_scale_d(const double* dyn, uint64_t t, do
     return sc;
 }
 
+// Programmatic dependent launch, at the top of every step kernel: wait until the previous
+// kernel of the stream has completed and its memory is visible (a no-op for a kernel launched
+// without the attribute), then let the next kernel's blocks launch (they wait the same way).
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 __device__ __forceinline__ uint32_t atom_of(const StepConst& c, uint32_t i) {
     return c.atom ? c.atom[i] : (c.nmat == 1 ? 0u : i % c.nmat);
 }

@@ -68,6 +68,23 @@ __device__ __forceinline__ size_t yk_index(const PlaneArgs& A, uint32_t Kz, uint
     return ((((size_t)c * Kz + kz) * A.ntile + (ky / PT)) * A.bx + x) * PT + (ky % PT);
 }
 
+// The elements ky = m + R1 q (q < R2) of one (c, kz, x) column that y-pass thread m touches, as a
+// pointer and a per-q stride: with R1 a multiple of PT, ky / PT = m / PT + q R1 / PT and
+// ky % PT = m % PT, so the column needs one multiply-add per element instead of the full index.
+template <int R1>
+struct YkCol {
+    static_assert(R1 % PT == 0, "the y transform's first factor is a multiple of the ky tile");
+    float2* p;
+    uint32_t qs;
+    __device__ __forceinline__ YkCol(float2* yk, const PlaneArgs& A, uint32_t Kz, uint32_t c, uint32_t kz, uint32_t x,
+                                     uint32_t m) {
+        const uint32_t tile = A.bx * PT;              // float2 per ky tile of one (c, kz)
+        p = yk + ((size_t)c * Kz + kz) * A.ntile * tile + (size_t)x * PT + (m / PT) * tile + (m % PT);
+        qs = (R1 / PT) * tile;
+    }
+    __device__ __forceinline__ float2& operator[](uint32_t q) const { return p[q * qs]; }
+};
+
 // Compile-time geometry of the z/y kernels: z rows of N = Z1 Z2 complex points (mesh z = 2N),
 // y transforms of M1 = R1 R2 points.  A (component, box row x) is shared by a cluster of CL
 // blocks: block `rank` transforms the z rows y in [rank HY, rank HY + HY) (the box's y extent
@@ -120,6 +137,7 @@ struct RowGroup {
 template <int Z1, int Z2, int R1, int R2>
 __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const float* __restrict__ mr, float2* __restrict__ yk,
                                                        const PlaneArgs A) {
+    pdl_enter();
     using G = ZYGeom<Z1, Z2, R1, R2>;
     constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
     constexpr uint32_t CL = G::CL, HY = G::HY, LDZ = G::LDZ, HK = G::HK, KPB = G::KPB;
@@ -135,7 +153,8 @@ __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const floa
     const uint32_t xl = blockIdx.x / CL, c = blockIdx.y, x = A.bx0 + xl;
     copy_tw(twz, A.twt, 2 * N + 1 + M1);
     __syncthreads();
-    const float2* row0 = reinterpret_cast<const float2*>(mr + (size_t)c * A.P) + A.zs;
+    // the box row x of component c from its y = by0 row on: pair n of row yl at rowx[yl N + n]
+    const float2* rowx = reinterpret_cast<const float2*>(mr + (size_t)c * A.P) + A.zs + ((size_t)x * M1 + A.by0) * N;
     const float2* ws = twz + N;
     const uint32_t ry0 = rank * HY, ry1 = min(A.by, ry0 + HY);
     const RowGroup<WLZ, TY, 32 / Z2> g;
@@ -145,20 +164,29 @@ __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const floa
         for (uint32_t e = g.t; e < g.nr * (N / 2); e += g.nt) {
             const uint32_t r = g.r0 + e / (N / 2), n = e % (N / 2), yl = y0 + r;
             float2 v = make_float2(0.f, 0.f);
-            if (yl < ry1 && n < A.nz) v = row0[((size_t)x * M1 + A.by0 + yl) * N + n];
+            if (yl < ry1 && n < A.nz) v = rowx[yl * N + n];
             scr[r * LD + n] = v;
         }
         group_sync<WLZ>();
         fft2pass<Z1, Z2, false, true, false>(scr, LD, twz, TY);
         // X_k and X_{N-k} from the same two values Z_k, Z_{N-k}
         constexpr uint32_t NH = N / 2 + 1;
-        for (uint32_t e = g.t; e < NH * g.nr; e += g.nt) {
-            const uint32_t r = g.r0 + e / NH, k = e % NH, yl = y0 + r;
-            if (yl >= ry1) continue;
+        auto split = [&](uint32_t r, uint32_t k) {
             const float2 zk = scr[r * LD + (k & (N - 1))], zm = scr[r * LD + ((N - k) & (N - 1))];
-            float2* zc = Zs + (yl - ry0);
+            float2* zc = Zs + (y0 + r - ry0);
             zc[k * LDZ] = r2c_split(zk, zm, ws[k]);
             if (k != N / 2) zc[(N - k) * LDZ] = r2c_split(zm, zk, ws[N - k]);
+        };
+        if constexpr (WLZ) {
+            // the warp's own rows one by one, k across the lanes (no division by NH)
+            for (uint32_t rr = 0; rr < g.nr; rr++)
+                if (y0 + g.r0 + rr < ry1)
+                    for (uint32_t k = g.t; k < NH; k += 32) split(g.r0 + rr, k);
+        } else {
+            for (uint32_t e = g.t; e < NH * g.nr; e += g.nt) {
+                const uint32_t r = g.r0 + e / NH, k = e % NH;
+                if (y0 + r < ry1) split(r, k);
+            }
         }
     }
     cl.sync();                                         // every block's rows are in its Zs
@@ -206,8 +234,14 @@ __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const floa
                 for (int t = 0; t < R2; t++) u[t] = scr[(kzl * R1 + m) * (R2 + 1) + t];
                 dft<R2, false>(u);
                 if (sl) {
+                    if constexpr (R1 % PT == 0) {
+                        const YkCol<R1> col(yk, A, KZ, c, sl, xl, m);
 #pragma unroll
-                    for (int q = 0; q < R2; q++) yk[yk_index(A, KZ, c, sl, xl, m + R1 * q)] = u[q];
+                        for (int q = 0; q < R2; q++) col[q] = u[q];
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < R2; q++) yk[yk_index(A, KZ, c, sl, xl, m + R1 * q)] = u[q];
+                    }
                 } else {
 #pragma unroll
                     for (int q = 0; q < R2; q++) cpk[m + R1 * q] = u[q];
@@ -238,6 +272,7 @@ template <int R1, int R2, bool CPLX>
 __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __restrict__ yk,
                                                                       const void* __restrict__ nkt, const uint32_t Kz,
                                                                       const PlaneArgs A) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ __align__(8) uint64_t bar;
     constexpr uint32_t T = PT;
@@ -371,6 +406,7 @@ __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __
 template <int Z1, int Z2, int R1, int R2>
 __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict__ yk, float* __restrict__ hr,
                                                        const PlaneArgs A) {
+    pdl_enter();
     using G = ZYGeom<Z1, Z2, R1, R2>;
     constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
     constexpr uint32_t CL = G::CL, HY = G::HY, LDZ = G::LDZ, HK = G::HK, KPB = G::KPB;
@@ -398,6 +434,8 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
             if (kzl < A.kzb && sl < s_hi) {
                 float2 u[R2];
                 if (sl) {
+                    // (the full index per element: with a per-q stride the loads are hoisted
+                    // together and the kernel no longer fits its register cap)
 #pragma unroll
                     for (int q = 0; q < R2; q++) u[q] = yk[yk_index(A, KZ, c, sl, xl, m + R1 * q)];
                 } else {
@@ -445,27 +483,43 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
     float2* out0 = reinterpret_cast<float2*>(hr + (size_t)c * A.P) + A.zs;
     const uint32_t ry0 = rank * HY, ry1 = min(A.by, ry0 + HY);
     const RowGroup<WLZ, TY, 32 / Z2> g;
+    float2* outx = out0 + ((size_t)x * M1 + A.by0) * N;   // pair n of row yl at outx[yl N + n]
+    constexpr uint32_t half = N / 2, nh = half + 1;
+    // Z'_k and Z'_{N-k} of row r from X_k, X_{N-k}, in place
+    auto pre = [&](uint32_t r, uint32_t k) {
+        const float2 xk = scr[r * LD + k], xm = scr[r * LD + (N - k)];
+        const float2 zk = c2r_pre(xk, xm, ws[k]);
+        if (k != 0 && k != half) scr[r * LD + (N - k)] = c2r_pre(xm, xk, ws[N - k]);
+        scr[r * LD + k] = zk;
+    };
     for (uint32_t y0 = ry0; y0 < ry1; y0 += TY) {
-        for (uint32_t e = g.t; e < KZ * g.nr; e += g.nt) {
-            const uint32_t r = g.r0 + e / KZ, k = e % KZ, yl = y0 + r;
-            scr[r * LD + k] = yl < ry1 ? Zs[k * LDZ + (yl - ry0)] : make_float2(0.f, 0.f);
-        }
-        group_sync<WLZ>();
-        // pairwise in place: thread (r, k) for k in [0, N/2] writes Z'_k and Z'_{N-k}
-        constexpr uint32_t half = N / 2, nh = half + 1;
-        for (uint32_t e = g.t; e < g.nr * nh; e += g.nt) {
-            const uint32_t r = g.r0 + e / nh, k = e % nh;
-            const float2 xk = scr[r * LD + k], xm = scr[r * LD + (N - k)];
-            const float2 zk = c2r_pre(xk, xm, ws[k]);
-            if (k != 0 && k != half) scr[r * LD + (N - k)] = c2r_pre(xm, xk, ws[N - k]);
-            scr[r * LD + k] = zk;
+        if constexpr (WLZ) {
+            // the warp's own rows one by one, k across the lanes (no division by KZ or nh)
+            for (uint32_t rr = 0; rr < g.nr; rr++) {
+                const uint32_t r = g.r0 + rr, yl = y0 + r;
+                for (uint32_t k = g.t; k < KZ; k += 32)
+                    scr[r * LD + k] = yl < ry1 ? Zs[k * LDZ + (yl - ry0)] : make_float2(0.f, 0.f);
+            }
+            __syncwarp();
+            for (uint32_t rr = 0; rr < g.nr; rr++)
+                for (uint32_t k = g.t; k < nh; k += 32) pre(g.r0 + rr, k);
+        } else {
+            for (uint32_t e = g.t; e < KZ * g.nr; e += g.nt) {
+                const uint32_t r = g.r0 + e / KZ, k = e % KZ, yl = y0 + r;
+                scr[r * LD + k] = yl < ry1 ? Zs[k * LDZ + (yl - ry0)] : make_float2(0.f, 0.f);
+            }
+            __syncthreads();
+            for (uint32_t e = g.t; e < g.nr * nh; e += g.nt) {
+                const uint32_t r = g.r0 + e / nh, k = e % nh;
+                pre(r, k);
+            }
         }
         group_sync<WLZ>();
         fft2pass<Z1, Z2, true, false, true>(scr, LD, twz, TY);   // pairs n < N/2 only
         for (uint32_t e = g.t; e < g.nr * (N / 2); e += g.nt) {
             const uint32_t r = g.r0 + e / (N / 2), n = e % (N / 2), yl = y0 + r;
             if (yl >= ry1 || n >= A.nz) continue;
-            out0[((size_t)x * M1 + A.by0 + yl) * N + n] = scr[r * LD + n];
+            outx[yl * N + n] = scr[r * LD + n];
         }
         group_sync<WLZ>();
     }
@@ -598,25 +652,6 @@ cudaError_t set_smem(K kern, size_t bytes) {
     return raise_smem_limit(reinterpret_cast<const void*>(kern), bytes);
 }
 
-// A launch with thread-block clusters of `cl` blocks along x.
-template <typename... KArgs, typename... Args>
-cudaError_t launch_clusters(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, uint32_t cl,
-                            Args... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = grid;
-    cfg.blockDim = block;
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = cl;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, args...);
-}
-
 // z split x y split instantiations: z N in {4..256}, y mesh in {8..256}
 #define ASD_ZY_CASES(M, Z1, Z2)                                                                           \
     switch (M) {                                                                                          \
@@ -641,7 +676,7 @@ cudaError_t launch_clusters(void (*kern)(KArgs...), dim3 grid, dim3 block, size_
     default: return cudaErrorInvalidValue;                                                                \
     }
 
-cudaError_t run_zy(const LongRange& L, const PlaneArgs& A, bool inverse, cudaStream_t st) {
+cudaError_t run_zy(const LongRange& L, const PlaneArgs& A, bool inverse, cudaStream_t st, bool pdl) {
     const size_t sm = zy_smem(L, A);
     const uint32_t CL = zy_cl(L.mesh[1]);
     const dim3 grid(A.bx * CL, 3);
@@ -653,10 +688,10 @@ cudaError_t run_zy(const LongRange& L, const PlaneArgs& A, bool inverse, cudaStr
 #define ASD_ZY_CALL(Z1, Z2, R1, R2)                                                                       \
     if (inverse) {                                                                                        \
         if ((e = set_smem(plane_yz_inv<Z1, Z2, R1, R2>, sm)) != cudaSuccess) return e;                    \
-        e = launch_clusters(plane_yz_inv<Z1, Z2, R1, R2>, grid, dim3(256), sm, st, CL, ykc, hr, A);       \
+        e = launch_step_kernel(plane_yz_inv<Z1, Z2, R1, R2>, grid, dim3(256), sm, st, CL, pdl, ykc, hr, A); \
     } else {                                                                                              \
         if ((e = set_smem(plane_zy_fwd<Z1, Z2, R1, R2>, sm)) != cudaSuccess) return e;                    \
-        e = launch_clusters(plane_zy_fwd<Z1, Z2, R1, R2>, grid, dim3(256), sm, st, CL, mr, yk, A);         \
+        e = launch_step_kernel(plane_zy_fwd<Z1, Z2, R1, R2>, grid, dim3(256), sm, st, CL, pdl, mr, yk, A);  \
     }
     ASD_Z_CASES(L.mesh[2] / 2, L.mesh[1])
 #undef ASD_ZY_CALL
@@ -664,30 +699,31 @@ cudaError_t run_zy(const LongRange& L, const PlaneArgs& A, bool inverse, cudaStr
 }
 
 template <int R1, int R2>
-cudaError_t run_xconv_t(const LongRange& L, const PlaneArgs& A, bool cplx, cudaStream_t st) {
+cudaError_t run_xconv_t(const LongRange& L, const PlaneArgs& A, bool cplx, cudaStream_t st, bool pdl) {
     const uint32_t Kz = L.mesh[2] / 2 + 1;
     const dim3 grid(A.ntile, Kz);
     const size_t sm = xconv_smem(A, cplx);
     cudaError_t e;
+    const void* nkt = L.nkt;
     if (cplx) {
         if ((e = set_smem(plane_x_conv<R1, R2, true>, sm)) != cudaSuccess) return e;
-        plane_x_conv<R1, R2, true><<<grid, PT * R1, sm, st>>>(L.yk, L.nkt, Kz, A);
+        e = launch_step_kernel(plane_x_conv<R1, R2, true>, grid, dim3(PT * R1), sm, st, 1, pdl, L.yk, nkt, Kz, A);
     } else {
         if ((e = set_smem(plane_x_conv<R1, R2, false>, sm)) != cudaSuccess) return e;
-        plane_x_conv<R1, R2, false><<<grid, PT * R1, sm, st>>>(L.yk, L.nkt, Kz, A);
+        e = launch_step_kernel(plane_x_conv<R1, R2, false>, grid, dim3(PT * R1), sm, st, 1, pdl, L.yk, nkt, Kz, A);
     }
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
-cudaError_t run_xconv(const LongRange& L, const PlaneArgs& A, bool cplx, cudaStream_t st) {
+cudaError_t run_xconv(const LongRange& L, const PlaneArgs& A, bool cplx, cudaStream_t st, bool pdl) {
     switch (A.m0) {
-    case 4: return run_xconv_t<2, 2>(L, A, cplx, st);
-    case 8: return run_xconv_t<4, 2>(L, A, cplx, st);
-    case 16: return run_xconv_t<4, 4>(L, A, cplx, st);
-    case 32: return run_xconv_t<8, 4>(L, A, cplx, st);
-    case 64: return run_xconv_t<8, 8>(L, A, cplx, st);
-    case 128: return run_xconv_t<16, 8>(L, A, cplx, st);
-    case 256: return run_xconv_t<16, 16>(L, A, cplx, st);
+    case 4: return run_xconv_t<2, 2>(L, A, cplx, st, pdl);
+    case 8: return run_xconv_t<4, 2>(L, A, cplx, st, pdl);
+    case 16: return run_xconv_t<4, 4>(L, A, cplx, st, pdl);
+    case 32: return run_xconv_t<8, 4>(L, A, cplx, st, pdl);
+    case 64: return run_xconv_t<8, 8>(L, A, cplx, st, pdl);
+    case 128: return run_xconv_t<16, 8>(L, A, cplx, st, pdl);
+    case 256: return run_xconv_t<16, 16>(L, A, cplx, st, pdl);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -790,13 +826,14 @@ cudaError_t launch_lr_planes(asd_handle* h) {
                             : 6.0 * 4.0 * A.nkx * L.mesh[1] * (L.mesh[2] / 2 + 1);
     cudaError_t e;
     timer_begin(h);
-    if ((e = run_zy(L, A, false, h->stream)) != cudaSuccess) return e;
+    const bool pdl = step_pdl(h);
+    if ((e = run_zy(L, A, false, h->stream, pdl)) != cudaSuccess) return e;
     timer_end(h, "plane_zy_fwd (z R2C + y FFT)", rows + spec);
     timer_begin(h);
-    if ((e = run_xconv(L, A, cplx, h->stream)) != cudaSuccess) return e;
+    if ((e = run_xconv(L, A, cplx, h->stream, pdl)) != cudaSuccess) return e;
     timer_end(h, "plane_x_conv (x FFT, N_k product, inverse x FFT)", 2.0 * spec + nkb);
     timer_begin(h);
-    if ((e = run_zy(L, A, true, h->stream)) != cudaSuccess) return e;
+    if ((e = run_zy(L, A, true, h->stream, pdl)) != cudaSuccess) return e;
     timer_end(h, "plane_yz_inv (inverse y FFT + z C2R)", spec + rows);
     h->launches += 3;
     return cudaSuccess;

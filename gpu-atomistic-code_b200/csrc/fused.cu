@@ -124,6 +124,7 @@ struct MinBlocks {
 template <typename R, int EX, bool FULL, bool COMP, int K>
 __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL, K>::value)
     stage_kernel(const StepConst c, const SellDev sell, const DiaDev dia, const StageArgs<R> a) {
+    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t stage_bar;
     R* tab = reinterpret_cast<R*>(smem_raw);
@@ -409,9 +410,15 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL, K>::value)
     if (stage_timeout) mbar_wait_bounded(&stage_bar, STAGE_WAIT_POLLS);
 }
 
-__global__ void advance_k(uint64_t* step, uint32_t n) { *step += n; }
+__global__ void advance_k(uint64_t* step, uint32_t n) {
+    pdl_enter();
+    *step += n;
+}
 // The det field is written at the step the device counter holds (the one-step graph's step).
-__global__ void det_here_k(const uint64_t* step, double* dyn) { dyn[DYN_DET_STEP] = (double)*step; }
+__global__ void det_here_k(const uint64_t* step, double* dyn) {
+    pdl_enter();
+    dyn[DYN_DET_STEP] = (double)*step;
+}
 
 template <typename R>
 Vec3<R> v3(R* const p[3]) { return Vec3<R>{{p[0], p[1], p[2]}}; }
@@ -469,7 +476,11 @@ cudaError_t launch_stage_k(asd_handle* hd, const StageArgs<R>& a) {
         if (e != cudaSuccess) return e;
     }
     timer_begin(hd);
-    stage_kernel<R, EX, FULL, COMP, K><<<grid, B, smem, hd->stream>>>(hd->sc, hd->sell, hd->dia, a);
+    {
+        const cudaError_t e = launch_step_kernel(stage_kernel<R, EX, FULL, COMP, K>, dim3(grid), dim3(B), smem,
+                                                 hd->stream, 1, step_pdl(hd), hd->sc, hd->sell, hd->dia, a);
+        if (e != cudaSuccess) return e;
+    }
     hd->launches += 1;
     if (hd->timing) {
         const bool typed = (EX == ASD_EXCH_CSR && hd->sell.typed) || (EX == ASD_EXCH_DIA && hd->dia.dtype);
@@ -664,15 +675,16 @@ cudaError_t launch_fused_step(asd_handle* h, uint32_t rel, bool) {
 }
 
 cudaError_t launch_det_here(asd_handle* h) {
-    det_here_k<<<1, 1, 0, h->stream>>>(h->d_step, h->d_dyn);
+    const cudaError_t e = launch_step_kernel(det_here_k, dim3(1), dim3(1), 0, h->stream, 1, step_pdl(h),
+                                             (const uint64_t*)h->d_step, h->d_dyn);
     h->launches += 1;
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_step_advance(asd_handle* h, uint32_t nsteps) {
-    advance_k<<<1, 1, 0, h->stream>>>(h->d_step, nsteps);
+    const cudaError_t e = launch_step_kernel(advance_k, dim3(1), dim3(1), 0, h->stream, 1, step_pdl(h), h->d_step, nsteps);
     h->launches += 1;
-    return cudaGetLastError();
+    return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 }  // namespace asd

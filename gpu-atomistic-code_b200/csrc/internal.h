@@ -4,6 +4,7 @@
 #include "common.cuh"
 #include <cufft.h>
 #include <string>
+#include <utility>
 #include <vector>
 
 namespace asd {
@@ -223,6 +224,10 @@ namespace asd {
 // Timed launches (asd_time_kernels): before the launch, an optional L2 flush and an event on the
 // handle's stream; after it, the event pair's device time accumulated under `name` with the
 // launch's algorithmic bytes.
+// Step kernels launch with programmatic dependent launch unless kernels are timed one by one or
+// ASD_FLAG_SERIAL_LAUNCH asks for strict order.
+inline bool step_pdl(const asd_handle* h) { return !h->timing && !(h->p.flags & ASD_FLAG_SERIAL_LAUNCH); }
+
 inline void timer_begin(asd_handle* h) {
     if (!h->timing) return;
     if (h->flush_buf) cudaMemsetAsync(h->flush_buf, 0, h->flush_bytes, h->stream);
@@ -284,6 +289,36 @@ cudaError_t launch_convert_spins_in(asd_handle* h, const double* d_aos);
 // Raise a kernel's dynamic shared-memory limit on the current device to at least `bytes`,
 // calling cudaFuncSetAttribute only when this (device, kernel) has not been raised that far.
 cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
+
+// Launch of a step kernel (one that starts with pdl_enter): with `pdl` its blocks may become
+// resident while the previous kernel of the stream finishes (programmatic dependent launch);
+// `cluster` > 1 groups the blocks into thread-block clusters along x.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_step_kernel(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                               uint32_t cluster, bool pdl, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[2];
+    unsigned n = 0;
+    if (cluster > 1) {
+        attr[n].id = cudaLaunchAttributeClusterDimension;
+        attr[n].val.clusterDim.x = cluster;
+        attr[n].val.clusterDim.y = 1;
+        attr[n].val.clusterDim.z = 1;
+        n++;
+    }
+    if (pdl) {
+        attr[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[n].val.programmaticStreamSerializationAllowed = 1;
+        n++;
+    }
+    cfg.attrs = attr;
+    cfg.numAttrs = n;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
 cudaError_t launch_check_spins(asd_handle* h, const double* d_aos, unsigned long long* d_check);
 cudaError_t launch_convert_out(asd_handle* h, int what, double* d_aos);
 cudaError_t build_nk_f32(asd_handle* h, const double* d_nr);

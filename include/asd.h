@@ -77,6 +77,9 @@ extern "C" {
                                                    the x transform leaves its tile, an invalid field);
                                                    the wait before a block retires keeps its bound;
                                                    asd_sync reports ASD_ETIMEOUT */
+#define ASD_FLAG_SERIAL_LAUNCH       (1u << 21) /* fused forms: launch the step kernels strictly one
+                                                   after another (no programmatic dependent launch:
+                                                   a comparison aid) */
 
 #define ASD_ALL_REPLICAS 0xFFFFFFFFu
 
