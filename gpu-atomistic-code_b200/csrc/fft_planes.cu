@@ -120,6 +120,10 @@ __device__ __forceinline__ void copy_tw(float2* dst, const float2* __restrict__ 
 // at its end, so the wait does not hold its global stores behind a fence.
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
 __device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+// Arrive without ordering any memory access: the start-of-kernel handshake (every block of the
+// cluster is running before any block touches a peer's shared memory), waited for just before
+// the first remote access.
+__device__ __forceinline__ void cluster_arrive_relaxed() { asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory"); }
 
 // The threads that handle a set of z rows: with warp-local rows (rows_warp_local<Z1, Z2>) warp w
 // loads, transforms and stores its own RW = 32 / Z2 rows of the TY, else the whole block
@@ -421,6 +425,7 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
     const uint32_t rank = cl.block_rank();
     const uint32_t xl = blockIdx.x / CL, c = blockIdx.y, x = A.bx0 + xl;
     copy_tw(twz, A.twt, 2 * N + 1 + M1);
+    cluster_arrive_relaxed();
     float2* zb[CL];
 #pragma unroll
     for (uint32_t o = 0; o < CL; o++) zb[o] = cl.map_shared_rank(Zs, o);
@@ -452,6 +457,7 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
                     scr[(kzl * R1 + m) * (R2 + 1) + t] = t ? cmulc(u[t], twy[t * m]) : u[t];
             }
         }
+        if (s0 == s_lo) cluster_wait();                // every peer is running: remote stores may start
         group_sync<WLY>();
         {
             const uint32_t kzl = threadIdx.x / R2, t = threadIdx.x % R2, sl = s0 + kzl;
