@@ -87,7 +87,7 @@ void free_all(asd_handle* h) {
     F(L.k1); F(L.k2); F(L.yk); F(L.nkt); F(L.twt);
     F(h->sq.idx); F(h->sq.sub); F(h->sq.uo); F(h->sq.kidx); F(h->sq.grid); F(h->sq.series);
     if (h->sq.plan) cufftDestroy(h->sq.plan);
-    F(h->d_magpart); F(h->d_mag); F(h->d_inv_count); F(h->d_sub_of_atom); F(h->d_stats);
+    F(h->d_magpart); F(h->d_mag); F(h->d_magcnt); F(h->d_inv_count); F(h->d_sub_of_atom); F(h->d_stats);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     if (h->graph1) cudaGraphExecDestroy(h->graph1);
     if (h->kev[0]) cudaEventDestroy(h->kev[0]);
@@ -1031,6 +1031,8 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
             h->magpart_len = (size_t)nsys * nchunk * h->nsub * 3;
             h->d_magpart = dalloc<double>(h->magpart_len);
             h->d_mag = dalloc<double>((size_t)nsys * h->nsub * 3);
+            h->d_magcnt = dalloc<uint32_t>(1);
+            CK(cudaMemset(h->d_magcnt, 0, sizeof(uint32_t)));
             h->d_stats = dalloc<double>((size_t)nsys * h->nsub * 4);
             std::vector<double> inv((size_t)nsys * h->nsub, 0.0);
             for (uint32_t r = 0; r < nsys; r++) {

@@ -185,6 +185,7 @@ struct asd_handle {
     double* d_magpart = nullptr;
     size_t magpart_len = 0;
     double* d_mag = nullptr;
+    uint32_t* d_magcnt = nullptr;        // block ticket of the one-launch magnetisation (rearmed to 0)
     double* d_inv_count = nullptr;
     uint32_t* d_sub_of_atom = nullptr;
     uint64_t graph_launches = 0;

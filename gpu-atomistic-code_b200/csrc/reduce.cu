@@ -25,13 +25,48 @@ __device__ __forceinline__ double block_sum(double v, double* sm) {
     return r;
 }
 
+struct MagFinish {
+    uint32_t* cnt;              // block ticket counter (nullptr: mag_final forms the means)
+    uint32_t nrep;
+    const double* inv_count;    // 1 / spins per (replica, sublattice)
+    double* out;                // means [nrep][nsub][3]
+};
+
+// The last block of a partial-sum launch to finish (ticket on *cnt) also forms the means:
+// out[q] = inv_count * (the chunk partials of output q, each summed by one warp in a fixed
+// order), the same whatever the order the blocks finish in; it then rearms the counter.  Used
+// when the outputs are few (cnt == nullptr: a separate mag_final launch does it).
+__device__ __forceinline__ void mag_finish_last(uint32_t* cnt, uint32_t nblocks, uint32_t nrep, uint32_t nsub,
+                                                uint32_t nchunk, const double* part, const double* inv_count,
+                                                double* out) {
+    if (!cnt) return;
+    __shared__ uint32_t last;
+    __threadfence();                                   // this block's partials before its ticket
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(cnt, 1u) == nblocks - 1 ? 1u : 0u;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // one warp per output: lane l sums the chunks l, l + 32, ..., then a shuffle tree
+    const uint32_t w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    for (uint32_t q = w; q < nrep * nsub * 3; q += nw) {
+        const uint32_t comp = q % 3, s = (q / 3) % nsub, r = q / (3 * nsub);
+        double acc = 0.0;
+        for (uint32_t ch = l; ch < nchunk; ch += 32)
+            acc += __ldcg(part + (((size_t)r * nchunk + ch) * nsub + s) * 3 + comp);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (l == 0) out[q] = acc * inv_count[r * nsub + s];
+    }
+    if (threadIdx.x == 0) *cnt = 0;
+}
+
 // Partial sums of S over one chunk of one replica, per sublattice, in FP64 and
 // a fixed reduction order (deterministic): part[((r*nchunk + c)*nsub + s)*3 + comp].
 template <typename R>
 __global__ void mag_partial(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
                             const R* __restrict__ sx, const R* __restrict__ sy, const R* __restrict__ sz,
                             const float* __restrict__ lx, const float* __restrict__ ly, const float* __restrict__ lz,
-                            uint32_t nchunk, double* __restrict__ part) {
+                            uint32_t nchunk, double* __restrict__ part, MagFinish f) {
     __shared__ double sm[32];
     const uint32_t r = blockIdx.y, ch = blockIdx.x;
     const uint32_t beg = c.rep_off[r] + ch * MAG_CHUNK;
@@ -49,16 +84,17 @@ __global__ void mag_partial(StepConst c, uint32_t nsub, const uint32_t* __restri
             o[0] = t0; o[1] = t1; o[2] = t2;
         }
     }
+    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out);
 }
 
-// Plain form: AoS doubles.
 // One pass over the chunk for up to NS sublattices, each spin added to its own sublattice's
 // register accumulators (the general kernel above re-reads the chunk once per sublattice).
 template <typename R, int NS>
 __global__ void mag_partial_ns(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
                                const R* __restrict__ sx, const R* __restrict__ sy, const R* __restrict__ sz,
                                const float* __restrict__ lx, const float* __restrict__ ly,
-                               const float* __restrict__ lz, uint32_t nchunk, double* __restrict__ part) {
+                               const float* __restrict__ lz, uint32_t nchunk, double* __restrict__ part,
+                               MagFinish f) {
     __shared__ double sm[32];
     const uint32_t r = blockIdx.y, ch = blockIdx.x;
     const uint32_t beg = c.rep_off[r] + ch * MAG_CHUNK;
@@ -88,10 +124,13 @@ __global__ void mag_partial_ns(StepConst c, uint32_t nsub, const uint32_t* __res
             o[0] = t[0]; o[1] = t[1]; o[2] = t[2];
         }
     }
+    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out);
 }
 
+// Plain form: AoS doubles.
 __global__ void mag_partial_aos(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
-                                const double* __restrict__ s3, uint32_t nchunk, double* __restrict__ part) {
+                                const double* __restrict__ s3, uint32_t nchunk, double* __restrict__ part,
+                                MagFinish f) {
     __shared__ double sm[32];
     const uint32_t r = blockIdx.y, ch = blockIdx.x;
     const uint32_t beg = c.rep_off[r] + ch * MAG_CHUNK;
@@ -108,6 +147,7 @@ __global__ void mag_partial_aos(StepConst c, uint32_t nsub, const uint32_t* __re
             o[0] = t0; o[1] = t1; o[2] = t2;
         }
     }
+    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out);
 }
 
 __global__ void mag_final(uint32_t nrep, uint32_t nsub, uint32_t nchunk, const double* __restrict__ part,
@@ -350,29 +390,35 @@ cudaError_t launch_magnetisation(asd_handle* h) {
     dim3 grid(nchunk ? nchunk : 1, h->nrep);
     const uint32_t* sub_of_atom = h->d_sub_of_atom;
     const double* inv_count = h->d_inv_count;
+    // few outputs: the last partial block forms the means (one launch); else mag_final does
+    const uint32_t nq = h->nrep * nsub * 3;
+    const MagFinish f{nq <= 48 ? h->d_magcnt : nullptr, h->nrep, inv_count, h->d_mag};
     if (h->p.precision == ASD_FP64_PLAIN) {
-        mag_partial_aos<<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->p_s, grid.x, h->d_magpart);
+        mag_partial_aos<<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->p_s, grid.x, h->d_magpart, f);
     } else if (h->p.precision == ASD_FP32) {
         const bool comp = (h->p.flags & ASD_FLAG_COMPENSATED) != 0;
         const float* lo[3] = {comp ? h->sl[0] : nullptr, comp ? h->sl[1] : nullptr, comp ? h->sl[2] : nullptr};
         if (nsub == 1)
             mag_partial_ns<float, 1><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1],
-                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart);
+                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart, f);
         else if (nsub == 2)
             mag_partial_ns<float, 2><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1],
-                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart);
+                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart, f);
         else if (nsub <= 4)
             mag_partial_ns<float, 4><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1],
-                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart);
+                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart, f);
         else
             mag_partial<float><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1], h->sf[2],
-                                                                 lo[0], lo[1], lo[2], grid.x, h->d_magpart);
+                                                                 lo[0], lo[1], lo[2], grid.x, h->d_magpart, f);
     } else {
         mag_partial<double><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sd[0], h->sd[1], h->sd[2],
-                                                              nullptr, nullptr, nullptr, grid.x, h->d_magpart);
+                                                              nullptr, nullptr, nullptr, grid.x, h->d_magpart, f);
     }
-    mag_final<<<h->nrep * nsub * 3, 128, 0, h->stream>>>(h->nrep, nsub, grid.x, h->d_magpart, inv_count, h->d_mag);
-    h->launches += 2;
+    h->launches += 1;
+    if (!f.cnt) {
+        mag_final<<<nq, 128, 0, h->stream>>>(h->nrep, nsub, grid.x, h->d_magpart, inv_count, h->d_mag);
+        h->launches += 1;
+    }
     return cudaGetLastError();
 }
 
