@@ -506,3 +506,30 @@ def test_four_spin_term(gpu, div3):
             assert d <= tol, (prec, d)
             if prec == A.FP64_PLAIN:
                 assert np.array_equal(h.get_field(), o.field())
+
+
+@pytest.mark.parametrize("prec", [A.FP32, A.FP64_FUSED])
+def test_dependent_launch_bit_identical(gpu, prec):
+    """Programmatic dependent launch (the default: each step kernel's blocks may become resident
+    while its predecessor finishes, and wait for it before touching memory) against strictly
+    ordered launches (ASD_FLAG_SERIAL_LAUNCH), through the 32-step graphs, the one-step graph
+    and direct launches: bit-identical spins at finite temperature, with the plane-kernel dipole
+    field and with RK4."""
+    cases = [(LT.bct2_antiferromagnet(5, T=300.0), {}),
+             (LT.sc_ferromagnet((16, 16, 8), pbc=(0, 0, 0), dipole=True, T=100.0), {}),
+             (LT.film_dia(12, 10, 3, dipole=True), dict(integrator=A.RK4))]
+    for s, kw in cases:
+        S0 = LT.random_spins(s.nspins, 12)
+        base = A.FLAG_COMPENSATED if prec == A.FP32 else 0
+        outs = []
+        for flags, single in ((base, False), (base | A.FLAG_SERIAL_LAUNCH, False), (base, True)):
+            with A.Handle(A.RunParams(precision=prec, flags=flags, seed=5, **kw), s) as h:
+                h.set_spins(S0)
+                if single:
+                    for _ in range(70):
+                        h.step(1)
+                else:
+                    h.step(70)                         # two 32-step graphs and 6 direct steps
+                outs.append(h.get_spins())
+        assert np.array_equal(outs[0], outs[1]), (s.nspins, maxdiff(outs[0], outs[1]))
+        assert np.array_equal(outs[0], outs[2]), (s.nspins, maxdiff(outs[0], outs[2]))
