@@ -33,12 +33,12 @@ struct MagFinish {
 };
 
 // The last block of a partial-sum launch to finish (ticket on *cnt) also forms the means:
-// out[q] = inv_count * (the chunk partials of output q, each summed by one warp in a fixed
-// order), the same whatever the order the blocks finish in; it then rearms the counter.  Used
+// out[q] = inv_count * (the chunk partials of output q summed by the block in a fixed order),
+// the same whatever the order the blocks finish in; it then rearms the counter.  Used
 // when the outputs are few (cnt == nullptr: a separate mag_final launch does it).
 __device__ __forceinline__ void mag_finish_last(uint32_t* cnt, uint32_t nblocks, uint32_t nrep, uint32_t nsub,
                                                 uint32_t nchunk, const double* part, const double* inv_count,
-                                                double* out) {
+                                                double* out, double* sm) {
     if (!cnt) return;
     __shared__ uint32_t last;
     __threadfence();                                   // this block's partials before its ticket
@@ -47,15 +47,14 @@ __device__ __forceinline__ void mag_finish_last(uint32_t* cnt, uint32_t nblocks,
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // one warp per output: lane l sums the chunks l, l + 32, ..., then a shuffle tree
-    const uint32_t w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
-    for (uint32_t q = w; q < nrep * nsub * 3; q += nw) {
+    // the whole block per output: thread t sums the chunks t, t + blockDim, ..., then a block sum
+    for (uint32_t q = 0; q < nrep * nsub * 3; q++) {
         const uint32_t comp = q % 3, s = (q / 3) % nsub, r = q / (3 * nsub);
         double acc = 0.0;
-        for (uint32_t ch = l; ch < nchunk; ch += 32)
+        for (uint32_t ch = threadIdx.x; ch < nchunk; ch += blockDim.x)
             acc += __ldcg(part + (((size_t)r * nchunk + ch) * nsub + s) * 3 + comp);
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-        if (l == 0) out[q] = acc * inv_count[r * nsub + s];
+        const double t = block_sum(acc, sm);
+        if (threadIdx.x == 0) out[q] = t * inv_count[r * nsub + s];
     }
     if (threadIdx.x == 0) *cnt = 0;
 }
@@ -84,7 +83,7 @@ __global__ void mag_partial(StepConst c, uint32_t nsub, const uint32_t* __restri
             o[0] = t0; o[1] = t1; o[2] = t2;
         }
     }
-    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out);
+    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out, sm);
 }
 
 // One pass over the chunk for up to NS sublattices, each spin added to its own sublattice's
@@ -124,7 +123,7 @@ __global__ void mag_partial_ns(StepConst c, uint32_t nsub, const uint32_t* __res
             o[0] = t[0]; o[1] = t[1]; o[2] = t[2];
         }
     }
-    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out);
+    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out, sm);
 }
 
 // Plain form: AoS doubles.
@@ -147,7 +146,7 @@ __global__ void mag_partial_aos(StepConst c, uint32_t nsub, const uint32_t* __re
             o[0] = t0; o[1] = t1; o[2] = t2;
         }
     }
-    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out);
+    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out, sm);
 }
 
 __global__ void mag_final(uint32_t nrep, uint32_t nsub, uint32_t nchunk, const double* __restrict__ part,
@@ -392,7 +391,7 @@ cudaError_t launch_magnetisation(asd_handle* h) {
     const double* inv_count = h->d_inv_count;
     // few outputs: the last partial block forms the means (one launch); else mag_final does
     const uint32_t nq = h->nrep * nsub * 3;
-    const MagFinish f{nq <= 48 ? h->d_magcnt : nullptr, h->nrep, inv_count, h->d_mag};
+    const MagFinish f{nq <= 12 ? h->d_magcnt : nullptr, h->nrep, inv_count, h->d_mag};
     if (h->p.precision == ASD_FP64_PLAIN) {
         mag_partial_aos<<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->p_s, grid.x, h->d_magpart, f);
     } else if (h->p.precision == ASD_FP32) {
