@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the sLLG step: spin-updates/s on one B200 (or N replicas on N GPUs).
 
-Default workload ("northstar"): the 1M-spin exchange + dipolar lattice, simple cubic
+Default workload ("sc128x128x64_dipole"): the 1M-spin exchange + dipolar lattice, simple cubic
 128x128x64 (1,048,576 spins), open boundaries, nearest-neighbour exchange in CSR (SELL-32 on
 the device) plus the point-dipole field by zero-padded FFT on the 256x256x128 mesh, refreshed
 every step, Heun, T=0, FP32 state with FP64 renormalisation.  Other workloads (--workload):
@@ -93,7 +93,7 @@ def make_workload(name):
         s = LT.sc_fft(128)
         return [s], dict(integrator=A.HEUN, dt=1e-16), {"lattice": "sc 128^3 open, pad 256^3", "nspins": s.nspins,
                                                          "field": "dipole+exchange via R2C/C2R FFT", "T_K": 0.0}
-    if name == "northstar":
+    if name == "sc128x128x64_dipole":
         s = LT.sc_ferromagnet((128, 128, 64), pbc=(0, 0, 0), dipole=True)
         return [s], dict(integrator=A.HEUN, dt=1e-16, update=1), {"lattice": "sc 128x128x64 open", "nspins": s.nspins,
                                                                    "field": "CSR NN exchange + FFT dipole every step",
@@ -163,17 +163,17 @@ class ClockSampler:
 
 # ---------------------------------------------------------------- reference arm
 # The reference's CPU step cannot evaluate the dipole field here (its FFT path needs FFTW3, which
-# is absent), so the north-star lattice runs on the FP64 restatement with the long-range field by
+# is absent), so the sc 128x128x64 dipole lattice runs on the FP64 restatement with the long-range field by
 # threaded FFT (oracle/fft_oracle.py, pinned against the direct-sum oracle); lattices without a
 # long-range field run the reference's own llgCPU compiled from source.  Neither loads the
-# product library: the north-star CSR comes from a numpy builder that is bit-exact with the
+# product library: the sc 128x128x64 CSR comes from a numpy builder that is bit-exact with the
 # reference's exchunitcell, the BCT-2 CSR from the reference's exchunitcell itself.
 NS_DIM = (128, 128, 64)
 REF_STEP_CAP = 60          # at most this many timed CPU steps per run (~1.3 s each at 1M spins, 8 cores)
 
 
-def cpu_port_northstar(steps, warmup, workers=None):
-    """FFT restatement on the north-star lattice: (spin-updates/s, seconds, spins, threads, steps)."""
+def cpu_port_sc128x128x64(steps, warmup, workers=None):
+    """FFT restatement on the sc 128x128x64 dipole lattice: (spin-updates/s, seconds, spins, threads, steps)."""
     sys.path[:0] = [REPO]
     from oracle import fft_oracle as F
     s = F.sc_dipole_system(NS_DIM)
@@ -226,14 +226,14 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic"}
     k = max(1, min(args.steps, REF_STEP_CAP))
-    if args.workload == "northstar":
-        rate, secs, n, thr, k = cpu_port_northstar(k, min(args.warmup, 2))
+    if args.workload == "sc128x128x64_dipole":
+        rate, secs, n, thr, k = cpu_port_sc128x128x64(k, min(args.warmup, 2))
         sample = (f"FP64 restatement of the reference's Heun step (oracle/fft_oracle.py: CSR exchange, dipole by "
                   f"threaded FFT on the 256x256x128 mesh, pinned against the direct-sum oracle) on the same "
                   f"sc 128x128x64 open lattice and initial spins, {k} timed steps of the whole lattice "
                   f"({secs:.1f} s), {thr} threads")
         kind = "port"
-        cfg = {"workload": "northstar", "lattice": "sc 128x128x64 open", "nspins": n,
+        cfg = {"workload": "sc128x128x64_dipole", "lattice": "sc 128x128x64 open", "nspins": n,
                "field": "CSR NN exchange + FFT dipole every step", "T_K": 0.0, "integrator": "heun",
                "same_config": True}
     elif args.workload == "bct2_64":
@@ -412,8 +412,8 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            if args.workload == "northstar":
-                rate, secs, nn, thr, k = cpu_port_northstar(args.cpu_steps, 1)
+            if args.workload == "sc128x128x64_dipole":
+                rate, secs, nn, thr, k = cpu_port_sc128x128x64(args.cpu_steps, 1)
                 cpu = {"value": rate, "unit": "spin-updates/s", "cores": thr, "kind": "port",
                        "sample": f"FP64 restatement (oracle/fft_oracle.py: CSR exchange, dipole by threaded FFT) on "
                                  f"the same sc 128x128x64 lattice and spins, {k} whole-lattice steps "
@@ -461,11 +461,11 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="northstar")
+    ap.add_argument("--workload", default="sc128x128x64_dipole")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=8,
-                    help="whole-lattice steps of the CPU baseline (north star: ~1.3 s each on 8 cores)")
+                    help="whole-lattice steps of the CPU baseline (sc 128x128x64 dipole lattice: ~1.3 s each on 8 cores)")
     ap.add_argument("--err-steps", type=int, default=100)
     ap.add_argument("--layout", default="", choices=["", "sell", "dia"],
                     help="device layout of the exchange matrix instead of the autotuner's choice")

@@ -19,7 +19,7 @@ Semantics (default flags of the oracle: the reference CUDA path with its bugs fi
     of every `update`-th step and kept for both stages (src/cuda.cu:47-90).
   * ASD_LR_FFT: the whole field of each stage from the interaction matrix (exchange folded in,
     src/cuda.cu:101-112).
-  * T = 0 only (no thermal term); the north-star lattice it times is a T = 0 workload.
+  * T = 0 only (no thermal term); the 1M-spin dipole lattice it times is a T = 0 workload.
 
 The transform is pruned to the spins' bounding box as the device path is: a real FFT along z of
 the box rows, complex FFTs along y then x of the rows that hold data, the 3x3 product with N_k on
@@ -104,7 +104,7 @@ def dipole_nr(L, abc=3e-10, mu_scale=1.0):
 
 def sc_dipole_system(L, J=1e-21, mu=1.5, lam=0.1, k1u=1e-23, pbc=(0, 0, 0), abc=3e-10):
     """The simple-cubic ferromagnet with CSR nearest-neighbour exchange and the point-dipole field
-    (the north-star lattice at L = (128, 128, 64), open boundaries), as a plain record."""
+    (the 1M-spin dipole lattice at L = (128, 128, 64), open boundaries), as a plain record."""
     L = tuple(int(x) for x in L)
     xadj, adj, val = sc_csr(L, J, mu, pbc)
     nr, mesh = dipole_nr(L, abc)

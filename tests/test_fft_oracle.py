@@ -1,5 +1,5 @@
 """Pins of the FFT restatement (oracle/fft_oracle.py) that the CPU baseline and the bench's
-reference arm time on the north-star lattice: its lattice builder against the reference's own
+reference arm time on the sc 128x128x64 dipole lattice: its lattice builder against the reference's own
 CSR assembly and the library's builder, and its FFT long-range field and Heun step against the
 direct-sum oracle (oracle/asd_oracle.c)."""
 import numpy as np

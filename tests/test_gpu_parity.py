@@ -3,7 +3,7 @@
 Tolerances:
   FP64 plain form: bit-exact (identical operation order, no FMA contraction, same noise);
   fused FP64 form: max|dS| <= 1e-10;
-  FP32 form:       max|dS| <= 1e-5 (north-star bound for the FP32 state vs FP64);
+  FP32 form:       max|dS| <= 1e-5 (the accuracy bound for the FP32 state vs FP64);
   FFT paths (cuFFT rounding): FP64 <= 1e-10, FP32 <= 1e-5.
 """
 import numpy as np

@@ -6,7 +6,7 @@
   CUDA kernels (src/cuint.cu, src/cufields.cu launched in the order of src/cuda.cu:43-258); the
   fused FP64 form within 1e-8 of the oracle; the FP32 form within 1e-5 after 3,000 steps and
   1e-4 after 10^4 (its per-step rounding, ~1e-10, grows with the trajectory's sensitivity).
-* The north-star lattice (sc 128x128x64, open, CSR NN exchange + FFT dipole every step), T = 0,
+* The 1M-spin dipole lattice (sc 128x128x64, open, CSR NN exchange + FFT dipole every step), T = 0,
   against the FP64 plain form: the FP32 form within 1e-5 up to 3,000 steps; after 10^4 steps the
   fused FP64 form (FP64 state and fields, FP32 dipole transform) within 2e-5 (measured 1.1e-5:
   the FP32 rounding of N_k and of the transform) and the FP32 form within 1e-3 (measured 2.0e-4).
@@ -77,7 +77,7 @@ def test_config0_full_length(gpu):
             rc.close()
 
 
-def test_north_star_accuracy_1e4(gpu):
+def test_sc128x128x64_dipole_accuracy_1e4(gpu):
     s = LT.sc_ferromagnet((128, 128, 64), pbc=(0, 0, 0), dipole=True)
     S0 = LT.random_spins(s.nspins, 0)
     S1 = S0.copy()
@@ -99,7 +99,7 @@ def test_north_star_accuracy_1e4(gpu):
         ectrl = maxdiff(hs["ctrl"].get_spins(), ref)
         efused = maxdiff(hs["fused"].get_spins(), ref)
         e32b = maxdiff(hs["fp32"].get_spins(), ref)
-        print(f"north star, 10^4 steps: fused FP64 {efused:.3e}, FP32 {e32b:.3e} (3000 steps: {e32:.3e}), "
+        print(f"sc 128x128x64 dipole, 10^4 steps: fused FP64 {efused:.3e}, FP32 {e32b:.3e} (3000 steps: {e32:.3e}), "
               f"FP64 control {ectrl:.3e}")
         assert ectrl <= 1e-9, ectrl
         assert efused <= 2e-5, efused

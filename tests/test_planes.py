@@ -1,6 +1,6 @@
 """Parity of the long-range field's plane kernels (z+y forward, x + N_k product + inverse x,
 inverse y+z) with the FP64 oracle: the direct-sum oracle on small lattices, the FFT restatement
-(itself pinned against the direct sum) on the north-star lattice, and the cuFFT (x, y) passes
+(itself pinned against the direct sum) on the sc 128x128x64 dipole lattice, and the cuFFT (x, y) passes
 the plane kernels replace.
 
 Tolerances: FP32 form max|dS| <= 1e-5 (and <= 1e-6 against the cuFFT passes, the same
@@ -118,8 +118,8 @@ def test_planes_field_readback(gpu):
         assert maxdiff(hg, ho) <= 1e-5 * np.abs(ho).max(), (prec, maxdiff(hg, ho))
 
 
-def test_planes_north_star_lattice_against_fft_restatement(gpu):
-    """The north-star lattice itself (sc 128x128x64, mesh 256x256x128), 10 steps, against the FFT
+def test_planes_sc128x128x64_lattice_against_fft_restatement(gpu):
+    """The 1M-spin dipole lattice (sc 128x128x64, mesh 256x256x128), 10 steps, against the FFT
     restatement of the step on the host."""
     s = LT.sc_ferromagnet((128, 128, 64), pbc=(0, 0, 0), dipole=True)
     S0 = LT.random_spins(s.nspins, 0)
