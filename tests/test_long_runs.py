@@ -1,6 +1,6 @@
 """Long runs at the sizes and lengths the benchmark configurations state.
 
-* Configuration 0 exactly: simple cubic 16^3 (4,096 spins), periodic, NN exchange in CSR, K1u along
+* Simple cubic 16^3 (4,096 spins), periodic, NN exchange in CSR, K1u along
   z, lambda = 0.1, dt = 1e-16 s, Heun, T = 0, 10^4 steps from uniformly random spins.  The FP64
   plain form must equal the FP64 oracle bit for bit and stay within 1e-10 of the reference's own
   CUDA kernels (src/cuint.cu, src/cufields.cu launched in the order of src/cuda.cu:43-258); the
@@ -8,8 +8,8 @@
   1e-4 after 10^4 (its per-step rounding, ~1e-10, grows with the trajectory's sensitivity).
 * The 1M-spin dipole lattice (sc 128x128x64, open, CSR NN exchange + FFT dipole every step), T = 0,
   against the FP64 plain form: the FP32 form within 1e-5 up to 3,000 steps; after 10^4 steps the
-  fused FP64 form (FP64 state and fields, FP32 dipole transform) within 2e-5 (measured 1.1e-5:
-  the FP32 rounding of N_k and of the transform) and the FP32 form within 1e-3 (measured 2.0e-4).
+  fused FP64 form (FP64 state and fields, FP32 dipole transform) within 2e-5 (measured 1.15e-5:
+  the FP32 rounding inside the transform passes) and the FP32 form within 1e-3 (measured 1.9e-4).
   Beside them, the FP64 plain form started from spins perturbed by 1e-15 measures how far the
   trajectory itself amplifies a difference: it stays below 1e-9 (measured 2.7e-11), so the FP32
   form's 2e-4 is its own arithmetic (FP32 neighbour spins, fields and torque; the fused FP64
@@ -36,7 +36,7 @@ def run(s, steps, precision, S0, **kw):
         return h.get_spins()
 
 
-def test_config0_full_length(gpu):
+def test_sc16_heun_full_length(gpu):
     s = LT.sc_ferromagnet(16)
     S0 = LT.random_spins(s.nspins, 0)
     o = O.Oracle(s, dt=1e-16)
@@ -63,7 +63,7 @@ def test_config0_full_length(gpu):
             ef = maxdiff(hs["fused"].get_spins(), ref)
             e32 = maxdiff(hs["fp32"].get_spins(), ref)
             er = maxdiff(plain, rc.spins()) if rc else 0.0
-            print(f"config 0, {cp} steps: fused FP64 {ef:.3e}, FP32 {e32:.3e}, reference CUDA kernels {er:.3e}")
+            print(f"sc 16^3, {cp} steps: fused FP64 {ef:.3e}, FP32 {e32:.3e}, reference CUDA kernels {er:.3e}")
             assert er <= 1e-10, (cp, er)
             assert ef <= 1e-8, (cp, ef)
             if cp == 3000:
