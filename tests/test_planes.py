@@ -148,3 +148,23 @@ def test_planes_shared_memory_limit_per_kernel(gpu):
         g, tune = run(s, 10, A.FP32, A.FLAG_COMPENSATED)
         assert PLANES in tune, tune
         assert maxdiff(g, o) <= 1e-5, (L, maxdiff(g, o))
+
+
+@pytest.mark.parametrize("update", [1, 2])
+def test_planes_dipole_finite_temperature(gpu, update):
+    """The plane-kernel dipole field at T = 300 K against the direct-sum oracle drawing the same
+    Philox noise: the thermal field and the held long-range field together, with the dipole
+    refreshed every step and every second step."""
+    s = LT.sc_ferromagnet((8, 8, 4), pbc=(0, 0, 0), dipole=True, T=300.0)
+    S0 = LT.random_spins(s.nspins, 3)
+    o = O.Oracle(s, update=update, seed=7)
+    o.set_spins(S0)
+    o.step(40)
+    ref = o.spins()
+    for prec, flags, tol in ((A.FP32, A.FLAG_COMPENSATED, 1e-5), (A.FP64_FUSED, 0, 1e-8)):
+        with A.Handle(A.RunParams(precision=prec, flags=flags, update=update, seed=7), s) as h:
+            h.set_spins(S0)
+            h.step(40)
+            assert PLANES in h.tuning(), h.tuning()
+            err = maxdiff(h.get_spins(), ref)
+        assert err <= tol, (prec, err)
