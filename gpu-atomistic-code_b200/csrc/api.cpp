@@ -67,6 +67,7 @@ void free_all(asd_handle* h) {
         F(h->nzf[c]); F(h->nzd[c]);
         for (int q = 0; q < 6; q++) { F(h->kf[q][c]); F(h->kd[q][c]); }
     }
+    if (h->h_err) cudaFreeHost(h->h_err);
     F(h->d_err); F(h->d_aos); F(h->d_check); F(h->d_rep_of_tile); F(h->d_ttm); F(h->d_q4ptr); F(h->d_q4jkl);
     F(h->sell.lwords); F(h->sell.span_ptr); F(h->sell.spans);
     F(h->sell.slice_ptr); F(h->sell.a); F(h->sell.b); F(h->sell.c); F(h->sell.col); F(h->sell.val);
@@ -1054,6 +1055,7 @@ int asd_create(const asd_params* pp, const asd_system* sys, uint32_t nsys, asd_h
         CK(cudaEventCreate(&h->kev[1]));
         h->d_err = dalloc<uint32_t>(1);
         h->sell.err = h->d_err;
+        CK(cudaHostAlloc(reinterpret_cast<void**>(&h->h_err), sizeof(uint32_t), cudaHostAllocDefault));
         if (!plain) {
             if (p.flags & ASD_FLAG_AUTOTUNE) autotune(h);
             else configure_stage(h, 256, 1);
@@ -1291,9 +1293,11 @@ int asd_sync(asd_handle* h) {
     if (!h) return ASD_EINVAL;
     try {
         CK(cudaSetDevice(h->device));
-        CK(cudaStreamSynchronize(h->stream));
+        // the error bits ride the stream behind its work: one copy, one wait
         uint32_t e = 0;
-        if (h->d_err) CK(cudaMemcpy(&e, h->d_err, sizeof e, cudaMemcpyDeviceToHost));
+        if (h->d_err) CK(cudaMemcpyAsync(h->h_err, h->d_err, sizeof e, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->d_err) e = *h->h_err;
         if (e & 2u) {
             CK(cudaMemset(h->d_err, 0, sizeof(uint32_t)));
             throw Fail{ASD_ETIMEOUT, "a long-range transform block's bulk-copy wait ran out; the long-range field of "
@@ -1668,8 +1672,18 @@ int asd_magnetisation(asd_handle* h, double* out, size_t out_len) {
     try {
         REQUIRE(out && out_len >= (size_t)h->nrep * h->nsub * 3, "output must hold nrep*nsub*3 doubles");
         CK(cudaSetDevice(h->device));
-        CK(launch_magnetisation(h));
-        CK(cudaMemcpyAsync(out, h->d_mag, (size_t)h->nrep * h->nsub * 3 * 8, cudaMemcpyDeviceToHost, h->stream));
+        // a page-locked caller buffer this device can address takes the means straight from the
+        // kernel; any other buffer gets them by a copy
+        double* hout = nullptr;
+        cudaPointerAttributes pa{};
+        if (cudaPointerGetAttributes(&pa, out) == cudaSuccess) {
+            if (pa.type == cudaMemoryTypeHost && pa.devicePointer) hout = static_cast<double*>(pa.devicePointer);
+        } else {
+            (void)cudaGetLastError();
+        }
+        CK(launch_magnetisation(h, hout));
+        if (!hout)
+            CK(cudaMemcpyAsync(out, h->d_mag, (size_t)h->nrep * h->nsub * 3 * 8, cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     } catch (const Fail& f) { return fail(h, f); }
     return ASD_OK;

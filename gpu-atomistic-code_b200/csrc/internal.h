@@ -48,7 +48,7 @@ struct SellDev {
     uint4* spans = nullptr;          // (start, len, off, 0) in elements
     uint32_t spin_slots = 0, spin_block = 0;
 };
-constexpr uint32_t MAG_CHUNK = 1024;  // spins per block of the magnetisation reduction
+constexpr uint32_t MAG_CHUNK = 2048;  // spins per block of the magnetisation reduction
 constexpr uint32_t SPIN_PAD = 8;     // zeroed elements after every gather-source spin array
 
 // Row-aligned DIA, values component-major val[c][d*N+row], c = 3 (diag) or 9;
@@ -192,6 +192,7 @@ struct asd_handle {
     std::vector<uint32_t> h_slice_ptr;   // SELL slice offsets (host copy, for staging capacity)
     std::vector<uint32_t> h_words;       // typed SELL words (host copy, for the local words)
     uint32_t* d_err = nullptr;           // device error bits (staging wait timeouts)
+    uint32_t* h_err = nullptr;           // page-locked host word the error bits are read into
     double* d_aos = nullptr;             // [3N] staging buffer of the spin / field transfers
     unsigned long long* d_check = nullptr; // [2] first non-finite component, first zero-length spin
     uint32_t* d_rep_of_tile = nullptr;   // replica of each 32-spin tile's first spin
@@ -281,7 +282,9 @@ cudaError_t launch_sq_sample(asd_handle* h);
 cudaError_t launch_sq_spectrum(asd_handle* h, int window, double alpha, double beta, uint32_t pixelwidth,
                                double sample_dt, double flo, double fhi, double* d_raw, double* d_smooth,
                                uint32_t* d_peaks);
-cudaError_t launch_magnetisation(asd_handle* h);
+// hout: the device address of a page-locked host buffer the means are also written to (the
+// kernel stores them there itself, so no copy follows), or nullptr.
+cudaError_t launch_magnetisation(asd_handle* h, double* hout = nullptr);
 cudaError_t launch_thermal_normals(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, double* d_out,
                                    cudaStream_t st);
 cudaError_t launch_thermal_normals_f(uint64_t seed, uint32_t stream, uint64_t step, uint32_t n, float* d_out,

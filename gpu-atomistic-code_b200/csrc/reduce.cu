@@ -11,157 +11,254 @@ namespace {
 inline unsigned nb(size_t n, int b) { return (unsigned)((n + b - 1) / b); }
 constexpr int MAG_BLOCK = 256;
 
-__device__ __forceinline__ double block_sum(double v, double* sm) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+// Sums N values over the block together (one shared-memory round for all N); the totals are
+// valid in thread 0.  The order is fixed, so the result does not depend on timing.  sm holds
+// N * 32 doubles.
+template <int N>
+__device__ __forceinline__ void block_sum_n(double (&v)[N], double* sm) {
+#pragma unroll
+    for (int k = 0; k < N; k++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
     __syncthreads();
-    if (l == 0) sm[w] = v;
-    __syncthreads();
-    double r = 0.0;
-    if (w == 0) {
-        r = l < (int)(blockDim.x >> 5) ? sm[l] : 0.0;
-        for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+    if (l == 0) {
+#pragma unroll
+        for (int k = 0; k < N; k++) sm[k * 32 + w] = v[k];
     }
-    return r;
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int k = 0; k < N; k++) {
+            double r = l < nw ? sm[k * 32 + l] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) r += __shfl_down_sync(0xffffffffu, r, o);
+            v[k] = r;
+        }
+    }
 }
+
+// Outputs the last partial block forms by itself (more: a separate mag_final launch).
+constexpr uint32_t MAG_FINISH_MAX = 12;
 
 struct MagFinish {
     uint32_t* cnt;              // block ticket counter (nullptr: mag_final forms the means)
     uint32_t nrep;
     const double* inv_count;    // 1 / spins per (replica, sublattice)
     double* out;                // means [nrep][nsub][3]
+    double* hout;               // the caller's page-locked host buffer (device address), or nullptr
 };
+
+// The means from the chunk partials, by one block: thread t adds the words t, t + blockDim, ...
+// of each replica's [chunk][sublattice][component] run of partials to the accumulator of the
+// word's output (NQ accumulators, at least nrep * nsub * 3), then one block sum of them all.
+template <int NQ>
+__device__ __forceinline__ void mag_sum_outputs(const MagFinish& f, uint32_t nsub, uint32_t nchunk,
+                                                const double* part, double* sm) {
+    double acc[NQ];
+#pragma unroll
+    for (int k = 0; k < NQ; k++) acc[k] = 0.0;
+    const uint32_t w = nsub * 3, m = nchunk * w;
+    for (uint32_t r = 0; r < f.nrep; r++) {
+        const double* p = part + (size_t)r * m;
+#pragma unroll 4
+        for (uint32_t e = threadIdx.x; e < m; e += blockDim.x) {
+            const double v = __ldcg(p + e);
+            const uint32_t q = r * w + e % w;
+#pragma unroll
+            for (uint32_t k = 0; k < (uint32_t)NQ; k++)
+                if (k == q) acc[k] += v;
+        }
+    }
+    block_sum_n<NQ>(acc, sm);
+    if (threadIdx.x == 0) {
+        const uint32_t nq = f.nrep * w;
+#pragma unroll
+        for (uint32_t k = 0; k < (uint32_t)NQ; k++) {
+            if (k < nq) {
+                const double mq = acc[k] * f.inv_count[k / 3];
+                f.out[k] = mq;
+                if (f.hout) f.hout[k] = mq;
+            }
+        }
+    }
+}
 
 // The last block of a partial-sum launch to finish (ticket on *cnt) also forms the means:
 // out[q] = inv_count * (the chunk partials of output q summed by the block in a fixed order),
-// the same whatever the order the blocks finish in; it then rearms the counter.  Used
-// when the outputs are few (cnt == nullptr: a separate mag_final launch does it).
-__device__ __forceinline__ void mag_finish_last(uint32_t* cnt, uint32_t nblocks, uint32_t nrep, uint32_t nsub,
-                                                uint32_t nchunk, const double* part, const double* inv_count,
-                                                double* out, double* sm) {
-    if (!cnt) return;
+// the same whatever the order the blocks finish in; it then rearms the counter.  Every caller
+// stores its block's partials from thread 0.
+__device__ __forceinline__ void mag_finish_last(const MagFinish& f, uint32_t nblocks, uint32_t nsub, uint32_t nchunk,
+                                                const double* part, double* sm) {
+    if (!f.cnt) return;
     __shared__ uint32_t last;
-    __threadfence();                                   // this block's partials before its ticket
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(cnt, 1u) == nblocks - 1 ? 1u : 0u;
+    // thread 0 stored this block's partials: its ticket, a release-acquire add, orders them
+    // before the count and, in the last block, every earlier block's partials before the reads
+    // below (the block barrier passes that on to the other threads)
+    if (threadIdx.x == 0) {
+        uint32_t old;
+        asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(old) : "l"(f.cnt) : "memory");
+        last = old == nblocks - 1 ? 1u : 0u;
+    }
     __syncthreads();
     if (!last) return;
-    __threadfence();
-    // the whole block per output: thread t sums the chunks t, t + blockDim, ..., then a block sum
-    for (uint32_t q = 0; q < nrep * nsub * 3; q++) {
-        const uint32_t comp = q % 3, s = (q / 3) % nsub, r = q / (3 * nsub);
-        double acc = 0.0;
-        for (uint32_t ch = threadIdx.x; ch < nchunk; ch += blockDim.x)
-            acc += __ldcg(part + (((size_t)r * nchunk + ch) * nsub + s) * 3 + comp);
-        const double t = block_sum(acc, sm);
-        if (threadIdx.x == 0) out[q] = t * inv_count[r * nsub + s];
-    }
-    if (threadIdx.x == 0) *cnt = 0;
+    const uint32_t nq = f.nrep * nsub * 3;
+    if (nq <= 3) mag_sum_outputs<3>(f, nsub, nchunk, part, sm);
+    else if (nq <= 6) mag_sum_outputs<6>(f, nsub, nchunk, part, sm);
+    else mag_sum_outputs<MAG_FINISH_MAX>(f, nsub, nchunk, part, sm);
+    if (threadIdx.x == 0) *f.cnt = 0;
 }
 
-// Partial sums of S over one chunk of one replica, per sublattice, in FP64 and
-// a fixed reduction order (deterministic): part[((r*nchunk + c)*nsub + s)*3 + comp].
+// Sixteen-byte vector of spin components: 4 floats or 2 doubles.
+template <typename R> struct Vec16;
+template <> struct Vec16<float> {
+    static constexpr uint32_t n = 4;
+    __device__ static void load(const float* p, double (&o)[4]) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+        o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+    }
+};
+template <> struct Vec16<double> {
+    static constexpr uint32_t n = 2;
+    __device__ static void load(const double* p, double (&o)[2]) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+        o[0] = v.x; o[1] = v.y;
+    }
+};
+
+// Partial sums of S over one chunk of one replica for NS >= nsub sublattices in one pass,
+// in FP64 and a fixed order (deterministic): part[((r*nchunk + c)*nsub + s)*3 + comp].  A
+// whole chunk that starts on a 16-byte boundary is read with one vector load per array and
+// thread per round (all of a thread's loads in flight together); other chunks spin by spin.
+template <typename R, int NS>
+__global__ void __launch_bounds__(MAG_BLOCK, 4)
+    mag_partial_ns(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom, const R* __restrict__ sx,
+                   const R* __restrict__ sy, const R* __restrict__ sz, const float* __restrict__ lx,
+                   const float* __restrict__ ly, const float* __restrict__ lz, uint32_t nchunk,
+                   double* __restrict__ part, MagFinish f) {
+    __shared__ double sm[MAG_FINISH_MAX * 32];
+    const uint32_t r = blockIdx.y, ch = blockIdx.x;
+    const uint32_t beg = c.rep_off[r] + ch * MAG_CHUNK;
+    const uint32_t end = min(c.rep_off[r + 1], beg + MAG_CHUNK);
+    double a[3 * NS];
+#pragma unroll
+    for (int k = 0; k < 3 * NS; k++) a[k] = 0.0;
+    auto add = [&](uint32_t i, double v0, double v1, double v2) {
+        const uint32_t s = NS == 1 ? 0u : sub_of_atom[atom_of(c, i)];
+#pragma unroll
+        for (int q = 0; q < NS; q++)
+            if (s == (uint32_t)q) { a[3 * q] += v0; a[3 * q + 1] += v1; a[3 * q + 2] += v2; }
+    };
+    constexpr uint32_t V = Vec16<R>::n;
+    constexpr uint32_t ROUNDS = MAG_CHUNK / (V * MAG_BLOCK);
+    static_assert(ROUNDS * V * MAG_BLOCK == MAG_CHUNK, "a chunk is a whole number of vector rounds");
+    const uintptr_t ptrs = reinterpret_cast<uintptr_t>(sx) | reinterpret_cast<uintptr_t>(sy) |
+                           reinterpret_cast<uintptr_t>(sz) | reinterpret_cast<uintptr_t>(lx) |
+                           reinterpret_cast<uintptr_t>(ly) | reinterpret_cast<uintptr_t>(lz);
+    if (end - beg == MAG_CHUNK && beg % V == 0 && (ptrs & 15u) == 0 && blockDim.x == MAG_BLOCK) {
+#pragma unroll
+        for (uint32_t k = 0; k < ROUNDS; k++) {
+            const uint32_t i = beg + V * (threadIdx.x + k * MAG_BLOCK);
+            double x[V], y[V], z[V];
+            Vec16<R>::load(sx + i, x); Vec16<R>::load(sy + i, y); Vec16<R>::load(sz + i, z);
+            if constexpr (sizeof(R) == 4) {
+                if (lx) {       // the low words of the compensated FP32 form
+                    double u[V], v[V], w[V];
+                    Vec16<float>::load(lx + i, u); Vec16<float>::load(ly + i, v); Vec16<float>::load(lz + i, w);
+#pragma unroll
+                    for (uint32_t j = 0; j < V; j++) { x[j] += u[j]; y[j] += v[j]; z[j] += w[j]; }
+                }
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < V; j++) add(i + j, x[j], y[j], z[j]);
+        }
+    } else {
+        for (uint32_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
+            double v0 = (double)sx[i], v1 = (double)sy[i], v2 = (double)sz[i];
+            if (lx) { v0 += (double)lx[i]; v1 += (double)ly[i]; v2 += (double)lz[i]; }
+            add(i, v0, v1, v2);
+        }
+    }
+    block_sum_n<3 * NS>(a, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NS; q++) {
+            if ((uint32_t)q < nsub) {
+                double* o = part + (((size_t)r * nchunk + ch) * nsub + q) * 3;
+                o[0] = a[3 * q]; o[1] = a[3 * q + 1]; o[2] = a[3 * q + 2];
+            }
+        }
+    }
+    mag_finish_last(f, gridDim.x * gridDim.y, nsub, nchunk, part, sm);
+}
+
+// Any number of sublattices: one pass over the chunk per sublattice.
 template <typename R>
-__global__ void mag_partial(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
-                            const R* __restrict__ sx, const R* __restrict__ sy, const R* __restrict__ sz,
-                            const float* __restrict__ lx, const float* __restrict__ ly, const float* __restrict__ lz,
-                            uint32_t nchunk, double* __restrict__ part, MagFinish f) {
-    __shared__ double sm[32];
+__global__ void __launch_bounds__(MAG_BLOCK)
+    mag_partial(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom, const R* __restrict__ sx,
+                const R* __restrict__ sy, const R* __restrict__ sz, const float* __restrict__ lx,
+                const float* __restrict__ ly, const float* __restrict__ lz, uint32_t nchunk,
+                double* __restrict__ part, MagFinish f) {
+    __shared__ double sm[MAG_FINISH_MAX * 32];
     const uint32_t r = blockIdx.y, ch = blockIdx.x;
     const uint32_t beg = c.rep_off[r] + ch * MAG_CHUNK;
     const uint32_t end = min(c.rep_off[r + 1], beg + MAG_CHUNK);
     for (uint32_t s = 0; s < nsub; s++) {
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        double a[3] = {0.0, 0.0, 0.0};
         for (uint32_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
             if (sub_of_atom[atom_of(c, i)] != s) continue;
-            a0 += (double)sx[i]; a1 += (double)sy[i]; a2 += (double)sz[i];
-            if (lx) { a0 += (double)lx[i]; a1 += (double)ly[i]; a2 += (double)lz[i]; }
+            a[0] += (double)sx[i]; a[1] += (double)sy[i]; a[2] += (double)sz[i];
+            if (lx) { a[0] += (double)lx[i]; a[1] += (double)ly[i]; a[2] += (double)lz[i]; }
         }
-        const double t0 = block_sum(a0, sm), t1 = block_sum(a1, sm), t2 = block_sum(a2, sm);
+        block_sum_n<3>(a, sm);
         if (threadIdx.x == 0) {
             double* o = part + (((size_t)r * nchunk + ch) * nsub + s) * 3;
-            o[0] = t0; o[1] = t1; o[2] = t2;
+            o[0] = a[0]; o[1] = a[1]; o[2] = a[2];
         }
     }
-    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out, sm);
-}
-
-// One pass over the chunk for up to NS sublattices, each spin added to its own sublattice's
-// register accumulators (the general kernel above re-reads the chunk once per sublattice).
-template <typename R, int NS>
-__global__ void mag_partial_ns(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
-                               const R* __restrict__ sx, const R* __restrict__ sy, const R* __restrict__ sz,
-                               const float* __restrict__ lx, const float* __restrict__ ly,
-                               const float* __restrict__ lz, uint32_t nchunk, double* __restrict__ part,
-                               MagFinish f) {
-    __shared__ double sm[32];
-    const uint32_t r = blockIdx.y, ch = blockIdx.x;
-    const uint32_t beg = c.rep_off[r] + ch * MAG_CHUNK;
-    const uint32_t end = min(c.rep_off[r + 1], beg + MAG_CHUNK);
-    double a[NS][3];
-#pragma unroll
-    for (int q = 0; q < NS; q++) a[q][0] = a[q][1] = a[q][2] = 0.0;
-    for (uint32_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
-        const uint32_t s = NS == 1 ? 0u : sub_of_atom[atom_of(c, i)];
-        double v0 = (double)sx[i], v1 = (double)sy[i], v2 = (double)sz[i];
-        if (lx) { v0 += (double)lx[i]; v1 += (double)ly[i]; v2 += (double)lz[i]; }
-#pragma unroll
-        for (int q = 0; q < NS; q++)
-            if (s == (uint32_t)q) { a[q][0] += v0; a[q][1] += v1; a[q][2] += v2; }
-    }
-    for (uint32_t q = 0; q < nsub; q++) {
-        double t[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            double v = 0.0;
-#pragma unroll
-            for (int qq = 0; qq < NS; qq++) if ((uint32_t)qq == q) v = a[qq][k];
-            t[k] = block_sum(v, sm);
-        }
-        if (threadIdx.x == 0) {
-            double* o = part + (((size_t)r * nchunk + ch) * nsub + q) * 3;
-            o[0] = t[0]; o[1] = t[1]; o[2] = t[2];
-        }
-    }
-    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out, sm);
+    mag_finish_last(f, gridDim.x * gridDim.y, nsub, nchunk, part, sm);
 }
 
 // Plain form: AoS doubles.
-__global__ void mag_partial_aos(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
-                                const double* __restrict__ s3, uint32_t nchunk, double* __restrict__ part,
-                                MagFinish f) {
-    __shared__ double sm[32];
+__global__ void __launch_bounds__(MAG_BLOCK)
+    mag_partial_aos(StepConst c, uint32_t nsub, const uint32_t* __restrict__ sub_of_atom,
+                    const double* __restrict__ s3, uint32_t nchunk, double* __restrict__ part, MagFinish f) {
+    __shared__ double sm[MAG_FINISH_MAX * 32];
     const uint32_t r = blockIdx.y, ch = blockIdx.x;
     const uint32_t beg = c.rep_off[r] + ch * MAG_CHUNK;
     const uint32_t end = min(c.rep_off[r + 1], beg + MAG_CHUNK);
     for (uint32_t s = 0; s < nsub; s++) {
-        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        double a[3] = {0.0, 0.0, 0.0};
         for (uint32_t i = beg + threadIdx.x; i < end; i += blockDim.x) {
             if (sub_of_atom[atom_of(c, i)] != s) continue;
-            a0 += s3[3 * (size_t)i]; a1 += s3[3 * (size_t)i + 1]; a2 += s3[3 * (size_t)i + 2];
+            a[0] += s3[3 * (size_t)i]; a[1] += s3[3 * (size_t)i + 1]; a[2] += s3[3 * (size_t)i + 2];
         }
-        const double t0 = block_sum(a0, sm), t1 = block_sum(a1, sm), t2 = block_sum(a2, sm);
+        block_sum_n<3>(a, sm);
         if (threadIdx.x == 0) {
             double* o = part + (((size_t)r * nchunk + ch) * nsub + s) * 3;
-            o[0] = t0; o[1] = t1; o[2] = t2;
+            o[0] = a[0]; o[1] = a[1]; o[2] = a[2];
         }
     }
-    mag_finish_last(f.cnt, gridDim.x * gridDim.y, f.nrep, nsub, nchunk, part, f.inv_count, f.out, sm);
+    mag_finish_last(f, gridDim.x * gridDim.y, nsub, nchunk, part, sm);
 }
 
 __global__ void mag_final(uint32_t nrep, uint32_t nsub, uint32_t nchunk, const double* __restrict__ part,
-                          const double* __restrict__ inv_count, double* __restrict__ out) {
+                          const double* __restrict__ inv_count, double* __restrict__ out, double* hout) {
     // one block per (replica, sublattice, component): its threads stride over the chunks, then a
     // block sum (fixed order, so the result does not depend on timing)
     __shared__ double sm[32];
     const uint32_t q = blockIdx.x;
     if (q >= nrep * nsub * 3) return;
     const uint32_t comp = q % 3, s = (q / 3) % nsub, r = q / (3 * nsub);
-    double acc = 0.0;
+    double acc[1] = {0.0};
     for (uint32_t ch = threadIdx.x; ch < nchunk; ch += blockDim.x)
-        acc += part[(((size_t)r * nchunk + ch) * nsub + s) * 3 + comp];
-    const double t = block_sum(acc, sm);
-    if (threadIdx.x == 0) out[q] = t * inv_count[r * nsub + s];
+        acc[0] += part[(((size_t)r * nchunk + ch) * nsub + s) * 3 + comp];
+    block_sum_n<1>(acc, sm);
+    if (threadIdx.x == 0) {
+        const double mq = acc[0] * inv_count[r * nsub + s];
+        out[q] = mq;
+        if (hout) hout[q] = mq;
+    }
 }
 
 template <typename R>
@@ -381,41 +478,48 @@ cudaError_t launch_field_only(asd_handle* h, double* d_out) {
     return field_t<double>(h, d_out);
 }
 
-cudaError_t launch_magnetisation(asd_handle* h) {
+template <typename R>
+void launch_mag_partial(asd_handle* h, dim3 grid, R* const s[3], const float* lx, const float* ly, const float* lz,
+                        const MagFinish& f) {
+    const uint32_t nsub = h->nsub;
+    const uint32_t* sub = h->d_sub_of_atom;
+    if (nsub == 1)
+        mag_partial_ns<R, 1><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub, s[0], s[1], s[2], lx, ly, lz, grid.x,
+                                                                h->d_magpart, f);
+    else if (nsub == 2)
+        mag_partial_ns<R, 2><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub, s[0], s[1], s[2], lx, ly, lz, grid.x,
+                                                                h->d_magpart, f);
+    else if (nsub <= 4)
+        mag_partial_ns<R, 4><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub, s[0], s[1], s[2], lx, ly, lz, grid.x,
+                                                                h->d_magpart, f);
+    else
+        mag_partial<R><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub, s[0], s[1], s[2], lx, ly, lz, grid.x,
+                                                          h->d_magpart, f);
+}
+
+cudaError_t launch_magnetisation(asd_handle* h, double* hout) {
     const uint32_t nsub = h->nsub;
     uint32_t maxrep = 0;
     for (uint32_t r = 0; r < h->nrep; r++) maxrep = std::max(maxrep, h->h_rep_off[r + 1] - h->h_rep_off[r]);
     const uint32_t nchunk = (maxrep + MAG_CHUNK - 1) / MAG_CHUNK;
     dim3 grid(nchunk ? nchunk : 1, h->nrep);
-    const uint32_t* sub_of_atom = h->d_sub_of_atom;
     const double* inv_count = h->d_inv_count;
     // few outputs: the last partial block forms the means (one launch); else mag_final does
     const uint32_t nq = h->nrep * nsub * 3;
-    const MagFinish f{nq <= 12 ? h->d_magcnt : nullptr, h->nrep, inv_count, h->d_mag};
+    const MagFinish f{nq <= MAG_FINISH_MAX ? h->d_magcnt : nullptr, h->nrep, inv_count, h->d_mag, hout};
     if (h->p.precision == ASD_FP64_PLAIN) {
-        mag_partial_aos<<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->p_s, grid.x, h->d_magpart, f);
+        mag_partial_aos<<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, h->d_sub_of_atom, h->p_s, grid.x,
+                                                           h->d_magpart, f);
     } else if (h->p.precision == ASD_FP32) {
         const bool comp = (h->p.flags & ASD_FLAG_COMPENSATED) != 0;
-        const float* lo[3] = {comp ? h->sl[0] : nullptr, comp ? h->sl[1] : nullptr, comp ? h->sl[2] : nullptr};
-        if (nsub == 1)
-            mag_partial_ns<float, 1><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1],
-                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart, f);
-        else if (nsub == 2)
-            mag_partial_ns<float, 2><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1],
-                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart, f);
-        else if (nsub <= 4)
-            mag_partial_ns<float, 4><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1],
-                                                                        h->sf[2], lo[0], lo[1], lo[2], grid.x, h->d_magpart, f);
-        else
-            mag_partial<float><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sf[0], h->sf[1], h->sf[2],
-                                                                 lo[0], lo[1], lo[2], grid.x, h->d_magpart, f);
+        launch_mag_partial<float>(h, grid, h->sf, comp ? h->sl[0] : nullptr, comp ? h->sl[1] : nullptr,
+                                  comp ? h->sl[2] : nullptr, f);
     } else {
-        mag_partial<double><<<grid, MAG_BLOCK, 0, h->stream>>>(h->sc, nsub, sub_of_atom, h->sd[0], h->sd[1], h->sd[2],
-                                                              nullptr, nullptr, nullptr, grid.x, h->d_magpart, f);
+        launch_mag_partial<double>(h, grid, h->sd, nullptr, nullptr, nullptr, f);
     }
     h->launches += 1;
     if (!f.cnt) {
-        mag_final<<<nq, 128, 0, h->stream>>>(h->nrep, nsub, grid.x, h->d_magpart, inv_count, h->d_mag);
+        mag_final<<<nq, 128, 0, h->stream>>>(h->nrep, nsub, grid.x, h->d_magpart, inv_count, h->d_mag, hout);
         h->launches += 1;
     }
     return cudaGetLastError();

@@ -1,7 +1,8 @@
 """asd_magnetisation against the per-(replica, sublattice) means of the spins computed on the
 host, in every form: one replica (the last partial-sum block forms the means, one launch), two
 sublattices, a few replicas (still one launch), many replicas (a separate reduction launch), and
-calls repeated between steps (the block ticket rearms itself)."""
+calls repeated between steps (the block ticket rearms itself); into pageable and page-locked
+host buffers."""
 import numpy as np
 import pytest
 
@@ -34,15 +35,23 @@ CASES = {
 
 @pytest.mark.parametrize("case", list(CASES))
 @pytest.mark.parametrize("prec", [A.FP64_PLAIN, A.FP32, A.FP64_FUSED])
-def test_magnetisation_matches_host_means(gpu, case, prec):
+@pytest.mark.parametrize("buf", ["pageable", "page-locked"])
+def test_magnetisation_matches_host_means(gpu, case, prec, buf):
+    """A page-locked output buffer takes the means from the kernel itself (no copy): it is
+    filled with NaN before every call, so a store that never came shows."""
+    import torch
+
     systems = CASES[case]()
     n = sum(s.nspins for s in systems)
     flags = A.FLAG_COMPENSATED if prec == A.FP32 else 0
     with A.Handle(A.RunParams(precision=prec, flags=flags), systems) as h:
         h.set_spins(LT.random_spins(n, 9))
+        nq = h.nrep * h.nsub * 3
+        out = torch.empty(nq, dtype=torch.float64).pin_memory().numpy() if buf == "page-locked" else np.empty(nq)
         for _ in range(3):
             h.step(2)
-            got = h.magnetisation()
+            out[:] = np.nan
+            got = h.magnetisation(out)
             want = host_means(systems, h.get_spins())
             assert got.shape == want.shape, (got.shape, want.shape)
             err = float(np.abs(got - want).max())
