@@ -81,9 +81,13 @@ __device__ __forceinline__ double site_scale_d(const double* dyn, uint64_t t, do
     return sc;
 }
 
-// Programmatic dependent launch, at the top of every step kernel: wait until the previous
-// kernel of the stream has completed and its memory is visible (a no-op for a kernel launched
-// without the attribute), then let the next kernel's blocks launch (they wait the same way).
+// Programmatic dependent launch, in every step kernel before its first access to memory that
+// an earlier kernel of the stream writes or reads: wait until the previous kernel has completed
+// and its memory is visible (a no-op for a kernel launched without the attribute), then let the
+// next kernel's blocks launch (they wait the same way).  Before it a kernel touches only
+// set-up data - twiddles, N_k tiles, the exchange words, tables and spans, the mesh index -
+// which are written at creation and complete (synchronous uploads, a device-wide free) before
+// the first step, so its prologue overlaps the previous kernel's last blocks.
 __device__ __forceinline__ void pdl_enter() {
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");

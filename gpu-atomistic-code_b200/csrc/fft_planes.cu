@@ -141,7 +141,6 @@ struct RowGroup {
 template <int Z1, int Z2, int R1, int R2>
 __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const float* __restrict__ mr, float2* __restrict__ yk,
                                                        const PlaneArgs A) {
-    pdl_enter();
     using G = ZYGeom<Z1, Z2, R1, R2>;
     constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
     constexpr uint32_t CL = G::CL, HY = G::HY, LDZ = G::LDZ, HK = G::HK, KPB = G::KPB;
@@ -155,7 +154,8 @@ __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const floa
     float2* twy = twz + 2 * N + 1;                     // M1 y twiddles
     const uint32_t rank = cl.block_rank();
     const uint32_t xl = blockIdx.x / CL, c = blockIdx.y, x = A.bx0 + xl;
-    copy_tw(twz, A.twt, 2 * N + 1 + M1);
+    copy_tw(twz, A.twt, 2 * N + 1 + M1);               // set-up data: before the wait
+    pdl_enter();
     __syncthreads();
     // the box row x of component c from its y = by0 row on: pair n of row yl at rowx[yl N + n]
     const float2* rowx = reinterpret_cast<const float2*>(mr + (size_t)c * A.P) + A.zs + ((size_t)x * M1 + A.by0) * N;
@@ -276,7 +276,6 @@ template <int R1, int R2, bool CPLX>
 __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __restrict__ yk,
                                                                       const void* __restrict__ nkt, const uint32_t Kz,
                                                                       const PlaneArgs A) {
-    pdl_enter();
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ __align__(8) uint64_t bar;
     constexpr uint32_t T = PT;
@@ -296,14 +295,17 @@ __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __
     float2* gy[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) gy[c] = yk + (((size_t)c * Kz + kz) * A.ntile + tile) * slab;
+    // the N_k tile and the twiddles are set-up data: copied before the wait, the spectrum after
     if (tid == 0) {
         mbar_init(&bar, 1);
         mbar_arrive_expect_tx(&bar, ys_bytes + ns_bytes);
-        for (int c = 0; c < 3; c++) bulk_copy_stream(Ys + c * slab, gy[c], slab * 8u, &bar);
         bulk_copy_stream(Nsb, static_cast<const unsigned char*>(nkt) + ((size_t)kz * A.ntile + tile) * ns_bytes,
                          ns_bytes, &bar);
     }
     copy_tw(twx, A.twt + A.twx_off, M0);
+    pdl_enter();
+    if (tid == 0)
+        for (int c = 0; c < 3; c++) bulk_copy_stream(Ys + c * slab, gy[c], slab * 8u, &bar);
     __syncthreads();
     if (__syncthreads_or(!mbar_wait_bounded(&bar, A.wait_once ? 0u : STAGE_WAIT_POLLS))) {
         // the copies did not land in time for some thread: the whole block flags it, leaves this
@@ -410,7 +412,6 @@ __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __
 template <int Z1, int Z2, int R1, int R2>
 __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict__ yk, float* __restrict__ hr,
                                                        const PlaneArgs A) {
-    pdl_enter();
     using G = ZYGeom<Z1, Z2, R1, R2>;
     constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
     constexpr uint32_t CL = G::CL, HY = G::HY, LDZ = G::LDZ, HK = G::HK, KPB = G::KPB;
@@ -424,11 +425,12 @@ __global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict_
     float2* twy = twz + 2 * N + 1;
     const uint32_t rank = cl.block_rank();
     const uint32_t xl = blockIdx.x / CL, c = blockIdx.y, x = A.bx0 + xl;
-    copy_tw(twz, A.twt, 2 * N + 1 + M1);
+    copy_tw(twz, A.twt, 2 * N + 1 + M1);               // set-up data: before the wait
     cluster_arrive_relaxed();
     float2* zb[CL];
 #pragma unroll
     for (uint32_t o = 0; o < CL; o++) zb[o] = cl.map_shared_rank(Zs, o);
+    pdl_enter();
     __syncthreads();
     // inverse y of this block's slots (slot 0: D = G_0 + i G_N of the real planes kz = 0 and N,
     // whose inverse is g_0 + i g_N); every box row's value goes to the Zs of the block owning it

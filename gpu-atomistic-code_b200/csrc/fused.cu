@@ -124,24 +124,17 @@ struct MinBlocks {
 template <typename R, int EX, bool FULL, bool COMP, int K>
 __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL, K>::value)
     stage_kernel(const StepConst c, const SellDev sell, const DiaDev dia, const StageArgs<R> a) {
-    pdl_enter();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t stage_bar;
     R* tab = reinterpret_cast<R*>(smem_raw);
-    if (threadIdx.x == 0 && a.npf) {
-        // the block's rows of every per-spin input: one bulk L2 prefetch each, so the loads
-        // after the exchange gather find them in L2; sizes stop at the last row (whole
-        // 16-byte units), so no prefetch reaches past an array
-        const uint32_t r0 = blockIdx.x * blockDim.x;
-        const uint32_t rows = min(blockDim.x, c.n - r0);
-        const uint32_t bytes = (rows * (uint32_t)sizeof(R)) & ~15u;
-        if (bytes)
-            for (uint32_t q = 0; q < a.npf; q++)
-                bulk_prefetch_l2(static_cast<const char*>(a.pf[q]) + (size_t)r0 * sizeof(R), bytes);
-    }
+    // Until pdl_enter below the block touches only set-up data (the exchange words, the tensor
+    // table, the spans, the mesh index): the copies of the words and the table start while the
+    // previous kernel's last blocks run; the neighbour-spin spans are copied after the wait.
     const uint32_t* staged = nullptr;
     const uint16_t* staged16 = nullptr;
     const R* sspin = nullptr;
+    R* span_dst = nullptr;           // shared-memory spin buffer the span copies fill after the wait
+    uint32_t span0 = 0, nspan = 0;
     uint32_t wbase = 0;
     if constexpr (EX == ASD_EXCH_CSR) {
         if (sell.typed) {
@@ -179,21 +172,12 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL, K>::value)
                             mbar_arrive_expect_tx(&stage_bar, tx);
                         }
                         __syncwarp();
-                        for (uint32_t k = threadIdx.x; k < 2 + 3 * nsp; k += 32) {
-                            if (k == 0) {
-                                bulk_copy_stream(wbuf, sell.lwords16 + wbase, bytes16, &stage_bar);
-                            } else if (k == 1) {
-                                bulk_copy(tab, table_of<R>(sell), tab_bytes, &stage_bar);
-                            } else {
-                                const uint4 sp = sell.spans[sp0 + (k - 2) / 3];
-                                const uint32_t c = (k - 2) % 3;
-                                bulk_copy(sbuf + c * sell.spin_slots + sp.z, a.src.p[c] + sp.x,
-                                          sp.y * (uint32_t)sizeof(R), &stage_bar);
-                            }
-                        }
+                        if (threadIdx.x == 0) bulk_copy_stream(wbuf, sell.lwords16 + wbase, bytes16, &stage_bar);
+                        if (threadIdx.x == 1) bulk_copy(tab, table_of<R>(sell), tab_bytes, &stage_bar);
                     }
                     staged16 = wbuf;
                     sspin = sbuf;
+                    span_dst = sbuf; span0 = sp0; nspan = nsp;
                     tab_staged = true;
                 } else if (!w16 && bytes) {
                     uint32_t* wbuf = reinterpret_cast<uint32_t*>(smem_raw + tb);
@@ -207,21 +191,12 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL, K>::value)
                             mbar_arrive_expect_tx(&stage_bar, tx);
                         }
                         __syncwarp();
-                        for (uint32_t k = threadIdx.x; k < 2 + 3 * nsp; k += 32) {
-                            if (k == 0) {
-                                bulk_copy_stream(wbuf, (nsp ? sell.lwords : sell.typed) + wbase, bytes, &stage_bar);
-                            } else if (k == 1) {
-                                bulk_copy(tab, table_of<R>(sell), tab_bytes, &stage_bar);
-                            } else {
-                                const uint4 sp = sell.spans[sp0 + (k - 2) / 3];
-                                const uint32_t c = (k - 2) % 3;
-                                bulk_copy(sbuf + c * sell.spin_slots + sp.z, a.src.p[c] + sp.x,
-                                          sp.y * (uint32_t)sizeof(R), &stage_bar);
-                            }
-                        }
+                        if (threadIdx.x == 0)
+                            bulk_copy_stream(wbuf, (nsp ? sell.lwords : sell.typed) + wbase, bytes, &stage_bar);
+                        if (threadIdx.x == 1) bulk_copy(tab, table_of<R>(sell), tab_bytes, &stage_bar);
                     }
                     staged = wbuf;
-                    if (nsp) sspin = sbuf;
+                    if (nsp) { sspin = sbuf; span_dst = sbuf; span0 = sp0; nspan = nsp; }
                     tab_staged = true;
                 }
             }
@@ -230,6 +205,28 @@ __global__ void __launch_bounds__(256, MinBlocks<R, EX, FULL, K>::value)
     }
     if constexpr (EX == ASD_EXCH_DIA) {
         if (dia.dtype) load_table<R>(table_of<R>(dia), table_stride<FULL>() *dia.ntypes, tab);
+    }
+    pdl_enter();
+    if constexpr (EX == ASD_EXCH_CSR) {
+        // the neighbour-spin spans: one copy per (span, component), on the staging barrier
+        if (threadIdx.x < 32)
+            for (uint32_t k = threadIdx.x; k < 3 * nspan; k += 32) {
+                const uint4 sp = sell.spans[span0 + k / 3];
+                const uint32_t cc = k % 3;
+                bulk_copy(span_dst + cc * sell.spin_slots + sp.z, a.src.p[cc] + sp.x, sp.y * (uint32_t)sizeof(R),
+                          &stage_bar);
+            }
+    }
+    if (threadIdx.x == 0 && a.npf) {
+        // the block's rows of every per-spin input: one bulk L2 prefetch each, so the loads
+        // after the exchange gather find them in L2; sizes stop at the last row (whole
+        // 16-byte units), so no prefetch reaches past an array
+        const uint32_t r0 = blockIdx.x * blockDim.x;
+        const uint32_t rows = min(blockDim.x, c.n - r0);
+        const uint32_t bytes = (rows * (uint32_t)sizeof(R)) & ~15u;
+        if (bytes)
+            for (uint32_t q = 0; q < a.npf; q++)
+                bulk_prefetch_l2(static_cast<const char*>(a.pf[q]) + (size_t)r0 * sizeof(R), bytes);
     }
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= c.n) return;     // thread 0 of every block has i < n and always waits below
