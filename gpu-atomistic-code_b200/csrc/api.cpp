@@ -85,7 +85,7 @@ void free_all(asd_handle* h) {
     if (L.c2r) cufftDestroy(L.c2r);
     if (L.z2z) cufftDestroy(L.z2z);
     if (L.c2c) cufftDestroy(L.c2c);
-    F(L.k1); F(L.k2); F(L.yk); F(L.nkt); F(L.twt);
+    F(L.k1); F(L.k2); F(L.yk); F(L.nkt); F(L.twt); F(L.xq);
     F(h->sq.idx); F(h->sq.sub); F(h->sq.uo); F(h->sq.kidx); F(h->sq.grid); F(h->sq.series);
     if (h->sq.plan) cufftDestroy(h->sq.plan);
     F(h->d_magpart); F(h->d_mag); F(h->d_magcnt); F(h->d_inv_count); F(h->d_sub_of_atom); F(h->d_stats);

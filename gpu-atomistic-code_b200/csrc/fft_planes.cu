@@ -22,6 +22,9 @@
 #include <algorithm>
 #include <cooperative_groups.h>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace asd {
 namespace {
@@ -47,6 +50,7 @@ struct PlaneArgs {
     uint32_t twx_off;                // offset of the x twiddles in twt (2N + 1 + m1)
     uint32_t* err;                   // device error bits
     uint32_t wait_once;              // test aid: the bulk-copy wait gives up at once (ASD_FLAG_WAIT_TIMEOUT)
+    uint32_t* xq;                    // x-pass item counters (zero between launches): next item, finished blocks
 };
 
 constexpr uint32_t ERR_FFT_TIMEOUT = 2u;
@@ -268,10 +272,18 @@ __global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_zy_fwd(const floa
 }
 
 // ---------------------------------------------------------------- x, N_k product, inverse x
-// Shared memory: Ys [3][bx][PT] (input and output), Ns (N_k tile: 6 x nkx x PT floats or
-// 9 x M0 x PT float2), E (exchange, R1 x (R2 PT + 8) float2), twx [M0].  A real N_k whose every
-// component is even or odd in kx is stored for kx <= M0/2 only (nkx = M0/2 + 1 rows); the rows
-// kx > M0/2 are read at M0 - kx with the component's sign.
+// Shared memory: Ys [3][bx][PT] (input), Ns (N_k tile: 6 x nkx x PT floats or 9 x M0 x PT
+// float2), E (exchange, R1 x (R2 PT + 8) float2), twx [M0].  A real N_k whose every component is
+// even or odd in kx is stored for kx <= M0/2 only (nkx = M0/2 + 1 rows); the rows kx > M0/2 are
+// read at M0 - kx with the component's sign.
+//
+// Persistent: block b starts with the (kz, tile) item b (item = kz * ntile + tile) and takes
+// each further item from a counter (blocks that started late, behind the previous kernel's
+// last blocks, take fewer).  The next item's spectrum is copied into Ys as soon as the forward
+// transform has read it, and its N_k tile into Ns once the product has read that, so both
+// copies run under the product and the inverse transform; the inverse writes its box rows
+// straight to global memory.  One mbarrier, one phase per item.  The last block to finish
+// zeroes the counters for the next launch.
 template <int R1, int R2, bool CPLX>
 __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __restrict__ yk,
                                                                       const void* __restrict__ nkt, const uint32_t Kz,
@@ -283,7 +295,7 @@ __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __
     constexpr uint32_t NQ = CPLX ? 9 : 6;
     constexpr uint32_t NB = CPLX ? 8 : 4;             // bytes per N_k component value
     constexpr uint32_t EP = R2 * T + 8;               // exchange pitch per m (padded: no bank conflicts)
-    const uint32_t tile = blockIdx.x, kz = blockIdx.y;
+    const uint32_t nitems = A.ntile * Kz;
     float2* Ys = reinterpret_cast<float2*>(smraw);
     const uint32_t ys_bytes = 3u * A.bx * T * 8u;
     unsigned char* Nsb = smraw + ((ys_bytes + 15u) & ~15u);
@@ -292,119 +304,144 @@ __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __
     float2* twx = E + R1 * EP;
     const uint32_t tid = threadIdx.x, j = tid % T, r = tid / T;
     const uint32_t slab = A.bx * T;                   // float2 per (c, kz, tile) slab
-    float2* gy[3];
-#pragma unroll
-    for (int c = 0; c < 3; c++) gy[c] = yk + (((size_t)c * Kz + kz) * A.ntile + tile) * slab;
+    // slab of component c of item it: [c][kz][tile] with it = kz * ntile + tile
+    auto slab_of = [&](uint32_t it, uint32_t c) {
+        return yk + ((size_t)c * Kz * A.ntile + it) * slab;
+    };
+    auto nk_of = [&](uint32_t it) { return static_cast<const unsigned char*>(nkt) + (size_t)it * ns_bytes; };
+    const uint32_t polls = A.wait_once ? 0u : STAGE_WAIT_POLLS;
+    __shared__ uint32_t next_item;
+    uint32_t item = blockIdx.x;                       // < nitems: the grid is at most the item count
     // the N_k tile and the twiddles are set-up data: copied before the wait, the spectrum after
     if (tid == 0) {
         mbar_init(&bar, 1);
         mbar_arrive_expect_tx(&bar, ys_bytes + ns_bytes);
-        bulk_copy_stream(Nsb, static_cast<const unsigned char*>(nkt) + ((size_t)kz * A.ntile + tile) * ns_bytes,
-                         ns_bytes, &bar);
+        bulk_copy_stream(Nsb, nk_of(item), ns_bytes, &bar);
     }
     copy_tw(twx, A.twt + A.twx_off, M0);
     pdl_enter();
     if (tid == 0)
-        for (int c = 0; c < 3; c++) bulk_copy_stream(Ys + c * slab, gy[c], slab * 8u, &bar);
+        for (uint32_t c = 0; c < 3; c++) bulk_copy_stream(Ys + c * slab, slab_of(item, c), slab * 8u, &bar);
     __syncthreads();
-    if (__syncthreads_or(!mbar_wait_bounded(&bar, A.wait_once ? 0u : STAGE_WAIT_POLLS))) {
-        // the copies did not land in time for some thread: the whole block flags it, leaves this
-        // tile untransformed, and retires only after the copies into shared memory have finished
-        // (bounded again)
-        if (tid == 0) atomicOr(A.err, ERR_FFT_TIMEOUT);
-        mbar_wait_bounded(&bar, STAGE_WAIT_POLLS);
-        return;
-    }
-    // forward x transform of the three components; thread (j, m) keeps X[c][m + R1 q]
-    float2 X[3][R2];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        if (r < R2) {
-            const uint32_t t = r;
-            float2 v[R1];
-#pragma unroll
-            for (int k = 0; k < R1 / 2; k++) {         // rows x >= M0/2 are zero
-                const uint32_t xx = t + R2 * k;
-                v[k] = xx < A.bx ? Ys[(c * A.bx + xx) * T + j] : make_float2(0.f, 0.f);
-            }
-            dftp<R1, false, true, false>(v);
-#pragma unroll
-            for (int m = 1; m < R1; m++) v[m] = cmul(v[m], twx[t * m]);
-#pragma unroll
-            for (int m = 0; m < R1; m++) E[m * EP + t * T + j] = v[m];
+    for (uint32_t phase = 0; item < nitems; phase ^= 1u) {
+        if (__syncthreads_or(!mbar_wait_parity_bounded(&bar, phase, polls))) {
+            // the copies did not land in time for some thread: the whole block flags it, leaves
+            // this item untransformed, and stops taking items once the copies into shared memory
+            // have finished (bounded again)
+            if (tid == 0) atomicOr(A.err, ERR_FFT_TIMEOUT);
+            mbar_wait_parity_bounded(&bar, phase, STAGE_WAIT_POLLS);
+            break;
         }
-        __syncthreads();
+        // forward x transform of the three components; thread (j, m) keeps X[c][m + R1 q]
+        float2 X[3][R2];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            if (r < R2) {
+                const uint32_t t = r;
+                float2 v[R1];
+#pragma unroll
+                for (int k = 0; k < R1 / 2; k++) {         // rows x >= M0/2 are zero
+                    const uint32_t xx = t + R2 * k;
+                    v[k] = xx < A.bx ? Ys[(c * A.bx + xx) * T + j] : make_float2(0.f, 0.f);
+                }
+                dftp<R1, false, true, false>(v);
+#pragma unroll
+                for (int m = 1; m < R1; m++) v[m] = cmul(v[m], twx[t * m]);
+#pragma unroll
+                for (int m = 0; m < R1; m++) E[m * EP + t * T + j] = v[m];
+            }
+            __syncthreads();
+            {
+                const uint32_t m = r;
+#pragma unroll
+                for (int t = 0; t < R2; t++) X[c][t] = E[m * EP + t * T + j];
+                dft<R2, false>(X[c]);
+            }
+            __syncthreads();
+        }
+        // the forward transform has read Ys (the barrier that ends its last component): the next
+        // item's spectrum goes there, the expected bytes counting its N_k tile too
+        if (tid == 0) {
+            const uint32_t nx = gridDim.x + atomicAdd(A.xq, 1u);
+            next_item = nx;
+            if (nx < nitems) {
+                fence_async_smem();
+                mbar_arrive_expect_tx(&bar, ys_bytes + ns_bytes);
+                for (uint32_t c = 0; c < 3; c++) bulk_copy_stream(Ys + c * slab, slab_of(nx, c), slab * 8u, &bar);
+            }
+        }
+        // H_k = N_k M_k at kx = m + R1 q
         {
             const uint32_t m = r;
 #pragma unroll
-            for (int t = 0; t < R2; t++) X[c][t] = E[m * EP + t * T + j];
-            dft<R2, false>(X[c]);
-        }
-        __syncthreads();
-    }
-    // H_k = N_k M_k at kx = m + R1 q
-    {
-        const uint32_t m = r;
+            for (int q = 0; q < R2; q++) {
+                const uint32_t kx = m + R1 * q;
+                const float2 a = X[0][q], b = X[1][q], cc = X[2][q];
+                if constexpr (!CPLX) {
+                    const float* Ns = reinterpret_cast<const float*>(Nsb);
+                    const bool mir = kx >= A.nkx;                  // kx > M0/2 in the half layout
+                    const uint32_t row = mir ? M0 - kx : kx, nk = A.nkx;
+                    const uint32_t neg = mir ? A.odd : 0u;
+                    float n6[6];
 #pragma unroll
-        for (int q = 0; q < R2; q++) {
-            const uint32_t kx = m + R1 * q;
-            const float2 a = X[0][q], b = X[1][q], cc = X[2][q];
-            if constexpr (!CPLX) {
-                const float* Ns = reinterpret_cast<const float*>(Nsb);
-                const bool mir = kx >= A.nkx;                  // kx > M0/2 in the half layout
-                const uint32_t row = mir ? M0 - kx : kx, nk = A.nkx;
-                const uint32_t neg = mir ? A.odd : 0u;
-                float n6[6];
+                    for (int q6 = 0; q6 < 6; q6++) {
+                        const float v = Ns[(q6 * nk + row) * T + j];
+                        n6[q6] = (neg >> q6) & 1u ? -v : v;
+                    }
+                    X[0][q] = make_float2(n6[0] * a.x + n6[1] * b.x + n6[2] * cc.x, n6[0] * a.y + n6[1] * b.y + n6[2] * cc.y);
+                    X[1][q] = make_float2(n6[1] * a.x + n6[3] * b.x + n6[4] * cc.x, n6[1] * a.y + n6[3] * b.y + n6[4] * cc.y);
+                    X[2][q] = make_float2(n6[2] * a.x + n6[4] * b.x + n6[5] * cc.x, n6[2] * a.y + n6[4] * b.y + n6[5] * cc.y);
+                } else {
+                    const float2* Ns = reinterpret_cast<const float2*>(Nsb);
+                    const float2 v[3] = {a, b, cc};
 #pragma unroll
-                for (int q6 = 0; q6 < 6; q6++) {
-                    const float v = Ns[(q6 * nk + row) * T + j];
-                    n6[q6] = (neg >> q6) & 1u ? -v : v;
-                }
-                X[0][q] = make_float2(n6[0] * a.x + n6[1] * b.x + n6[2] * cc.x, n6[0] * a.y + n6[1] * b.y + n6[2] * cc.y);
-                X[1][q] = make_float2(n6[1] * a.x + n6[3] * b.x + n6[4] * cc.x, n6[1] * a.y + n6[3] * b.y + n6[4] * cc.y);
-                X[2][q] = make_float2(n6[2] * a.x + n6[4] * b.x + n6[5] * cc.x, n6[2] * a.y + n6[4] * b.y + n6[5] * cc.y);
-            } else {
-                const float2* Ns = reinterpret_cast<const float2*>(Nsb);
-                const float2 v[3] = {a, b, cc};
+                    for (int al = 0; al < 3; al++) {
+                        float2 o = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int al = 0; al < 3; al++) {
-                    float2 o = make_float2(0.f, 0.f);
-#pragma unroll
-                    for (int be = 0; be < 3; be++) o = cadd(o, cmul(Ns[((3 * al + be) * M0 + kx) * T + j], v[be]));
-                    X[al][q] = o;
+                        for (int be = 0; be < 3; be++) o = cadd(o, cmul(Ns[((3 * al + be) * M0 + kx) * T + j], v[be]));
+                        X[al][q] = o;
+                    }
                 }
             }
         }
-    }
-    // inverse x transform, box rows only, into Ys
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        {
-            const uint32_t m = r;
-            dft<R2, true>(X[c]);
-#pragma unroll
-            for (int t = 0; t < R2; t++) E[m * EP + t * T + j] = t ? cmulc(X[c][t], twx[t * m]) : X[c][t];
+        __syncthreads();                              // every thread has read its N_k values
+        const uint32_t next = next_item;
+        if (next < nitems && tid == 0) {
+            fence_async_smem();
+            bulk_copy_stream(Nsb, nk_of(next), ns_bytes, &bar);
         }
-        __syncthreads();
-        if (r < R2) {
-            const uint32_t t = r;
-            float2 w[R1];
+        // inverse x transform, box rows only, straight to the item's slabs in global memory
 #pragma unroll
-            for (int m = 0; m < R1; m++) w[m] = E[m * EP + t * T + j];
-            dftp<R1, true, false, true>(w);            // the rows x < M0/2 only
+        for (int c = 0; c < 3; c++) {
+            {
+                const uint32_t m = r;
+                dft<R2, true>(X[c]);
 #pragma unroll
-            for (int k = 0; k < R1 / 2; k++) {
-                const uint32_t xx = t + R2 * k;
-                if (xx < A.bx) Ys[(c * A.bx + xx) * T + j] = w[k];
+                for (int t = 0; t < R2; t++) E[m * EP + t * T + j] = t ? cmulc(X[c][t], twx[t * m]) : X[c][t];
             }
+            __syncthreads();
+            if (r < R2) {
+                const uint32_t t = r;
+                float2 w[R1];
+#pragma unroll
+                for (int m = 0; m < R1; m++) w[m] = E[m * EP + t * T + j];
+                dftp<R1, true, false, true>(w);        // the rows x < M0/2 only
+                float2* gy = slab_of(item, c);
+#pragma unroll
+                for (int k = 0; k < R1 / 2; k++) {
+                    const uint32_t xx = t + R2 * k;
+                    if (xx < A.bx) gy[xx * T + j] = w[k];
+                }
+            }
+            __syncthreads();
         }
-        __syncthreads();
+        item = next;
     }
-    fence_async_smem();
-    __syncthreads();
+    // every block has taken its last item once all have finished: the last one rearms the counters
     if (tid == 0) {
-        for (int c = 0; c < 3; c++) bulk_store(gy[c], Ys + c * slab, slab * 8u);
-        bulk_commit_wait_read();
+        uint32_t done;
+        asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], 1;" : "=r"(done) : "l"(A.xq + 1) : "memory");
+        if (done == gridDim.x - 1) { A.xq[0] = 0u; A.xq[1] = 0u; }
     }
 }
 
@@ -640,6 +677,7 @@ PlaneArgs plane_args(const LongRange& L) {
     A.P = L.P;
     A.twt = L.twt;
     A.twx_off = 2 * N + 1 + m1;
+    A.xq = L.xq;
     return A;
 }
 
@@ -706,21 +744,45 @@ cudaError_t run_zy(const LongRange& L, const PlaneArgs& A, bool inverse, cudaStr
     return e != cudaSuccess ? e : cudaGetLastError();
 }
 
+// Blocks of a persistent kernel: as many as are resident on the device at once (cached per
+// kernel, block size, shared memory and device), at most `work`.
+template <typename K>
+cudaError_t resident_grid(K kern, uint32_t block, size_t smem, uint32_t work, uint32_t* grid) {
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, uint32_t, size_t, int>, uint32_t> cache;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const auto key = std::make_tuple(reinterpret_cast<const void*>(kern), block, smem, dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+        int per_sm = 0, sms = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)block, smem)) != cudaSuccess) return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        it = cache.emplace(key, (uint32_t)std::max(1, per_sm) * (uint32_t)std::max(1, sms)).first;
+    }
+    *grid = std::min(work, it->second);
+    return cudaSuccess;
+}
+
+template <int R1, int R2, bool CPLX>
+cudaError_t run_xconv_k(const LongRange& L, const PlaneArgs& A, cudaStream_t st, bool pdl) {
+    const uint32_t Kz = L.mesh[2] / 2 + 1;
+    const size_t sm = xconv_smem(A, CPLX);
+    const uint32_t block = PT * R1;
+    cudaError_t e;
+    uint32_t grid = 0;
+    if ((e = set_smem(plane_x_conv<R1, R2, CPLX>, sm)) != cudaSuccess) return e;
+    if ((e = resident_grid(plane_x_conv<R1, R2, CPLX>, block, sm, A.ntile * Kz, &grid)) != cudaSuccess) return e;
+    const void* nkt = L.nkt;
+    e = launch_step_kernel(plane_x_conv<R1, R2, CPLX>, dim3(grid), dim3(block), sm, st, 1, pdl, L.yk, nkt, Kz, A);
+    return e != cudaSuccess ? e : cudaGetLastError();
+}
+
 template <int R1, int R2>
 cudaError_t run_xconv_t(const LongRange& L, const PlaneArgs& A, bool cplx, cudaStream_t st, bool pdl) {
-    const uint32_t Kz = L.mesh[2] / 2 + 1;
-    const dim3 grid(A.ntile, Kz);
-    const size_t sm = xconv_smem(A, cplx);
-    cudaError_t e;
-    const void* nkt = L.nkt;
-    if (cplx) {
-        if ((e = set_smem(plane_x_conv<R1, R2, true>, sm)) != cudaSuccess) return e;
-        e = launch_step_kernel(plane_x_conv<R1, R2, true>, grid, dim3(PT * R1), sm, st, 1, pdl, L.yk, nkt, Kz, A);
-    } else {
-        if ((e = set_smem(plane_x_conv<R1, R2, false>, sm)) != cudaSuccess) return e;
-        e = launch_step_kernel(plane_x_conv<R1, R2, false>, grid, dim3(PT * R1), sm, st, 1, pdl, L.yk, nkt, Kz, A);
-    }
-    return e != cudaSuccess ? e : cudaGetLastError();
+    return cplx ? run_xconv_k<R1, R2, true>(L, A, st, pdl) : run_xconv_k<R1, R2, false>(L, A, st, pdl);
 }
 
 cudaError_t run_xconv(const LongRange& L, const PlaneArgs& A, bool cplx, cudaStream_t st, bool pdl) {
@@ -809,12 +871,15 @@ cudaError_t build_nk_tiles(asd_handle* h, const double2* z, uint32_t ncomp, bool
     return cudaGetLastError();
 }
 
-// Twiddle table of the plane kernels (allocates L.twt).
+// Twiddle table of the plane kernels (allocates L.twt) and the x pass's item counters (L.xq,
+// zeroed).
 cudaError_t build_plane_twiddles(asd_handle* h) {
     LongRange& L = h->lr;
     const uint32_t N = L.mesh[2] / 2, n = 2 * N + 1 + L.mesh[1] + L.mesh[0];
     cudaError_t e = cudaMalloc(&L.twt, sizeof(float2) * n);
     if (e != cudaSuccess) return e;
+    if ((e = cudaMalloc(&L.xq, 2 * sizeof(uint32_t))) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(L.xq, 0, 2 * sizeof(uint32_t), h->stream)) != cudaSuccess) return e;
     tw_table_k<<<nbk(n, 256), 256, 0, h->stream>>>(N, L.mesh[1], L.mesh[0], L.twt);
     return cudaGetLastError();
 }

@@ -77,6 +77,12 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t limit)
         if (mbar_try_wait(bar, 0)) return true;
     return false;
 }
+// The same for phase `parity` of a barrier that completes once per item of a loop.
+__device__ __forceinline__ bool mbar_wait_parity_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    for (uint32_t it = 0; it < limit; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
 constexpr uint32_t STAGE_WAIT_POLLS = 1u << 22;
 constexpr uint32_t ERR_STAGE_TIMEOUT = 1u;
 

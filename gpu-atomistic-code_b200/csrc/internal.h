@@ -107,6 +107,7 @@ struct LongRange {
     float2* yk = nullptr;
     void* nkt = nullptr;
     float2* twt = nullptr;          // twiddle table of the plane kernels
+    uint32_t* xq = nullptr;           // x-pass item counters: next item, finished blocks
     // FP64 plain: complex padded arrays [3][P] and full complex N_k [9][P]
     double2 *zr = nullptr, *zk = nullptr, *zh = nullptr, *znk = nullptr;
     cufftHandle z2z = 0;
