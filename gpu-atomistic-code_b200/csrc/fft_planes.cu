@@ -22,9 +22,6 @@
 #include <algorithm>
 #include <cooperative_groups.h>
 #include <cstring>
-#include <map>
-#include <mutex>
-#include <tuple>
 
 namespace asd {
 namespace {
@@ -64,7 +61,6 @@ __device__ __forceinline__ void bulk_commit_wait_read() {
     asm volatile("cp.async.bulk.commit_group;" ::: "memory");
     asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
 }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Y element (c, kz, x, ky) in the tiled spectrum layout [c][kz][ky / PT][x][ky % PT].
 __device__ __forceinline__ size_t yk_index(const PlaneArgs& A, uint32_t Kz, uint32_t c, uint32_t kz, uint32_t x,
@@ -744,28 +740,6 @@ cudaError_t run_zy(const LongRange& L, const PlaneArgs& A, bool inverse, cudaStr
     return e != cudaSuccess ? e : cudaGetLastError();
 }
 
-// Blocks of a persistent kernel: as many as are resident on the device at once (cached per
-// kernel, block size, shared memory and device), at most `work`.
-template <typename K>
-cudaError_t resident_grid(K kern, uint32_t block, size_t smem, uint32_t work, uint32_t* grid) {
-    static std::mutex mu;
-    static std::map<std::tuple<const void*, uint32_t, size_t, int>, uint32_t> cache;
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    const auto key = std::make_tuple(reinterpret_cast<const void*>(kern), block, smem, dev);
-    std::lock_guard<std::mutex> lock(mu);
-    auto it = cache.find(key);
-    if (it == cache.end()) {
-        int per_sm = 0, sms = 0;
-        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, (int)block, smem)) != cudaSuccess) return e;
-        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
-        it = cache.emplace(key, (uint32_t)std::max(1, per_sm) * (uint32_t)std::max(1, sms)).first;
-    }
-    *grid = std::min(work, it->second);
-    return cudaSuccess;
-}
-
 template <int R1, int R2, bool CPLX>
 cudaError_t run_xconv_k(const LongRange& L, const PlaneArgs& A, cudaStream_t st, bool pdl) {
     const uint32_t Kz = L.mesh[2] / 2 + 1;
@@ -774,7 +748,9 @@ cudaError_t run_xconv_k(const LongRange& L, const PlaneArgs& A, cudaStream_t st,
     cudaError_t e;
     uint32_t grid = 0;
     if ((e = set_smem(plane_x_conv<R1, R2, CPLX>, sm)) != cudaSuccess) return e;
-    if ((e = resident_grid(plane_x_conv<R1, R2, CPLX>, block, sm, A.ntile * Kz, &grid)) != cudaSuccess) return e;
+    if ((e = resident_grid(reinterpret_cast<const void*>(plane_x_conv<R1, R2, CPLX>), block, sm, A.ntile * Kz, &grid)) !=
+        cudaSuccess)
+        return e;
     const void* nkt = L.nkt;
     e = launch_step_kernel(plane_x_conv<R1, R2, CPLX>, dim3(grid), dim3(block), sm, st, 1, pdl, L.yk, nkt, Kz, A);
     return e != cudaSuccess ? e : cudaGetLastError();

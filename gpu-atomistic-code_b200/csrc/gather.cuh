@@ -77,6 +77,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t limit)
         if (mbar_try_wait(bar, 0)) return true;
     return false;
 }
+// Orders this thread's earlier generic-proxy shared-memory accesses (and, after a block barrier,
+// the block's) before its later bulk copies into the same memory.
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
 // The same for phase `parity` of a barrier that completes once per item of a loop.
 __device__ __forceinline__ bool mbar_wait_parity_bounded(uint64_t* bar, uint32_t parity, uint32_t limit) {
     for (uint32_t it = 0; it < limit; it++)

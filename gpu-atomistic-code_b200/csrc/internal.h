@@ -294,6 +294,9 @@ cudaError_t launch_convert_spins_in(asd_handle* h, const double* d_aos);
 // Raise a kernel's dynamic shared-memory limit on the current device to at least `bytes`,
 // calling cudaFuncSetAttribute only when this (device, kernel) has not been raised that far.
 cudaError_t raise_smem_limit(const void* kernel, size_t bytes);
+// Blocks of a persistent kernel: as many as are resident on the device at once (cached per
+// kernel, block size, shared memory and device), at most `work` (and at least 1).
+cudaError_t resident_grid(const void* kernel, uint32_t block, size_t smem, uint32_t work, uint32_t* grid);
 
 // Launch of a step kernel (one that starts with pdl_enter): with `pdl` its blocks may become
 // resident while the previous kernel of the stream finishes (programmatic dependent launch);

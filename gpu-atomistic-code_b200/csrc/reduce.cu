@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <map>
 #include <mutex>
+#include <tuple>
 
 namespace asd {
 namespace {
@@ -538,6 +539,26 @@ cudaError_t raise_smem_limit(const void* kernel, size_t bytes) {
     e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e == cudaSuccess) have = bytes;
     return e;
+}
+
+cudaError_t resident_grid(const void* kernel, uint32_t block, size_t smem, uint32_t work, uint32_t* grid) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    static std::mutex mu;
+    static std::map<std::tuple<const void*, uint32_t, size_t, int>, uint32_t> cache;
+    const auto key = std::make_tuple(kernel, block, smem, dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it == cache.end()) {
+        int per_sm = 0, sms = 0;
+        if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (int)block, smem)) != cudaSuccess)
+            return e;
+        if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+        it = cache.emplace(key, (uint32_t)std::max(1, per_sm) * (uint32_t)std::max(1, sms)).first;
+    }
+    *grid = std::max(1u, std::min(work, it->second));
+    return cudaSuccess;
 }
 
 cudaError_t launch_check_spins(asd_handle* h, const double* d_aos, unsigned long long* d_check) {
