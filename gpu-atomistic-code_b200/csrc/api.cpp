@@ -91,6 +91,7 @@ void free_all(asd_handle* h) {
     F(h->d_magpart); F(h->d_mag); F(h->d_magcnt); F(h->d_inv_count); F(h->d_sub_of_atom); F(h->d_stats);
     if (h->graph) cudaGraphExecDestroy(h->graph);
     if (h->graph1) cudaGraphExecDestroy(h->graph1);
+    if (h->graph1_src) cudaGraphDestroy(h->graph1_src);
     if (h->kev[0]) cudaEventDestroy(h->kev[0]);
     if (h->kev[1]) cudaEventDestroy(h->kev[1]);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -573,6 +574,15 @@ void autotune(asd_handle* h) {
 void destroy_graph(asd_handle* h) {
     if (h->graph) { cudaGraphExecDestroy(h->graph); h->graph = nullptr; h->graph_steps = 0; }
     if (h->graph1) { cudaGraphExecDestroy(h->graph1); h->graph1 = nullptr; }
+    if (h->graph1_src) { cudaGraphDestroy(h->graph1_src); h->graph1_src = nullptr; }
+    h->det_node = nullptr;
+}
+
+// The applied field on the device, where a single-step graph has not yet written it.
+void flush_applied(asd_handle* h) {
+    if (!h->applied_pending) return;
+    CK(launch_set_vec3(h, h->d_dyn + DYN_APPLIED, h->d_dynf + DYN_APPLIED, h->p.applied));
+    h->applied_pending = false;
 }
 
 // Capture `steps` fused steps + the counter advance into one graph, and a one-step graph for
@@ -613,7 +623,20 @@ void build_graph(asd_handle* h, uint32_t steps) {
     CK(e);
     CK(e2);
     CK(cudaGraphInstantiate(&h->graph1, g, 0));
-    cudaGraphDestroy(g);
+    // keep the captured graph and its det_here_k node: asd_set_applied updates the node in place
+    h->graph1_src = g;
+    size_t nn = 0;
+    CK(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType ty;
+        CK(cudaGraphNodeGetType(nd, &ty));
+        if (ty != cudaGraphNodeTypeKernel) continue;
+        cudaKernelNodeParams kp{};
+        CK(cudaGraphKernelNodeGetParams(nd, &kp));
+        if (kp.func == det_here_kernel()) { h->det_node = nd; break; }
+    }
 }
 
 void run_steps(asd_handle* h, uint64_t nsteps) {
@@ -625,12 +648,14 @@ void run_steps(asd_handle* h, uint64_t nsteps) {
     }
     scatter_if_needed(h);
     if (nsteps == 1 && h->graph1 && !h->timing) {
-        // one launch: the graph sets the det-field step to the step it runs
+        // one launch: the graph sets the det-field step to the step it runs, and the applied field
         CK(cudaGraphLaunch(h->graph1, h->stream));
         h->launches += h->graph1_launches;
+        h->applied_pending = false;
         h->step += 1;
         return;
     }
+    flush_applied(h);
     set_dyn(h, DYN_DET_STEP, (double)(h->step + nsteps - 1));
     const uint32_t upd = h->p.update ? h->p.update : 1;
     const uint32_t G = h->graph_steps;
@@ -1138,6 +1163,7 @@ static int read_back(asd_handle* h, int what, double* out, size_t n_spins) {
             return ASD_OK;
         }
         double* d = aos_buffer(h);
+        if (what == 2) flush_applied(h);
         cudaError_t e = what == 2 ? launch_field_only(h, d) : launch_convert_out(h, what, d);
         if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, h->stream);
         cudaError_t e2 = cudaStreamSynchronize(h->stream);
@@ -1456,7 +1482,15 @@ int asd_set_applied(asd_handle* h, const double applied[3]) {
         CK(cudaSetDevice(h->device));
         for (int a = 0; a < 3; a++) REQUIRE(std::isfinite(applied[a]), "non-finite applied field");
         for (int a = 0; a < 3; a++) h->p.applied[a] = applied[a];
-        CK(launch_set_vec3(h, h->d_dyn + DYN_APPLIED, h->d_dynf + DYN_APPLIED, applied));
+        if (h->graph1 && h->det_node) {
+            // the one-step graph's first node carries it (a parameter update, no launch); any
+            // other work that reads it flushes it first
+            CK(update_det_applied(h));
+            h->applied_pending = true;
+        } else {
+            CK(launch_set_vec3(h, h->d_dyn + DYN_APPLIED, h->d_dynf + DYN_APPLIED, applied));
+            h->applied_pending = false;
+        }
     } catch (const Fail& f) { return fail(h, f); }
     return ASD_OK;
 }

@@ -412,9 +412,16 @@ __global__ void advance_k(uint64_t* step, uint32_t n) {
     *step += n;
 }
 // The det field is written at the step the device counter holds (the one-step graph's step).
-__global__ void det_here_k(const uint64_t* step, double* dyn) {
+// The applied field rides in the parameters of this first node of the one-step graph: a new
+// value updates the node in place, so a single-step call needs no launch of its own for it.
+struct AppliedArg { double v[3]; };
+__global__ void det_here_k(const uint64_t* step, double* dyn, float* dynf, AppliedArg applied) {
     pdl_enter();
     dyn[DYN_DET_STEP] = (double)*step;
+    for (int k = 0; k < 3; k++) {
+        dyn[DYN_APPLIED + k] = applied.v[k];
+        dynf[DYN_APPLIED + k] = (float)applied.v[k];
+    }
 }
 
 template <typename R>
@@ -672,10 +679,30 @@ cudaError_t launch_fused_step(asd_handle* h, uint32_t rel, bool) {
 }
 
 cudaError_t launch_det_here(asd_handle* h) {
+    const AppliedArg ap{{h->p.applied[0], h->p.applied[1], h->p.applied[2]}};
     const cudaError_t e = launch_step_kernel(det_here_k, dim3(1), dim3(1), 0, h->stream, 1, step_pdl(h),
-                                             (const uint64_t*)h->d_step, h->d_dyn);
+                                             (const uint64_t*)h->d_step, h->d_dyn, h->d_dynf, ap);
     h->launches += 1;
     return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+const void* det_here_kernel() { return reinterpret_cast<const void*>(det_here_k); }
+
+cudaError_t update_det_applied(asd_handle* h) {
+    if (!h->graph1 || !h->det_node) return cudaErrorInvalidValue;
+    const uint64_t* step = h->d_step;
+    double* dyn = h->d_dyn;
+    float* dynf = h->d_dynf;
+    AppliedArg ap{{h->p.applied[0], h->p.applied[1], h->p.applied[2]}};
+    void* args[] = {&step, &dyn, &dynf, &ap};
+    cudaKernelNodeParams kp{};
+    kp.func = reinterpret_cast<void*>(det_here_k);
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(1);
+    kp.sharedMemBytes = 0;
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    return cudaGraphExecKernelNodeSetParams(h->graph1, h->det_node, &kp);
 }
 
 cudaError_t launch_step_advance(asd_handle* h, uint32_t nsteps) {

@@ -213,6 +213,9 @@ struct asd_handle {
     cudaGraphExec_t graph = nullptr;
     uint32_t graph_steps = 0;
     cudaGraphExec_t graph1 = nullptr;    // one step (single-step calls)
+    cudaGraph_t graph1_src = nullptr;    // its captured graph (kept: its det node is updated in place)
+    cudaGraphNode_t det_node = nullptr;  // the one-step graph's det_here_k, which also writes the applied field
+    bool applied_pending = false;        // the applied field awaits the next one-step graph or a flush
     uint64_t graph1_launches = 0;
     int block = 256;
     // timing of the dominant kernel
@@ -261,6 +264,9 @@ cudaError_t launch_plain_step(asd_handle* h, uint64_t t);
 cudaError_t launch_fused_step(asd_handle* h, uint32_t rel, bool in_capture);
 cudaError_t launch_step_advance(asd_handle* h, uint32_t nsteps);
 cudaError_t launch_det_here(asd_handle* h);
+// The one-step graph's det_here_k node with the applied field h->p.applied (no launch).
+cudaError_t update_det_applied(asd_handle* h);
+const void* det_here_kernel();
 cudaError_t launch_lr_eval_f32(asd_handle* h);
 cudaError_t launch_lr_scatter(asd_handle* h);
 cudaError_t launch_lr_planes(asd_handle* h);

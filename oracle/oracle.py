@@ -181,6 +181,7 @@ class Oracle:
                               _ptr(self._an[1], C.c_double), an.get("k4perp", 0.0), _ptr(self._an[2], C.c_double),
                               an.get("k4par", 0.0), _ptr(self._an[3], C.c_double), basemm)
         ap = a64(applied)
+        self._integrator, self._rdt = integrator, dt * GYRO
         L.orc_set_dynamics(self.c, integrator, dt * GYRO, _ptr(ap, C.c_double))
         roff = au32(np.concatenate([[0], np.cumsum([s.nspins for s in systems])]))
         T = a64([s.temperature for s in systems])
@@ -277,6 +278,12 @@ class Oracle:
     def step(self, k):
         olib().orc_run(self.c, self.t, k)
         self.t += k
+
+    def set_applied(self, b):
+        """The applied field from the next step on, as the reference's field ramp sets
+        llg::applied between steps (src/ramp_field.cpp:221-223)."""
+        ap = a64(b)
+        olib().orc_set_dynamics(self.c, self._integrator, self._rdt, _ptr(ap, C.c_double))
 
     def magnetisation(self):
         out = np.empty(len(self.systems) * self.nsub * 3)
