@@ -442,8 +442,10 @@ __global__ void __launch_bounds__(PT * R1, CPLX ? 1 : 3) plane_x_conv(float2* __
 }
 
 // ---------------------------------------------------------------- inverse: y then z (C2R)
+// 4 blocks per SM (64 registers, no spill) where the z rows are at most 64 points (8 × 8), 3
+// for the longer rows, whose passes spill at 64; like the forward kernel.
 template <int Z1, int Z2, int R1, int R2>
-__global__ void __launch_bounds__(256, 3) plane_yz_inv(const float2* __restrict__ yk, float* __restrict__ hr,
+__global__ void __launch_bounds__(256, (Z1 > 8 ? 3 : 4)) plane_yz_inv(const float2* __restrict__ yk, float* __restrict__ hr,
                                                        const PlaneArgs A) {
     using G = ZYGeom<Z1, Z2, R1, R2>;
     constexpr uint32_t N = G::N, KZ = G::KZ, TY = G::TY, LD = G::LD, M1 = G::M1;
