@@ -109,14 +109,15 @@ __constant__ double FRK5B[5][5] = {
 __constant__ double FRK5C[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
 __constant__ double FRK4C[4] = {1.0 / 6.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 6.0};
 
-// Register caps of the FP32 kernels, chosen from ptxas reports so that none spills: 6 blocks
-// of 256 per SM (40 registers) for the full-tensor SELL kernels but their RK stages before the
-// last, and for the field-only kernels; 5 (48) for the rest; the FP64 kernels keep the default
-// cap.
+// Register caps of the FP32 kernels: 6 blocks of 256 per SM (40 registers) for the SELL and
+// the field-only kernels, 5 (48) for the DIA kernels; the FP64 kernels keep the default cap.
+// At 40 the diagonal-tensor SELL kernels spill 76 bytes a thread (the others none), and still
+// run faster than at 48: the extra warps hide more of the gather's latency than the spills add
+// (96 replicas 564 → 534 µs per step, the north star unchanged, A/B on one box).
 template <typename R, int EX, bool FULL, int K>
 struct MinBlocks {
     static constexpr int value =
-        sizeof(R) != 4 ? 1 : ((EX == ASD_EXCH_CSR && FULL && K != 3) || EX == ASD_EXCH_NONE) ? 6 : 5;
+        sizeof(R) != 4 ? 1 : (EX == ASD_EXCH_CSR || EX == ASD_EXCH_NONE) ? 6 : 5;
 };
 
 // K: the stage kind at compile time (1 Heun predictor, 2 Heun corrector, 3 RK stage before the
