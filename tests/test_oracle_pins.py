@@ -127,6 +127,30 @@ def test_single_spin_precession_matches_analytic():
     assert abs(((phi - expect + math.pi) % (2 * math.pi)) - math.pi) < 1e-4
 
 
+def test_oracle_applied_field_change_between_steps():
+    """set_applied between steps (the reference's field ramp, src/ramp_field.cpp:221-223) gives
+    the run of an oracle built with that field from the same spins and step on (to the rounding
+    of set_spins' renormalisation), and one kept at the old field differs."""
+    s = LT.sc_ferromagnet(4, T=30.0)
+    S = LT.random_spins(s.nspins, 6)
+    a = O.Oracle(s, applied=(0.0, 0.0, 0.5))
+    a.set_spins(S)
+    a.step(5)
+    a.set_applied((0.3, -0.2, 1.0))
+    mid = a.spins().copy()
+    b = O.Oracle(s, applied=(0.3, -0.2, 1.0))
+    b.set_spins(mid)
+    b.t = a.t
+    a.step(7)
+    b.step(7)
+    assert maxdiff(a.spins(), b.spins()) <= 1e-13, maxdiff(a.spins(), b.spins())
+    c = O.Oracle(s, applied=(0.0, 0.0, 0.5))
+    c.set_spins(mid)
+    c.t = 5
+    c.step(7)
+    assert maxdiff(a.spins(), c.spins()) > 1e-9     # the new field changed the dynamics
+
+
 def test_magnetisation_oracle():
     s = LT.sc_ferromagnet(4)
     o = O.Oracle(s)
