@@ -176,7 +176,9 @@ int asd_set_state(asd_handle* h, const void* buf, size_t len);
 
 /* llg::T (passed per launch, src/cuda.cu:159); replica ASD_ALL_REPLICAS sets all. */
 int asd_set_temperature(asd_handle* h, uint32_t replica, double T);
-/* llg::applied (src/cuda.cu:159). */
+/* llg::applied (src/cuda.cu:159), in effect from the next step.  In the fused forms a following
+ * asd_step(h, 1) carries it in its one-step graph (no launch of its own); any other call that
+ * reads it on the device sends it first. */
 int asd_set_applied(asd_handle* h, const double applied[3]);
 /* cullg::CsetStagFields / CsetStagFieldsZero (src/cuda_util.cu:563-588): profile 3N [T], NULL zeroes it. */
 int asd_set_site_field(asd_handle* h, const double* profile, size_t n_spins);
@@ -188,7 +190,9 @@ int asd_set_site_field_scale(asd_handle* h, double rv);
  * profile with t = step*dt [s]; amp = 0 switches the envelope off (site field = rv * profile). */
 int asd_set_site_field_pulse(asd_handle* h, double amp, double t0, double sigma);
 
-/* util::calc_mag method 0 (src/util_mag.cpp:44-65) per replica: out[(r*nsub+s)*3+c], FP64 sums. */
+/* util::calc_mag method 0 (src/util_mag.cpp:44-65) per replica: out[(r*nsub+s)*3+c], FP64 sums.
+ * A page-locked `out` (cudaHostAlloc / cudaHostRegister) that this device can address receives
+ * the means from the reduction kernel itself; any other buffer by a copy.  Returns after both. */
 int asd_magnetisation(asd_handle* h, double* out, size_t out_len);
 /* Sublattice-mean magnetisation of spins that already sit in device memory, without any
  * device allocation.  No counterpart in the reference: it exists for callers that cannot call
